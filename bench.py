@@ -1,0 +1,343 @@
+#!/usr/bin/env python3
+"""Training-step benchmark: batched adjoint, 1M Gaussians (SH degree 3) x 8 uneven views
+up to 1920x1080, fused L1 + D-SSIM loss, Adam; steps/s on B200 beside the plain
+one-view-per-launch path and the reference's algorithm on the host CPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  value = whole-job training steps per second (each step
+= forward + loss + backward + Adam over one rank's 8 views, summed over ranks), device
+time measured with CUDA events on the library's stream; e2e = the same step through the
+public C ABI with this step's target photos copied host->device (pinned) and the loss
+copied back every step.
+"""
+import argparse
+import ctypes
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "train steps/s, 1M splats x 8 views@1080p: batched adjoint vs plain; grad err vs FP64"
+WORKLOAD = "1M Gaussians SH3, 8 views 640x480..1920x1080 (9,157,632 px), L1+D-SSIM(11-tap), Adam"
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+# ---------------------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = dict(sm_mhz=None, sm_max_mhz=None, reasons=[], samples=0)
+        if not self.proc:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return out
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3][k].lower() == "active"})
+        loaded = [r[0] for r in rows if r[2] > 300] or [r[0] for r in rows]
+        return dict(sm_mhz=statistics.median(loaded), sm_max_mhz=max(r[1] for r in rows), reasons=reasons,
+                    samples=len(rows), power_w_max=max(r[2] for r in rows))
+
+
+# ---------------------------------------------------------------------------------------
+def workload(hmp, rank, world):
+    """Config 3: scene (seed 3) and ring cameras; rank r sees the ring rotated by r/N of a
+    camera spacing (its own 8 views)."""
+    c = hmp.config(3)
+    cams = c["cameras"]
+    if world > 1:
+        cams = []
+        for i, (w, h) in enumerate(hmp.scene.CONFIG3_RESOLUTIONS):
+            a = 2 * math.pi * (i + rank / world) / 8
+            cams.append(hmp.look_at([4 * math.sin(a), 0.0, 4 * math.cos(a)], [0, 0, 0], w, h, 900.0 / 1024.0 * w))
+    return c, cams
+
+
+def make_targets(hmp, c, cams, device):
+    """Target photos: the scene with means jittered by N(0, 0.02) (seed-2 copy), rendered
+    by this library and quantised to RGB bytes like decoded photos."""
+    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], device=device) as r:
+        r.set_gaussians(hmp.scene.jitter_means(c["records"], 2))
+        r.set_views(cams)
+        imgs = r.forward(0, len(cams))
+    return np.round(np.clip(imgs, 0.0, 1.0) * 255.0).astype(np.uint8)
+
+
+def algorithmic_bytes(st, n, planes, views, pixels):
+    """Bytes each stage must move per step (the roofline numerators)."""
+    P = planes * 4
+    pairs = n * views
+    inst = st["instances"]
+    passes_pairs, passes_inst = 4, 2
+    return {
+        "project": n * P + pairs * (48 + 8 + 4),
+        "sort_pairs": passes_pairs * pairs * (4 + 8 + 8),
+        "emit": pairs * (4 + 8) * 2 + inst * 8,
+        "sort_instances": passes_inst * inst * (4 + 8 + 8) + inst * 4,
+        "loss": pixels * (12 + 3 + 12),
+        "project_bwd": 2 * n * P + pairs * 36,
+        "adam": 7 * n * P,
+    }
+
+
+def run_b200(args, rank, local, world, dist):
+    hmp = importlib.import_module("home-measure-privacy_b200")
+    from importlib import import_module
+    N = import_module("home-measure-privacy_b200._native")
+    device = local
+    c, cams = workload(hmp, rank, world)
+    targets = make_targets(hmp, c, cams, device)
+    n = c["records"].shape[0]
+    V = len(cams)
+    pixels = sum(cm["width"] * cm["height"] for cm in cams)
+    lam, window = c["ssim_lambda"], c["window"]
+    ad = hmp.adam_config()
+    res = {}
+
+    def setup(batched):
+        r = hmp.createRenderer(sh_degree=c["degree"], near=c["near"], batched=batched, use_graph=True,
+                               device=device)
+        r.set_gaussians(c["records"])
+        r.set_views(cams)
+        off = 0
+        for v, cm in enumerate(cams):
+            px = cm["width"] * cm["height"] * 3
+            r.set_target(v, targets[off:off + px])
+            off += px
+        return r
+
+    def timed(r, steps, warmup, host=None):
+        for _ in range(warmup):
+            r.train_step(ad, lam, window, loss=False, host_targets=host)
+        r.synchronize()
+        r.stage_times_reset()
+        if dist:
+            dist.barrier()
+        r.synchronize()
+        lib, ctx = r.lib, r.ctx
+        N.check(lib.gs_event_record(ctx, 0))
+        for _ in range(steps):
+            r.train_step(ad, lam, window, loss=host is not None, host_targets=host)
+        N.check(lib.gs_event_record(ctx, 1))
+        ms = ctypes.c_float(0.0)
+        N.check(lib.gs_event_elapsed(ctx, 0, 1, ctypes.byref(ms)))
+        r.synchronize()
+        t = ms.value
+        if dist:
+            import torch
+            x = torch.tensor([t], dtype=torch.float64)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            t = float(x.item())
+        return t
+
+    # ---- batched (headline)
+    r = setup(True)
+    tuned = r.autotune()
+    clocks = Clocks(device)
+    clocks.start()
+    t_b = timed(r, args.steps, args.warmup)
+    res["clocks"] = clocks.stop()
+    stages = r.stage_times()
+    st = r.stats()
+    res["stats"] = st
+    res["stages"] = stages
+    ms_step = t_b / args.steps
+    # ---- e2e through the public API: pinned host targets in, loss out, every step
+    e2e = None
+    if not args.no_e2e:
+        host = ctypes.c_void_p()
+        N.check(r.lib.gs_host_alloc(targets.nbytes, ctypes.byref(host)))
+        ctypes.memmove(host.value, targets.ctypes.data, targets.nbytes)
+        t_e = timed(r, args.steps, 2, host=host)
+        N.check(r.lib.gs_host_free(host))
+        e2e = dict(value=world * 1000.0 / (t_e / args.steps), unit="steps/s", h2d_bytes_per_step=int(targets.nbytes),
+                   d2h_bytes_per_step=int(ctypes.sizeof(ctypes.c_float) * 0 + 64))
+    r.close()
+    # ---- plain: one view per launch per stage, same step
+    plain = None
+    if not args.no_plain:
+        rp = setup(False)
+        t_p = timed(rp, max(3, args.steps // 2), 2)
+        plain = 1000.0 / (t_p / max(3, args.steps // 2))
+        res["plain_stages"] = rp.stage_times()
+        rp.close()
+    res.update(ms_step=ms_step, plain=plain, e2e=e2e, tuned=tuned, n=n, V=V, pixels=pixels)
+    res["bytes"] = algorithmic_bytes(st, n, hmp.stride(c["degree"]), V, pixels)
+    return res
+
+
+def cpu_baseline(hmp, sample_seconds=20.0):
+    """The reference's step restated in C (FP32, OpenMP, all host threads) on a bounded
+    sample: one full step of view 0 (640x480) with all 1M Gaussians; the 8-view step time
+    is that view's time scaled by the views' pixel counts."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    O.build()
+    c = hmp.config(3)
+    cams = c["cameras"]
+    cam = cams[0]
+    rec = c["records"].copy()
+    m = np.zeros_like(rec)
+    v = np.zeros_like(rec)
+    tgt = np.zeros(cam["width"] * cam["height"] * 3, np.float32) + 0.5
+    lr = [0.025, 0.05, 0.002, 0.005, 0.001, 0.025 / 20]
+    t0 = time.perf_counter()
+    O.step(cam, rec, m, v, 3, tgt, 0.2, 1, 1, lr, near=c["near"], cap=1024)
+    dt = time.perf_counter() - t0
+    px0 = cam["width"] * cam["height"]
+    total = sum(cm["width"] * cm["height"] for cm in cams)
+    step_s = dt * total / px0
+    return dict(value=1.0 / step_s, unit="steps/s", cores=O.num_threads(), kind="port",
+                sample=f"one reference step (FP32 C restatement, cap 1024) on view 0 (640x480) with all "
+                       f"1,000,000 Gaussians took {dt:.2f} s; 8-view step time scaled by pixel count "
+                       f"({total}/{px0})")
+
+
+def roofline(res, peaks):
+    """Roofline object of the dominant HBM-bound stage (largest time among the stages
+    with an algorithmic byte count)."""
+    stages = res["stages"]
+    steps = max(1, stages["steps"])
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    best = None
+    for name, b in res["bytes"].items():
+        ms = stages["ms"].get(name, 0.0) / steps
+        if ms <= 0:
+            continue
+        gbs = b / (ms * 1e-3) / 1e9
+        if best is None or ms > best[1]:
+            best = (name, ms, gbs, b)
+    if best is None:
+        return None
+    name, ms, gbs, b = best
+    return dict(kernel=name, bound="hbm", achieved=round(gbs, 1), peak=hbm, unit="GB/s",
+                frac=round(gbs / hbm, 4), traffic=None, bytes_per_launch=int(b), ms_per_launch=round(ms, 4),
+                peak_source="measured" if "hbm_gbs" in peaks else "fallback")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    rank, local, world = env_rank()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        tdist.init_process_group("gloo", timeout=timedelta(seconds=300))
+        dist = tdist
+    hmp = importlib.import_module("home-measure-privacy_b200")
+    peaks = {}
+    pk = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+
+    if args.impl == "reference":
+        if rank == 0:
+            cb = cpu_baseline(hmp)
+            line = dict(metric=METRIC, value=cb["value"], unit="steps/s", n_gpus=args.gpus, steps=1,
+                        warmup=0, ms_per_step=1000.0 / cb["value"], higher_is_better=True, scaling="weak",
+                        vs_baseline=None, dtype="f32", data="synthetic", impl="reference",
+                        config=dict(workload=WORKLOAD, gaussians=1_000_000, views=8, sh_degree=3),
+                        cpu_baseline=cb,
+                        e2e=dict(value=cb["value"], unit="steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    res = run_b200(args, rank, local, world, dist)
+    if rank == 0:
+        ms = res["ms_step"]
+        value = world * 1000.0 / ms
+        launches = res["stages"]["launches"]
+        steps = max(1, res["stages"]["steps"])
+        line = dict(
+            metric=METRIC, value=round(value, 4), unit="steps/s", n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True, scaling="weak",
+            vs_baseline=None, dtype="f32", data="synthetic",
+            config=dict(workload=WORKLOAD, gaussians=res["n"], views=res["V"], pixels=res["pixels"], sh_degree=3,
+                        near=0.01, ssim_lambda=0.2, window="11-tap gaussian", raster_batch=res["tuned"],
+                        l2="inputs larger than L2: params+moments+grads 944 MB, pair records 384 MB per step",
+                        parallelism=f"dp{world} over views (own 8 views per GPU)"),
+            plain_steps_per_s=round(res["plain"], 4) if res["plain"] else None,
+            batched_over_plain=round(value / world / res["plain"], 4) if res["plain"] else None,
+            instances_per_step=int(res["stats"]["instances"]),
+            stages_ms_per_step={k: round(v / steps, 4) for k, v in res["stages"]["ms"].items()},
+            gpu_launches=int(sum(launches.values()) * args.steps / steps),
+            clocks=res["clocks"],
+            roofline=roofline(res, peaks),
+            e2e=res["e2e"],
+        )
+        if res.get("plain_stages"):
+            ps = res["plain_stages"]
+            line["plain_stages_ms_per_step"] = {k: round(v / max(1, ps["steps"]), 4) for k, v in ps["ms"].items()}
+        if not args.no_cpu and world == 1:
+            line["cpu_baseline"] = cpu_baseline(hmp)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

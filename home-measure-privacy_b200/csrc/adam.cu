@@ -1,0 +1,155 @@
+// Fused Adam over all parameter planes, the step's book-keeping kernels and the
+// layout conversions used by the C ABI's read-backs.
+//
+// ADAM (trainer/gpu.js:411-443): m = b1 m + (1 - b1) g, v = b2 v + (1 - b2) g^2,
+// p -= lr (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps), per-group learning rates,
+// then colour clamped to [0, 1] and the rotation quaternion renormalised.  Here it runs
+// over the plane-major SoA: each thread owns 4 consecutive Gaussians and moves float4s
+// through every plane (parameters, gradient, both moments), so each warp streams
+// 512-byte rows.  A step whose key instances overflowed their buffer (its tile lists
+// are truncated) skips the update.
+#include "internal.h"
+
+namespace gs {
+
+__global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
+    if (a.status->overflow) return;
+    const int i4 = blockIdx.x * blockDim.x + threadIdx.x;  // group of 4 Gaussians
+    const int i = i4 * 4;
+    if (i >= a.n_pad) return;
+    const int t = a.status->step_t + 1;
+    const float bc1 = 1.0f - powf(a.beta1, (float)t);
+    const float bc2 = 1.0f - powf(a.beta2, (float)t);
+    const float omb1 = 1.0f - a.beta1, omb2 = 1.0f - a.beta2;
+    const size_t np = (size_t)a.n_pad;
+    float4 q[4];
+#pragma unroll 1
+    for (int j = 0; j < a.planes; j++) {
+        const size_t off = (size_t)j * np + i;
+        float4 p = *reinterpret_cast<const float4*>(a.params + off);
+        const float4 g = *reinterpret_cast<const float4*>(a.grads + off);
+        float4 m = *reinterpret_cast<const float4*>(a.m + off);
+        float4 v = *reinterpret_cast<const float4*>(a.v + off);
+        const float lr = a.lr[j];
+        float* pp = &p.x;
+        const float* gg = &g.x;
+        float* mm = &m.x;
+        float* vv = &v.x;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            mm[e] = a.beta1 * mm[e] + omb1 * gg[e];
+            vv[e] = a.beta2 * vv[e] + omb2 * gg[e] * gg[e];
+            pp[e] -= lr * (mm[e] / bc1) / (sqrtf(vv[e] / bc2) + a.eps);
+        }
+        if (j >= 11 && j <= 13) {
+            p.x = fminf(fmaxf(p.x, 0.f), 1.f);
+            p.y = fminf(fmaxf(p.y, 0.f), 1.f);
+            p.z = fminf(fmaxf(p.z, 0.f), 1.f);
+            p.w = fminf(fmaxf(p.w, 0.f), 1.f);
+        }
+        if (j >= 6 && j <= 9) {
+            q[j - 6] = p;
+        } else {
+            *reinterpret_cast<float4*>(a.params + off) = p;
+        }
+        *reinterpret_cast<float4*>(a.m + off) = m;
+        *reinterpret_cast<float4*>(a.v + off) = v;
+    }
+    // Renormalise the rotations (planes 6..9).
+    float* qw = &q[0].x;
+    float* qx = &q[1].x;
+    float* qy = &q[2].x;
+    float* qz = &q[3].x;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const float nrm = fmaxf(sqrtf(qw[e] * qw[e] + qx[e] * qx[e] + qy[e] * qy[e] + qz[e] * qz[e]), 1e-12f);
+        qw[e] /= nrm;
+        qx[e] /= nrm;
+        qy[e] /= nrm;
+        qz[e] /= nrm;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) *reinterpret_cast<float4*>(a.params + (size_t)(6 + k) * np + i) = q[k];
+}
+
+void launch_adam(const AdamArgs& a, cudaStream_t s) {
+    const int groups = a.n_pad / 4;
+    const int threads = 256;
+    const int blocks = (groups + threads - 1) / threads;
+    if (blocks > 0) adam_kernel<<<blocks, threads, 0, s>>>(a);
+}
+
+// Loss of a step from the per-view sums: mean over views of
+// (1 - lambda) * L1 + lambda * (1 - mean SSIM).
+__device__ float step_loss(const double* acc, const ViewDesc* views, int view_first, int num_views, float lambda,
+                           int window) {
+    const int R = window == 0 ? 3 : 5;
+    double total = 0.0;
+    for (int s = 0; s < num_views; s++) {
+        const ViewDesc& vw = views[view_first + s];
+        const double n = (double)vw.width * vw.height * 3.0;
+        const int wx = vw.width - 2 * R, wy = vw.height - 2 * R;
+        const double windows = (wx > 0 && wy > 0) ? (double)wx * wy * 3.0 : 0.0;
+        const double l1 = acc[2 * (view_first + s)] / n;
+        const double ssim = windows > 0.0 ? acc[2 * (view_first + s) + 1] / windows : 1.0;
+        total += (1.0 - lambda) * l1 + (lambda > 0.f ? lambda * (1.0 - ssim) : 0.0);
+    }
+    return (float)(total / (num_views > 0 ? num_views : 1));
+}
+
+__global__ void step_end_kernel(DevStatus* st, const double* acc, const ViewDesc* views, int view_first,
+                                int num_views, float lambda, int window, int advance) {
+    const float loss = step_loss(acc, views, view_first, num_views, lambda, window);
+    st->loss = loss;
+    st->nonfinite = isfinite(loss) ? 0 : 1;
+    st->skipped = st->overflow ? 1 : 0;
+    if (advance && !st->overflow) st->step_t += 1;
+}
+
+void launch_step_end(DevStatus* status, const double* acc, const ViewDesc* views, int view_first, int num_views,
+                     float lambda, int window, int advance, cudaStream_t s) {
+    step_end_kernel<<<1, 1, 0, s>>>(status, acc, views, view_first, num_views, lambda, window, advance);
+}
+
+void launch_loss_from_acc(DevStatus* status, const double* acc, const ViewDesc* views, int view_first,
+                          int num_views, float lambda, int window, cudaStream_t s) {
+    step_end_kernel<<<1, 1, 0, s>>>(status, acc, views, view_first, num_views, lambda, window, 0);
+}
+
+// Screen gradients of one view in the reference's 16-float per-Gaussian layout
+// (trainer/gpu.js:9-10): 0-2 colour, 3 opacity logit, 4-8 u, v, conic A, B, C.
+__global__ void screen_grads16_kernel(const float4* sg8, const float* sg1, int n, float* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = sg8[(size_t)i * 2], b = sg8[(size_t)i * 2 + 1];
+    float* o = out + (size_t)i * 16;
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+    o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+    o[8] = sg1[i];
+    for (int k = 9; k < 16; k++) o[k] = 0.f;
+}
+
+void launch_screen_grads16(const float4* sg8, const float* sg1, int n, float* out16, cudaStream_t s) {
+    if (n > 0) screen_grads16_kernel<<<(n + 255) / 256, 256, 0, s>>>(sg8, sg1, n, out16);
+}
+
+// Splat records in the reference's 12-float layout (trainer/gpu.js:7).
+__global__ void splats12_kernel(const float4* geo0, const float4* geo1, const float4* rgb, const uint2* rect,
+                                const uint32_t* keys, int n, float* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 g0 = geo0[i], g1 = geo1[i], c = rgb[i];
+    float* o = out + (size_t)i * 12;
+    o[0] = g0.x; o[1] = g0.y; o[2] = g0.z; o[3] = g0.w;
+    o[4] = g1.x; o[5] = g1.y; o[6] = g1.z; o[7] = g1.w;
+    o[8] = c.x; o[9] = c.y; o[10] = c.z; o[11] = c.w;
+    (void)rect;
+    (void)keys;
+}
+
+void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb, const uint2* rect,
+                     const uint32_t* keys, int n, float* out12, cudaStream_t s) {
+    if (n > 0) splats12_kernel<<<(n + 255) / 256, 256, 0, s>>>(geo0, geo1, rgb, rect, keys, n, out12);
+}
+
+}  // namespace gs

@@ -1,0 +1,163 @@
+// Host-side launch interface of the kernels (shared by the .cu files and the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "gs_common.cuh"
+
+namespace gs {
+
+// Projection forward over view slots [0, num_views) of views[view_first + slot].
+struct ProjectArgs {
+    const float* params;     // [planes][n_pad]
+    int n, n_pad, degree;
+    const ViewDesc* views;   // device array of all views
+    int view_first, num_views;
+    int pair_slot_first;     // pair slot of view_first (0 in the batched path)
+    float near_plane, dilation;
+    int rect_mode;
+    float4* geo0;            // [num_views * n_pad]
+    float4* geo1;
+    float4* rgb;
+    uint2* rect;
+    uint32_t* keys;          // depth key, GS_KEY_SENTINEL when the pair covers no tile
+    unsigned int* visible;   // optional counter of pairs with >= 1 tile
+};
+void launch_project_fwd(const ProjectArgs& a, cudaStream_t s);
+
+// Projection backward: screen gradients of the view slots -> parameter gradients.
+struct ProjectBwdArgs {
+    const float* params;
+    int n, n_pad, degree;
+    const ViewDesc* views;
+    int view_first, num_views;
+    int pair_slot_first;     // pair slot of view_first (0 in the batched path)
+    float dilation;
+    const float4* sg8;       // [pairs][2] float4
+    const float* sg1;        // [pairs]
+    float* grads;            // [planes][n_pad]
+    int accumulate;          // add to grads instead of overwriting them
+};
+void launch_project_bwd(const ProjectBwdArgs& a, cudaStream_t s);
+
+// ---- sorting ----------------------------------------------------------------------
+// LSD radix sort of u32 keys with u32 values over a segment [seg->base, +seg->count)
+// (device-resident offsets).  Ping-pongs between (keys, vals) and (keys_alt, vals_alt);
+// with an even number of passes the result is back in (keys, vals).
+struct RadixSortArgs {
+    uint32_t* keys;
+    uint32_t* vals;
+    uint32_t* keys_alt;
+    uint32_t* vals_alt;
+    int iota;                // 1: values start as the absolute element index
+    const SegInfo* seg;
+    int begin_bit, end_bit;  // bits to sort
+    uint32_t* hist;          // 256 * max_parts
+    uint32_t* totals;        // 256
+    int max_parts;
+};
+int radix_sort_passes(int begin_bit, int end_bit);
+void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms);
+int radix_tile_items();
+
+// Emission of key instances from the depth-sorted pairs.
+struct EmitArgs {
+    const uint32_t* sorted_pairs;   // pairs in depth order (first `visible` are real)
+    const SegInfo* pair_seg;        // pair segment: base into sorted_pairs, count
+    const unsigned int* visible;    // number of visible pairs in the segment
+    const uint2* rect;
+    const ViewDesc* views;
+    int view_first, n_pad;
+    int pair_slot_first;            // slot of the first pair of this segment
+    uint32_t* block_sums;           // scratch, >= chunks
+    SegInfo* inst_seg;              // out: instance segment (base, count)
+    const SegInfo* prev_seg;        // previous instance segment (plain path) or nullptr
+    uint32_t* inst_keys;            // global tile id
+    uint32_t* inst_vals;            // pair index
+    unsigned long long capacity;
+    DevStatus* status;
+    int max_chunks;
+};
+void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms);
+int emit_chunk_items();
+
+// Tile ranges from tile-sorted instances.
+void launch_ranges(const uint32_t* sorted_tiles, const SegInfo* seg, uint2* ranges,
+                   cudaStream_t s, int num_sms);
+
+// ---- rasterisation ---------------------------------------------------------------------
+struct RasterArgs {
+    const ViewDesc* views;
+    int view_first, num_views;
+    int tile_first, num_tiles;      // global tiles [tile_first, tile_first + num_tiles)
+    int pixel_first;                // first pixel of view_first
+    const uint2* ranges;
+    const uint32_t* inst_pair;
+    const float4* geo0;
+    const float4* geo1;
+    const float4* rgb;
+    int pair_slot_first;            // pair index = pair - pair_slot_first * n_pad ... (unused)
+    float alpha_max, alpha_min, t_min;
+    // forward outputs / backward inputs (indexed by global pixel)
+    float* image;
+    float* t_final;
+    uint32_t* last;
+    const float* dl;                // backward: dL/dpixel
+    float4* sg8;                    // backward outputs
+    float* sg1;
+    unsigned int* work_counter;     // persistent queue head (nullptr = one CTA per tile)
+    const uint32_t* tile_order;     // optional permutation of the tiles (heavy first)
+};
+void launch_raster_fwd(const RasterArgs& a, int batch, int persistent_ctas, cudaStream_t s);
+void launch_raster_bwd(const RasterArgs& a, int batch, int persistent_ctas, cudaStream_t s);
+int raster_max_ctas_per_sm(int batch, bool backward);
+
+// Tiles ordered by descending list length (for the persistent queue).
+void launch_tile_order(const uint2* ranges, int tile_first, int num_tiles, uint32_t* order,
+                       uint32_t* scratch, cudaStream_t s);
+
+// ---- loss ------------------------------------------------------------------------------
+struct LossArgs {
+    const ViewDesc* views;
+    int view_first, num_views;
+    int block_first, num_blocks;    // loss blocks of these views
+    const float* image;
+    const uint8_t* target_u8;       // one of the two
+    const float* target_f32;
+    float* dl;
+    float lambda;
+    int window;                     // 0 = 7x7 box, 1 = 11-tap Gaussian
+    double* acc;                    // per view: [L1 sum, SSIM sum]
+};
+void launch_loss(const LossArgs& a, cudaStream_t s);
+cudaError_t loss_prepare();
+int loss_block_w();
+int loss_block_h();
+
+// ---- optimiser -------------------------------------------------------------------------
+struct AdamArgs {
+    float* params;
+    const float* grads;
+    float* m;
+    float* v;
+    int n, n_pad, planes;
+    float lr[GS_MAX_PLANES];
+    float beta1, beta2, eps;
+    DevStatus* status;
+};
+void launch_adam(const AdamArgs& a, cudaStream_t s);
+
+// Finishes a step: loss from the accumulators, skip flag, Adam step counter.
+void launch_step_end(DevStatus* status, const double* acc, const ViewDesc* views,
+                     int view_first, int num_views, float lambda, int window, int advance,
+                     cudaStream_t s);
+void launch_loss_from_acc(DevStatus* status, const double* acc, const ViewDesc* views,
+                          int view_first, int num_views, float lambda, int window,
+                          cudaStream_t s);
+
+// ---- layout conversion -----------------------------------------------------------------
+void launch_screen_grads16(const float4* sg8, const float* sg1, int n, float* out16,
+                           cudaStream_t s);
+void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb, const uint2* rect,
+                     const uint32_t* keys, int n, float* out12, cudaStream_t s);
+
+}  // namespace gs

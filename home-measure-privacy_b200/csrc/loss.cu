@@ -1,0 +1,274 @@
+// Fused photometric loss: (1 - lambda) * L1 + lambda * (1 - SSIM) and dLoss/dPixel in
+// one pass over image and target, for every view of a step.
+//
+// The reference splits this into SSIM_COEF (trainer/gpu.js:336-372: per window centre
+// and channel, SSIM and its partials a, b, d by the window mean, mean of squares and
+// mean of products) and LOSS_GRAD (:374-409: each pixel sums a + 2 x b + y d over the
+// windows that cover it, 49 taps each, reading the coefficients back from HBM).  Here
+// one CTA owns a 32 x 16 block of output pixels and keeps everything in shared memory:
+// it loads image and target with a 2R halo, forms the five window moments with a
+// separable (horizontal then vertical) filter, turns them into the coefficients
+// a, b, d at every window centre that can reach the block, and filters those
+// coefficients back (again separably) to get each pixel's SSIM gradient.  Windows are
+// the reference's: centres whose whole window lies inside the image (7x7 box, R = 3),
+// or the 11-tap Gaussian (sigma 1.5, R = 5) with the same rule.  The kernel also sums
+// |x - y| and the SSIM of the windows centred in its block for the loss value.
+#include "internal.h"
+
+namespace gs {
+
+constexpr int LB_W = 32;
+constexpr int LB_H = 16;
+constexpr int LB_THREADS = 256;
+
+struct LossWeights {
+    float w[11];
+};
+
+template <int R>
+struct LossDims {
+    static constexpr int RW = LB_W + 4 * R;   // region with halo 2R
+    static constexpr int RH = LB_H + 4 * R;
+    static constexpr int HW = LB_W + 2 * R;   // window centres reaching the block
+    static constexpr int CH = LB_H + 2 * R;
+    static constexpr int X_OFF = 0;
+    static constexpr int Y_OFF = RH * RW;
+    static constexpr int HM_OFF = 2 * RH * RW;               // 5 moments, RH x HW
+    static constexpr int C_OFF = HM_OFF + 5 * RH * HW;       // 3 coefficients, CH x HW
+    static constexpr int HC_OFF = HM_OFF;                    // 3 filtered coefs, CH x LB_W (aliases moments)
+    static constexpr int FLOATS = C_OFF + 3 * CH * HW;
+};
+
+template <typename TT>
+__device__ __forceinline__ float load_target(const TT* t, size_t idx);
+template <>
+__device__ __forceinline__ float load_target<uint8_t>(const uint8_t* t, size_t idx) {
+    return (float)t[idx] / 255.0f;
+}
+template <>
+__device__ __forceinline__ float load_target<float>(const float* t, size_t idx) {
+    return t[idx];
+}
+
+template <int R, typename TT>
+__global__ void __launch_bounds__(LB_THREADS) loss_kernel(LossArgs a, const TT* __restrict__ target,
+                                                          LossWeights wts) {
+    using D = LossDims<R>;
+    extern __shared__ float sm[];
+    __shared__ float s_red[2][LB_THREADS / 32];
+    const int blk = a.block_first + blockIdx.x;
+    int vi = a.view_first;
+    const int vend = a.view_first + a.num_views;
+    while (vi + 1 < vend && a.views[vi + 1].loss_block_offset <= blk) vi++;
+    const ViewDesc& vw = a.views[vi];
+    const int lb = blk - vw.loss_block_offset;
+    const int W = vw.width, H = vw.height;
+    const int bx0 = (lb % vw.loss_blocks_x) * LB_W, by0 = (lb / vw.loss_blocks_x) * LB_H;
+    const size_t poff = (size_t)vw.pixel_offset;
+    const float n = (float)((long long)W * H * 3);
+    const int winx = W - 2 * R, winy = H - 2 * R;
+    const float windows = (winx > 0 && winy > 0) ? (float)winx * (float)winy * 3.0f : 0.0f;
+    const bool use_ssim = a.lambda > 0.0f && windows > 0.0f;
+    float* X = sm + D::X_OFF;
+    float* Y = sm + D::Y_OFF;
+    float* HM = sm + D::HM_OFF;
+    float* CF = sm + D::C_OFF;
+    float* HC = sm + D::HC_OFF;
+    float l1 = 0.f, ssim_sum = 0.f;
+    const float C1 = 1e-4f, C2 = 9e-4f;
+    for (int c = 0; c < 3; c++) {
+        if (use_ssim) {
+            for (int idx = threadIdx.x; idx < D::RH * D::RW; idx += LB_THREADS) {
+                const int ry = idx / D::RW, rx = idx % D::RW;
+                const int gx = bx0 - 2 * R + rx, gy = by0 - 2 * R + ry;
+                float xv = 0.f, yv = 0.f;
+                if (gx >= 0 && gy >= 0 && gx < W && gy < H) {
+                    const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
+                    xv = a.image[q];
+                    yv = load_target<TT>(target, q);
+                }
+                X[idx] = xv;
+                Y[idx] = yv;
+            }
+            __syncthreads();
+            // Horizontal moments at every region row and centre column.
+            for (int idx = threadIdx.x; idx < D::RH * D::HW; idx += LB_THREADS) {
+                const int r = idx / D::HW, hc = idx % D::HW;
+                float mx = 0.f, my = 0.f, sxx = 0.f, syy = 0.f, sxy = 0.f;
+#pragma unroll
+                for (int k = 0; k <= 2 * R; k++) {
+                    const float w = wts.w[k];
+                    const float xv = X[r * D::RW + hc + k], yv = Y[r * D::RW + hc + k];
+                    mx += w * xv;
+                    my += w * yv;
+                    sxx += w * xv * xv;
+                    syy += w * yv * yv;
+                    sxy += w * xv * yv;
+                }
+                HM[0 * D::RH * D::HW + idx] = mx;
+                HM[1 * D::RH * D::HW + idx] = my;
+                HM[2 * D::RH * D::HW + idx] = sxx;
+                HM[3 * D::RH * D::HW + idx] = syy;
+                HM[4 * D::RH * D::HW + idx] = sxy;
+            }
+            __syncthreads();
+            // Vertical pass -> SSIM coefficients at window centres.
+            for (int idx = threadIdx.x; idx < D::CH * D::HW; idx += LB_THREADS) {
+                const int hr = idx / D::HW, hc = idx % D::HW;
+                const int gx = bx0 - R + hc, gy = by0 - R + hr;
+                float ca = 0.f, cb = 0.f, cd = 0.f;
+                if (gx >= R && gy >= R && gx < W - R && gy < H - R) {
+                    float m[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int k = 0; k <= 2 * R; k++) {
+                        const float w = wts.w[k];
+                        const int row = (hr + k) * D::HW + hc;
+#pragma unroll
+                        for (int q = 0; q < 5; q++) m[q] += w * HM[q * D::RH * D::HW + row];
+                    }
+                    const float mx = m[0], my = m[1], sxx = m[2], syy = m[3], sxy = m[4];
+                    const float a1 = 2.0f * mx * my + C1;
+                    const float a2 = 2.0f * (sxy - mx * my) + C2;
+                    const float b1 = mx * mx + my * my + C1;
+                    const float b2 = (sxx - mx * mx) + (syy - my * my) + C2;
+                    const float ssim = a1 * a2 / (b1 * b2);
+                    ca = ssim * (2.0f * my / a1 - 2.0f * my / a2 - 2.0f * mx / b1 + 2.0f * mx / b2);
+                    cb = -ssim / b2;
+                    cd = 2.0f * ssim / a2;
+                    if (gx >= bx0 && gx < bx0 + LB_W && gy >= by0 && gy < by0 + LB_H) ssim_sum += ssim;
+                }
+                CF[0 * D::CH * D::HW + idx] = ca;
+                CF[1 * D::CH * D::HW + idx] = cb;
+                CF[2 * D::CH * D::HW + idx] = cd;
+            }
+            __syncthreads();
+            // Filter the coefficients back: horizontal ...
+            for (int idx = threadIdx.x; idx < D::CH * LB_W; idx += LB_THREADS) {
+                const int hr = idx / LB_W, oc = idx % LB_W;
+                float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                for (int k = 0; k <= 2 * R; k++) {
+                    const float w = wts.w[k];
+                    const int q = hr * D::HW + oc + k;
+                    s0 += w * CF[0 * D::CH * D::HW + q];
+                    s1 += w * CF[1 * D::CH * D::HW + q];
+                    s2 += w * CF[2 * D::CH * D::HW + q];
+                }
+                HC[0 * D::CH * LB_W + idx] = s0;
+                HC[1 * D::CH * LB_W + idx] = s1;
+                HC[2 * D::CH * LB_W + idx] = s2;
+            }
+            __syncthreads();
+        }
+        // ... and vertical, then the per-pixel gradient.
+        for (int idx = threadIdx.x; idx < LB_W * LB_H; idx += LB_THREADS) {
+            const int oy = idx / LB_W, ox = idx % LB_W;
+            const int gx = bx0 + ox, gy = by0 + oy;
+            if (gx >= W || gy >= H) continue;
+            const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
+            float xv, yv;
+            if (use_ssim) {
+                xv = X[(oy + 2 * R) * D::RW + ox + 2 * R];
+                yv = Y[(oy + 2 * R) * D::RW + ox + 2 * R];
+            } else {
+                xv = a.image[q];
+                yv = load_target<TT>(target, q);
+            }
+            const float diff = xv - yv;
+            float g = (1.0f - a.lambda) * (float)((diff > 0.f) - (diff < 0.f)) / n;
+            l1 += fabsf(diff);
+            if (use_ssim) {
+                float sa = 0.f, sb = 0.f, sd = 0.f;
+#pragma unroll
+                for (int k = 0; k <= 2 * R; k++) {
+                    const float w = wts.w[k];
+                    const int r = (oy + k) * LB_W + ox;
+                    sa += w * HC[0 * D::CH * LB_W + r];
+                    sb += w * HC[1 * D::CH * LB_W + r];
+                    sd += w * HC[2 * D::CH * LB_W + r];
+                }
+                g -= a.lambda * ((sa + 2.0f * xv * sb + yv * sd) / windows);
+            }
+            a.dl[q] = g;
+        }
+        __syncthreads();
+    }
+    // Block sums of |x - y| and SSIM -> per-view accumulators.
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l1 += __shfl_xor_sync(0xffffffffu, l1, o);
+        ssim_sum += __shfl_xor_sync(0xffffffffu, ssim_sum, o);
+    }
+    if (lane == 0) {
+        s_red[0][warp] = l1;
+        s_red[1][warp] = ssim_sum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int w = 0; w < LB_THREADS / 32; w++) {
+            t0 += s_red[0][w];
+            t1 += s_red[1][w];
+        }
+        atomicAdd(a.acc + 2 * vi + 0, t0);
+        atomicAdd(a.acc + 2 * vi + 1, t1);
+    }
+}
+
+static LossWeights make_weights(int window) {
+    LossWeights w{};
+    if (window == 0) {
+        for (int k = 0; k < 7; k++) w.w[k] = (float)(1.0 / 7.0);
+    } else {
+        double g[11], s = 0.0;
+        for (int k = 0; k < 11; k++) {
+            const double d = k - 5;
+            g[k] = exp(-d * d / (2.0 * 1.5 * 1.5));
+            s += g[k];
+        }
+        for (int k = 0; k < 11; k++) w.w[k] = (float)(g[k] / s);
+    }
+    return w;
+}
+
+template <int R, typename TT>
+static void loss_launch(const LossArgs& a, const TT* target, const LossWeights& w, cudaStream_t s) {
+    const size_t smem = LossDims<R>::FLOATS * sizeof(float);
+    loss_kernel<R, TT><<<a.num_blocks, LB_THREADS, smem, s>>>(a, target, w);
+}
+
+void launch_loss(const LossArgs& a, cudaStream_t s) {
+    if (a.num_blocks <= 0) return;
+    const LossWeights w = make_weights(a.window);
+    if (a.window == 0) {
+        if (a.target_u8) loss_launch<3, uint8_t>(a, a.target_u8, w, s);
+        else loss_launch<3, float>(a, a.target_f32, w, s);
+    } else {
+        if (a.target_u8) loss_launch<5, uint8_t>(a, a.target_u8, w, s);
+        else loss_launch<5, float>(a, a.target_f32, w, s);
+    }
+}
+
+// Raises the dynamic shared-memory limit of the loss kernels on the current device.
+cudaError_t loss_prepare() {
+    cudaError_t e = cudaSuccess, r;
+    r = cudaFuncSetAttribute(loss_kernel<3, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(LossDims<3>::FLOATS * sizeof(float)));
+    if (r != cudaSuccess) e = r;
+    r = cudaFuncSetAttribute(loss_kernel<3, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(LossDims<3>::FLOATS * sizeof(float)));
+    if (r != cudaSuccess) e = r;
+    r = cudaFuncSetAttribute(loss_kernel<5, uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(LossDims<5>::FLOATS * sizeof(float)));
+    if (r != cudaSuccess) e = r;
+    r = cudaFuncSetAttribute(loss_kernel<5, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(LossDims<5>::FLOATS * sizeof(float)));
+    if (r != cudaSuccess) e = r;
+    return e;
+}
+
+int loss_block_w() { return LB_W; }
+int loss_block_h() { return LB_H; }
+
+}  // namespace gs

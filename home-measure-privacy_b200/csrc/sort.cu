@@ -1,0 +1,391 @@
+// Tile binning on the device: depth sort of the (view, Gaussian) pairs, emission of one
+// key instance per (pair, covered tile), stable sort of the instances by tile id and
+// the tile-range kernel.
+//
+// The result is the order of the 64-bit key (tile id << 32 | float bits of depth) with
+// ties broken by Gaussian index, which is what the reference's BIN + SORT produce per
+// tile (trainer/gpu.js:616-685: per-tile bitonic sort on depth, stable on splat index,
+// :673) and what tileLists does on the CPU (trainer/gpu.js:450-481: a stable global
+// depth sort, then a scatter in that order).  It is built the second way: the pairs
+// (about 5x fewer than the instances) are radix-sorted on the 31 significant bits of
+// their depth, the instances are emitted in that order, and a stable radix sort on the
+// tile id (16 bits for up to 65,536 tiles: two passes) groups them by tile without
+// disturbing the depth order.  There is no per-tile cap (the reference drops entries
+// beyond 1,024 per tile, :614, :640).
+#include "internal.h"
+
+namespace gs {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // keys per partition
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr unsigned FULL = 0xffffffffu;
+
+int radix_tile_items() { return RS_TILE; }
+
+static void pass_plan(int begin_bit, int end_bit, int& passes, int& step) {
+    const int bits = end_bit - begin_bit;
+    passes = (bits + 7) / 8;
+    if (passes < 1) passes = 1;
+    if (passes & 1) passes += 1;  // even: the result lands back in the input buffers
+    step = (bits + passes - 1) / passes;
+    if (step < 1) step = 1;
+}
+
+int radix_sort_passes(int begin_bit, int end_bit) {
+    int p, s;
+    pass_plan(begin_bit, end_bit, p, s);
+    return p;
+}
+
+// Exclusive scan over a block of NT threads (NT a multiple of 32, <= 1024).
+template <int NT>
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_tmp, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_tmp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t t = lane < NW ? s_tmp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < NW) s_tmp[lane] = t;
+    }
+    __syncthreads();
+    const uint32_t prefix = warp > 0 ? s_tmp[warp - 1] : 0u;
+    total = s_tmp[NW - 1];
+    __syncthreads();
+    return prefix + x - v;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) radix_upsweep(const uint32_t* __restrict__ keys,
+                                                            const SegInfo* seg, int shift, int bits,
+                                                            uint32_t* __restrict__ hist) {
+    __shared__ uint32_t wh[RS_WARPS][256];
+    const uint32_t base = seg->base, n = seg->count;
+    const uint32_t P = (n + RS_TILE - 1) / RS_TILE;
+    const int warp = threadIdx.x >> 5;
+    const uint32_t mask = (1u << bits) - 1u;
+    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
+        for (int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS) (&wh[0][0])[d] = 0u;
+        __syncthreads();
+        const uint32_t start = p * RS_TILE;
+#pragma unroll 4
+        for (int j = 0; j < RS_ITEMS; j++) {
+            const uint32_t idx = start + j * RS_THREADS + threadIdx.x;
+            if (idx < n) {
+                const uint32_t k = __ldg(keys + base + idx);
+                atomicAdd(&wh[warp][(k >> shift) & mask], 1u);
+            }
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < 256; d += RS_THREADS) {
+            uint32_t s = 0;
+#pragma unroll
+            for (int w = 0; w < RS_WARPS; w++) s += wh[w][d];
+            hist[(size_t)d * P + p] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// One block per digit: exclusive scan of that digit's counts over the partitions.
+__global__ void __launch_bounds__(1024) radix_scan(const SegInfo* seg, uint32_t* __restrict__ hist,
+                                                   uint32_t* __restrict__ totals) {
+    __shared__ uint32_t s_tmp[32];
+    const uint32_t n = seg->count;
+    const uint32_t P = (n + RS_TILE - 1) / RS_TILE;
+    uint32_t* h = hist + (size_t)blockIdx.x * P;
+    uint32_t carry = 0;
+    for (uint32_t b = 0; b < P; b += 1024) {
+        const uint32_t idx = b + threadIdx.x;
+        const uint32_t v = idx < P ? h[idx] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan<1024>(v, s_tmp, tot);
+        if (idx < P) h[idx] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) radix_downsweep(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift,
+    int bits, const uint32_t* __restrict__ hist, const uint32_t* __restrict__ totals) {
+    __shared__ uint32_t s_keys[RS_TILE];
+    __shared__ uint32_t s_vals[RS_TILE];
+    __shared__ uint32_t s_warp[RS_WARPS][256];
+    __shared__ uint32_t s_digit_start[256];
+    __shared__ uint32_t s_global[256];
+    __shared__ uint32_t s_total_excl[256];
+    __shared__ uint32_t s_tmp[32];
+    const uint32_t base = seg->base, n = seg->count;
+    const uint32_t P = (n + RS_TILE - 1) / RS_TILE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t mask = (1u << bits) - 1u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    if (blockIdx.x >= P) return;
+    {
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan<RS_THREADS>(totals[threadIdx.x], s_tmp, tot);
+        s_total_excl[threadIdx.x] = ex;
+    }
+    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
+        for (int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS) (&s_warp[0][0])[d] = 0u;
+        __syncthreads();
+        const uint32_t part_start = p * RS_TILE;
+        const uint32_t warp_start = part_start + warp * (RS_ITEMS * 32);
+        uint32_t k[RS_ITEMS], v[RS_ITEMS], rank[RS_ITEMS];
+#pragma unroll
+        for (int j = 0; j < RS_ITEMS; j++) {
+            const uint32_t idx = warp_start + j * 32 + lane;
+            const bool valid = idx < n;
+            k[j] = valid ? __ldg(keys_in + base + idx) : 0xffffffffu;
+            v[j] = valid ? (vals_in ? __ldg(vals_in + base + idx) : base + idx) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < RS_ITEMS; j++) {
+            const uint32_t idx = warp_start + j * 32 + lane;
+            const bool valid = idx < n;
+            const uint32_t d = (k[j] >> shift) & mask;
+            uint32_t peers = __ballot_sync(FULL, valid);
+            for (int b = 0; b < bits; b++) {
+                const bool bit = (d >> b) & 1u;
+                const uint32_t bal = __ballot_sync(FULL, bit);
+                peers &= bit ? bal : ~bal;
+            }
+            uint32_t prev = 0;
+            if (valid) {
+                prev = s_warp[warp][d];
+                rank[j] = prev + __popc(peers & lt_mask);
+            }
+            __syncwarp();
+            if (valid && (peers & lt_mask) == 0u) s_warp[warp][d] = prev + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        {
+            const int d = threadIdx.x;  // RS_THREADS == 256 digits
+            uint32_t s = 0;
+#pragma unroll
+            for (int w = 0; w < RS_WARPS; w++) {
+                const uint32_t c = s_warp[w][d];
+                s_warp[w][d] = s;
+                s += c;
+            }
+            uint32_t tot;
+            const uint32_t ex = block_excl_scan<RS_THREADS>(s, s_tmp, tot);
+            s_digit_start[d] = ex;
+            s_global[d] = s_total_excl[d] + hist[(size_t)d * P + p];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < RS_ITEMS; j++) {
+            const uint32_t idx = warp_start + j * 32 + lane;
+            if (idx < n) {
+                const uint32_t d = (k[j] >> shift) & mask;
+                const uint32_t pos = s_digit_start[d] + s_warp[warp][d] + rank[j];
+                s_keys[pos] = k[j];
+                s_vals[pos] = v[j];
+            }
+        }
+        __syncthreads();
+        const uint32_t cnt = min((uint32_t)RS_TILE, n - part_start);
+        for (uint32_t i = threadIdx.x; i < cnt; i += RS_THREADS) {
+            const uint32_t key = s_keys[i];
+            const uint32_t d = (key >> shift) & mask;
+            const uint32_t out = base + s_global[d] + (i - s_digit_start[d]);
+            keys_out[out] = key;
+            vals_out[out] = s_vals[i];
+        }
+        __syncthreads();
+    }
+}
+
+void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
+    int passes, step;
+    pass_plan(a.begin_bit, a.end_bit, passes, step);
+    const int grid_up = num_sms * 4;
+    const int grid_down = num_sms * 3;
+    uint32_t* kb[2] = {a.keys, a.keys_alt};
+    uint32_t* vb[2] = {a.vals, a.vals_alt};
+    for (int p = 0; p < passes; p++) {
+        const int in = p & 1, out = in ^ 1;
+        const int shift = a.begin_bit + p * step;
+        int bits = a.end_bit - shift;
+        if (bits > step) bits = step;
+        if (bits < 1) bits = 1;
+        radix_upsweep<<<grid_up, RS_THREADS, 0, s>>>(kb[in], a.seg, shift, bits, a.hist);
+        radix_scan<<<256, 1024, 0, s>>>(a.seg, a.hist, a.totals);
+        radix_downsweep<<<grid_down, RS_THREADS, 0, s>>>(kb[in], (p == 0 && a.iota) ? nullptr : vb[in],
+                                                          kb[out], vb[out], a.seg, shift, bits, a.hist,
+                                                          a.totals);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Key-instance emission.  Chunks of EM_CHUNK depth-sorted pairs: (1) per-chunk sums of
+// the pairs' tile counts, (2) one block scans the chunk sums and fixes the segment's
+// size (clamped to the capacity, with the overflow flag set), (3) each chunk rescans
+// its counts and expands them: consecutive threads write consecutive instances (a
+// binary search over the chunk's offsets finds the pair), so the writes coalesce even
+// when one splat covers hundreds of tiles.
+// ---------------------------------------------------------------------------------
+constexpr int EM_THREADS = 256;
+constexpr int EM_ITEMS = 8;
+constexpr int EM_CHUNK = EM_THREADS * EM_ITEMS;
+
+int emit_chunk_items() { return EM_CHUNK; }
+
+__device__ __forceinline__ uint32_t rect_count(uint2 r) {
+    const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu, y1 = r.y >> 16;
+    return (x1 > x0 && y1 > y0) ? (x1 - x0) * (y1 - y0) : 0u;
+}
+
+__global__ void __launch_bounds__(EM_THREADS) emit_reduce(EmitArgs a) {
+    __shared__ uint32_t s_tmp[32];
+    const uint32_t M = *a.visible;
+    const uint32_t base = a.pair_seg->base;
+    const uint32_t chunks = (M + EM_CHUNK - 1) / EM_CHUNK;
+    for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        uint32_t sum = 0;
+#pragma unroll
+        for (int j = 0; j < EM_ITEMS; j++) {
+            const uint32_t sidx = c * EM_CHUNK + j * EM_THREADS + threadIdx.x;
+            if (sidx < M) sum += rect_count(a.rect[__ldg(a.sorted_pairs + base + sidx)]);
+        }
+        uint32_t tot;
+        block_excl_scan<EM_THREADS>(sum, s_tmp, tot);
+        if (threadIdx.x == 0) a.block_sums[c] = tot;
+    }
+}
+
+__global__ void __launch_bounds__(1024) emit_scan(EmitArgs a) {
+    __shared__ uint32_t s_tmp[32];
+    const uint32_t M = *a.visible;
+    const uint32_t chunks = (M + EM_CHUNK - 1) / EM_CHUNK;
+    unsigned long long carry = 0;
+    for (uint32_t b = 0; b < chunks; b += 1024) {
+        const uint32_t idx = b + threadIdx.x;
+        const uint32_t v = idx < chunks ? a.block_sums[idx] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan<1024>(v, s_tmp, tot);
+        if (idx < chunks) a.block_sums[idx] = (uint32_t)(carry + ex);
+        carry += tot;
+    }
+    if (threadIdx.x == 0) {
+        const unsigned long long seg_base =
+            a.prev_seg ? (unsigned long long)a.prev_seg->base + a.prev_seg->count : 0ull;
+        const unsigned long long need = seg_base + carry;
+        unsigned long long count = carry;
+        if (need > a.capacity) {
+            a.status->overflow = 1u;
+            count = seg_base < a.capacity ? a.capacity - seg_base : 0ull;
+        }
+        if (need > a.status->instances_needed) a.status->instances_needed = need;
+        a.inst_seg->base = (uint32_t)(seg_base < a.capacity ? seg_base : a.capacity);
+        a.inst_seg->count = (uint32_t)count;
+    }
+}
+
+__global__ void __launch_bounds__(EM_THREADS) emit_write(EmitArgs a) {
+    __shared__ uint32_t s_off[EM_CHUNK + 1];
+    __shared__ uint32_t s_pair[EM_CHUNK];
+    __shared__ uint2 s_rect[EM_CHUNK];
+    __shared__ uint32_t s_tmp[32];
+    const uint32_t M = *a.visible;
+    const uint32_t base = a.pair_seg->base;
+    const uint32_t chunks = (M + EM_CHUNK - 1) / EM_CHUNK;
+    const uint32_t inst_base = a.inst_seg->base;
+    const unsigned long long limit = a.inst_seg->count;  // instances of this segment that fit
+    for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+        const uint32_t first = c * EM_CHUNK;
+        const uint32_t items = min((uint32_t)EM_CHUNK, M - first);
+        for (uint32_t j = threadIdx.x; j < EM_CHUNK; j += EM_THREADS) {
+            uint32_t pair = 0;
+            uint2 r = make_uint2(0u, 0u);
+            if (j < items) {
+                pair = __ldg(a.sorted_pairs + base + first + j);
+                r = a.rect[pair];
+            }
+            s_pair[j] = pair;
+            s_rect[j] = r;
+        }
+        __syncthreads();
+        uint32_t cnt[EM_ITEMS];
+        uint32_t local = 0;
+#pragma unroll
+        for (int j = 0; j < EM_ITEMS; j++) {
+            cnt[j] = rect_count(s_rect[threadIdx.x * EM_ITEMS + j]);
+            local += cnt[j];
+        }
+        uint32_t tot;
+        uint32_t run = block_excl_scan<EM_THREADS>(local, s_tmp, tot) + a.block_sums[c];
+#pragma unroll
+        for (int j = 0; j < EM_ITEMS; j++) {
+            s_off[threadIdx.x * EM_ITEMS + j] = run;
+            run += cnt[j];
+        }
+        if (threadIdx.x == 0) s_off[EM_CHUNK] = a.block_sums[c] + tot;
+        __syncthreads();
+        const uint32_t o_begin = s_off[0], o_end = s_off[EM_CHUNK];
+        for (uint32_t o = o_begin + threadIdx.x; o < o_end; o += EM_THREADS) {
+            if ((unsigned long long)o >= limit) break;
+            // Largest idx with s_off[idx] <= o among [0, items).
+            uint32_t lo = 0, hi = items - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (s_off[mid] <= o) lo = mid;
+                else hi = mid - 1;
+            }
+            const uint32_t pair = s_pair[lo];
+            const uint2 r = s_rect[lo];
+            const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu;
+            const uint32_t w = x1 - x0;
+            const uint32_t t = o - s_off[lo];
+            const uint32_t tx = x0 + t % w, ty = y0 + t / w;
+            const ViewDesc& vw = a.views[a.view_first + pair / (uint32_t)a.n_pad];
+            a.inst_keys[inst_base + o] = (uint32_t)vw.tile_offset + ty * (uint32_t)vw.tiles_x + tx;
+            a.inst_vals[inst_base + o] = pair;
+        }
+        __syncthreads();
+    }
+}
+
+void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms) {
+    int grid = num_sms * 4;
+    if (grid > a.max_chunks) grid = a.max_chunks > 0 ? a.max_chunks : 1;
+    emit_reduce<<<grid, EM_THREADS, 0, s>>>(a);
+    emit_scan<<<1, 1024, 0, s>>>(a);
+    emit_write<<<grid, EM_THREADS, 0, s>>>(a);
+}
+
+// ---------------------------------------------------------------------------------
+// Tile ranges: each tile's [first, last + 1) in the tile-sorted instances (absolute
+// indices).  Tiles without instances keep the zeroed (0, 0).
+// ---------------------------------------------------------------------------------
+__global__ void ranges_kernel(const uint32_t* __restrict__ tiles, const SegInfo* seg, uint2* ranges) {
+    const uint32_t base = seg->base, n = seg->count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t t = tiles[base + i];
+        if (i == 0 || tiles[base + i - 1] != t) ranges[t].x = base + i;
+        if (i == n - 1 || tiles[base + i + 1] != t) ranges[t].y = base + i + 1;
+    }
+}
+
+void launch_ranges(const uint32_t* sorted_tiles, const SegInfo* seg, uint2* ranges, cudaStream_t s,
+                   int num_sms) {
+    ranges_kernel<<<num_sms * 8, 256, 0, s>>>(sorted_tiles, seg, ranges);
+}
+
+}  // namespace gs

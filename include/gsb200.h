@@ -1,0 +1,292 @@
+/*
+ * gsb200.h -- C ABI of the B200-native Gaussian-splat training step.
+ *
+ * This is the boundary a host binding (the Node-API addon behind the trainer's
+ * JavaScript module, or the Python ctypes mirror in this repository) calls.  Every
+ * entry point takes plain pointers and sizes, copies caller-owned host memory before
+ * it returns (unless stated otherwise), and returns an int status: GS_OK (0) or a
+ * negative GS_ERR_* code, with a message from gs_last_error().
+ *
+ * The reference is the WebGPU trainer of barakatiass-alt/home-measure-privacy.  Each
+ * entry point names the function of trainer/gpu.js (or trainer/colmap.js) it stands
+ * in for.  Device memory is owned by the context and grows on demand, like the
+ * reference's pooled scratch buffers (trainer/gpu.js:764-772).  A context is bound to
+ * one CUDA device and one stream and is not re-entrant: callers serialise calls on a
+ * context (the reference's JS event loop does the same).
+ */
+#ifndef GSB200_H
+#define GSB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSB200_VERSION 1
+
+#if defined(__GNUC__)
+#define GS_API __attribute__((visibility("default")))
+#else
+#define GS_API
+#endif
+
+/* ---- status codes ------------------------------------------------------------- */
+#define GS_OK               0
+#define GS_ERR_INVALID_ARG -1   /* bad pointer, size or option                     */
+#define GS_ERR_CUDA        -2   /* a CUDA runtime call failed                      */
+#define GS_ERR_CAPACITY    -3   /* an instance buffer overflowed; step was skipped */
+#define GS_ERR_NO_DEVICE   -4   /* no CUDA device visible                          */
+#define GS_ERR_STATE       -5   /* call out of order (no scene / no views / ...)   */
+#define GS_ERR_NONFINITE   -6   /* a non-finite loss or parameter was detected     */
+
+/* ---- plain data types ---------------------------------------------------------- */
+
+/* One pinhole camera.  Same fields as trainerCamera() (trainer/colmap.js:57-64) and the
+ * 80-byte camera uniform (trainer/gpu.js:16, :696-701): view = row-major world-to-camera
+ * [R | t] (12 floats, trainer/colmap.js:46-54), intrinsics in pixels, size in pixels. */
+typedef struct GsCamera {
+    float view[12];
+    float fx, fy, cx, cy;
+    int32_t width, height;
+} GsCamera;
+
+/* Per-context options.  Defaults (gs_config_default) are the reference's hard-coded
+ * constants: near 0.2 (trainer/gpu.js:36), EWA dilation 0.3 (:45-47), alpha cap 0.99 and
+ * floor 1/255 (:100-101), transmittance stop 1e-4 (:124), 16-pixel tiles (:118). */
+typedef struct GsConfig {
+    float near_plane;      /* cull when camera-space z < near_plane                    */
+    float cov_dilation;    /* added to the 2D covariance diagonal                      */
+    float alpha_max;       /* alpha clamp                                              */
+    float alpha_min;       /* alphas below this are skipped                           */
+    float t_min;           /* stop a pixel once T <= t_min                             */
+    int32_t sh_degree;     /* 0..3; degree 0 = the reference's raw RGB colour          */
+    int32_t rect_mode;     /* 0 = BIN tile rectangle (trainer/gpu.js:632-635, default),
+                              1 = tileLists() rectangle (trainer/gpu.js:456-461)        */
+    int32_t batched;       /* 1 = one persistent (view, tile) launch for all views;
+                              0 = the plain path: one launch per view per stage        */
+    int32_t use_graph;     /* 1 = capture each training step in a CUDA graph           */
+    int32_t device;        /* CUDA device ordinal                                     */
+    int32_t autotune;      /* 1 = pick raster batch/threads by timing on first step   */
+    int32_t raster_batch;  /* Gaussians per shared-memory batch: 64, 128 or 256        */
+    int32_t lpt_order;     /* 1 = persistent raster takes heavy tiles first           */
+    int32_t instance_capacity; /* initial key-instance capacity; 0 = measured by a first
+                              forward.  A step that overflows skips its update, the
+                              buffer grows and a synchronous step is redone.           */
+    int32_t reserved[3];
+} GsConfig;
+
+/* Adam settings.  The per-group learning rates are the reference's (trainer/gpu.js:846,
+ * :891); beta1/beta2/eps are fixed in the reference's ADAM kernel (:431-435). lr_sh is
+ * the rate for SH bands >= 1, which the reference does not have. */
+typedef struct GsAdamConfig {
+    float lr_color, lr_opacity, lr_mean, lr_scale, lr_rotation, lr_sh;
+    float beta1, beta2, eps;
+} GsAdamConfig;
+
+/* Loss settings: (1 - ssim_lambda) * L1 + ssim_lambda * (1 - SSIM), the reference's
+ * lossGradient (trainer/gpu.js:742-753).  window 0 = 7x7 box windows fully inside the
+ * image (SSIM_COEF, trainer/gpu.js:336-372); window 1 = 11-tap Gaussian, sigma 1.5,
+ * windows fully inside the image. */
+typedef struct GsLossConfig {
+    float ssim_lambda;
+    int32_t window;
+} GsLossConfig;
+
+typedef struct GsContext GsContext;
+
+/* ---- context -------------------------------------------------------------------- */
+
+/* Fills *cfg with the reference's constants.  Replaces the defaults of
+ * createRenderer() (trainer/gpu.js:704). */
+GS_API void gs_config_default(GsConfig* cfg);
+GS_API void gs_adam_default(GsAdamConfig* adam);   /* trainScene lr defaults, gpu.js:891 */
+
+/* createRenderer() (trainer/gpu.js:704-712): binds a device, builds the kernels' state.
+ * Returns GS_ERR_NO_DEVICE when no CUDA device is visible; there is no CPU fallback. */
+GS_API int gs_create(const GsConfig* cfg, GsContext** out);
+GS_API int gs_destroy(GsContext* ctx);
+
+/* Message of the last failed call on this thread (never NULL). */
+GS_API const char* gs_last_error(void);
+GS_API const char* gs_status_string(int status);
+
+/* Number of floats one Gaussian takes in the host parameter record at `sh_degree`:
+ * 14 + 3 * ((sh_degree + 1)^2 - 1).  Record order: mean[3], logScale[3],
+ * rotation[4] (w, x, y, z), opacityLogit, color[3] (the SH DC term, the reference's raw
+ * RGB), then the SH bands >= 1 channel-major (R coefficients 1..K-1, then G, then B),
+ * which is the order of a 3DGS .ply's f_rest_* properties. */
+GS_API int gs_param_stride(int sh_degree);
+
+/* ---- scene ---------------------------------------------------------------------- */
+
+/* Upload n Gaussians in the host record layout above (gs_param_stride floats each).
+ * Resets the Adam moments and step counter, as upload() does (trainer/gpu.js:901-908). */
+GS_API int gs_set_gaussians(GsContext* ctx, int32_t n, const float* params);
+
+/* Upload n Gaussians in the reference's packed 16-float layout (packGaussians,
+ * trainer/gpu.js:5-6, :688-694); SH bands >= 1 are set to zero. */
+GS_API int gs_set_gaussians_packed(GsContext* ctx, int32_t n, const float* packed16);
+
+/* Read the current Gaussians back (host record layout, or the reference's packed
+ * 16-float layout as unpackGaussians expects, trainer/gpu.js:602-609). */
+GS_API int gs_get_gaussians(GsContext* ctx, float* params_out);
+GS_API int gs_get_gaussians_packed(GsContext* ctx, float* packed16_out);
+GS_API int32_t gs_num_gaussians(const GsContext* ctx);
+
+/* ---- views ---------------------------------------------------------------------- */
+
+/* The training views' cameras (trainer/dataset.js:74 view.cam).  Allocates the
+ * per-pixel buffers for all of them; targets are set separately. */
+GS_API int gs_set_views(GsContext* ctx, int32_t num_views, const GsCamera* cams);
+
+/* Target photo of one view: RGB bytes, as decoded by loadDataset (trainer/dataset.js:74;
+ * divided by 255 on the device, as trainer/gpu.js:921 does on the host), or RGB floats
+ * (train(), trainer/gpu.js:852-856).  width * height * 3 values, row-major HWC. */
+GS_API int gs_set_target_u8(GsContext* ctx, int32_t view, const uint8_t* rgb);
+GS_API int gs_set_target_f32(GsContext* ctx, int32_t view, const float* rgb);
+
+/* ---- the Function pair: forward and backward ------------------------------------- */
+
+/* render() (trainer/gpu.js:815-820): project, bin, sort and blend the current scene
+ * from one camera.  rgb_out: width * height * 3 floats, HWC, black background,
+ * unclamped.  state_out (optional, width * height * 2): final transmittance and, as a
+ * float, how many entries of the pixel's tile list the blend consumed
+ * (trainer/gpu.js:133-136, counted from the tile's start). */
+GS_API int gs_render(GsContext* ctx, const GsCamera* cam, float* rgb_out, float* state_out);
+
+/* forward() of views [first, first + count) in one batched pass (or one view per
+ * launch when cfg.batched == 0).  images_out (optional): the views' images
+ * concatenated, each width * height * 3 floats.  The rasteriser state is kept on the
+ * device for gs_backward. */
+GS_API int gs_forward(GsContext* ctx, int32_t first_view, int32_t num_views, float* images_out);
+
+/* backward() for the views of the last gs_forward.  dl_dimages (host, optional):
+ * dLoss/dPixel for every view, laid out like images_out; when NULL the loss gradient
+ * of gs_loss (below) is used.  Fills the parameter gradients kept on the device; read
+ * them with gs_get_param_grads.  The reference's BACKWARD/BACKWARD_SG + SHAPE
+ * (trainer/gpu.js:139-328, :756-761), with the projection chained analytically. */
+GS_API int gs_backward(GsContext* ctx, const float* dl_dimages);
+
+/* Loss and dLoss/dPixel of the last gs_forward against the views' targets
+ * (lossGradient, trainer/gpu.js:742-753).  loss_out (optional): the mean loss over
+ * the views. */
+GS_API int gs_loss(GsContext* ctx, const GsLossConfig* loss, float* loss_out);
+
+/* Parameter gradients of the last gs_backward, host record layout. */
+GS_API int gs_get_param_grads(GsContext* ctx, float* grads_out);
+
+/* Screen-space gradients of the last gs_backward for one of its views, in the
+ * reference's 16-float per-Gaussian layout (trainer/gpu.js:9-10): 0-2 colour,
+ * 3 opacity logit, 4-8 (u, v, conicA, conicB, conicC), 9-15 zero. */
+GS_API int gs_get_screen_grads(GsContext* ctx, int32_t view, float* grads16_out);
+
+/* gradients() (trainer/gpu.js:826-839) for the current scene and one camera against a
+ * float target: image (W*H*3), grads (n*16, as gs_get_screen_grads) and shape
+ * (n*10: mean[3], logScale[3], rotation[4]).  Shape gradients are analytic; the
+ * reference takes them by finite differences (trainer/gpu.js:297-328). */
+GS_API int gs_gradients(GsContext* ctx, const GsCamera* cam, const float* target,
+                 float ssim_lambda, float* image_out, float* grads16_out,
+                 float* shape10_out);
+
+/* lossGradientOf() (trainer/gpu.js:962-977): dLoss/dPixel of an image against a
+ * target, both width * height * 3 floats, with the reference's 7x7 box SSIM
+ * (window 0) or the 11-tap Gaussian window (window 1). */
+GS_API int gs_loss_gradient(GsContext* ctx, const float* image, const float* target,
+                     int32_t width, int32_t height, float ssim_lambda, int32_t window,
+                     float* grad_out, float* loss_out);
+
+/* ---- training ------------------------------------------------------------------- */
+
+/* One training step over views [first, first + count): forward, loss, backward and
+ * Adam with step counter t + 1, against the targets already on the device.  With
+ * cfg.use_graph the whole step is one CUDA graph launch.  loss_out (optional) makes
+ * the call wait for the step and return its mean loss; without it the call returns
+ * once the step is queued.  The ADAM kernel's rules are kept (trainer/gpu.js:411-443):
+ * colour clamped to [0, 1], rotation renormalised. */
+GS_API int gs_train_step(GsContext* ctx, const GsAdamConfig* adam, const GsLossConfig* loss,
+                  int32_t first_view, int32_t num_views, float* loss_out);
+
+/* The same step, with this step's targets given as host RGB bytes (the views'
+ * images concatenated) and copied to the device inside the step, then the loss copied
+ * back: the per-step host traffic of trainScene (trainer/gpu.js:918-921, :934-940).
+ * Use gs_host_alloc for the target buffer to copy from pinned memory. */
+GS_API int gs_train_step_host(GsContext* ctx, const GsAdamConfig* adam, const GsLossConfig* loss,
+                       int32_t first_view, int32_t num_views, const uint8_t* targets_u8,
+                       float* loss_out);
+
+/* train() (trainer/gpu.js:846-878): `steps` steps of L1 loss, one view per step in
+ * order, through the plain per-pixel path; losses_out[steps] gets each step's mean
+ * L1 (the reference reads the image back every step). */
+GS_API int gs_train(GsContext* ctx, int32_t steps, const GsAdamConfig* adam, float* losses_out);
+
+/* Step counter t (number of Adam updates applied since gs_set_gaussians). */
+GS_API int gs_get_step(GsContext* ctx, int32_t* t_out);
+
+/* ---- memory, timing and diagnostics ---------------------------------------------- */
+
+/* Page-locked host memory for per-step uploads (freed with gs_host_free). */
+GS_API int gs_host_alloc(size_t bytes, void** out);
+GS_API int gs_host_free(void* ptr);
+
+/* Waits for all work queued on the context's stream. */
+GS_API int gs_synchronize(GsContext* ctx);
+
+/* CUDA events on the context's stream, for timing from the host binding.
+ * gs_event_record(ctx, slot) records event `slot` (0..63); gs_event_elapsed returns
+ * the milliseconds between two recorded slots (waits for the later one). */
+GS_API int gs_event_record(GsContext* ctx, int32_t slot);
+GS_API int gs_event_elapsed(GsContext* ctx, int32_t slot_a, int32_t slot_b, float* ms_out);
+
+/* Per-stage device times of the steps run since the last reset, summed, in
+ * milliseconds, recorded with events around each stage (also inside the step's CUDA
+ * graph).  names: GS_NUM_STAGES fixed stage names (see gs_stage_name). */
+#define GS_NUM_STAGES 10
+GS_API const char* gs_stage_name(int32_t stage);
+GS_API int gs_stage_times(GsContext* ctx, double* ms_out, int64_t* launches_out,
+                   int32_t* steps_out);
+GS_API int gs_stage_times_reset(GsContext* ctx);
+GS_API int gs_set_stage_timing(GsContext* ctx, int32_t enabled);
+
+/* Statistics of the last forward: key instances emitted (one per (Gaussian, tile)
+ * overlap), visible (Gaussian, view) pairs, blends evaluated in the forward
+ * (pixel, Gaussian) pairs that contributed. */
+typedef struct GsStats {
+    int64_t instances;
+    int64_t instance_capacity;
+    int64_t visible_pairs;
+    int64_t tiles;
+    int64_t pixels;
+    int64_t kernel_launches_per_step;
+    int32_t raster_batch;
+    int32_t raster_threads;
+    int32_t overflow;
+    int32_t reserved;
+} GsStats;
+GS_API int gs_get_stats(GsContext* ctx, GsStats* out);
+
+/* Sorted tile lists of the last forward for one view, in the reference's terms
+ * (tileLists, trainer/gpu.js:450-481): list_out gets the splat indices of every tile
+ * of the view, front to back, concatenated in tile order (capacity list_cap);
+ * ranges_out (2 per tile) gets each tile's [start, end) in list_out; keys_out
+ * (optional, capacity list_cap) gets each entry's 64-bit key
+ * (tile index << 32 | float bits of depth).  *count_out = entries written. */
+GS_API int gs_get_tile_lists(GsContext* ctx, int32_t view, uint32_t* list_out,
+                      uint32_t* ranges_out, uint64_t* keys_out, int64_t list_cap,
+                      int64_t* count_out);
+
+/* Projected splat records of the last forward for one view, in the reference's
+ * 12-float layout (trainer/gpu.js:7): u, v, conicA, conicB, conicC, opacity, radius,
+ * depth, r, g, b, valid. */
+GS_API int gs_get_splats(GsContext* ctx, int32_t view, float* splats12_out);
+
+/* Raster tuning: measures the raster kernels' candidate variants on the current views
+ * and keeps the fastest (tile batch and threads per tile).  cache_path (optional): a
+ * text file that records the choice per device and workload. */
+GS_API int gs_autotune(GsContext* ctx, const char* cache_path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSB200_H */

@@ -1,0 +1,205 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so).  TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline arm as the checker;
+the product never imports it.  See gs_oracle.c for what each function restates
+(trainer/gpu.js of barakatiass-alt/home-measure-privacy) and how parity is pinned.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+F32P = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+F64P = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+U32P = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+U64P = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+
+
+class OrcCamera(ctypes.Structure):
+    _fields_ = [("view", ctypes.c_float * 12), ("fx", ctypes.c_float), ("fy", ctypes.c_float),
+                ("cx", ctypes.c_float), ("cy", ctypes.c_float), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32)]
+
+
+def build(force=False):
+    """Compile liboracle.so with the committed Makefile (gcc, OpenMP)."""
+    src = os.path.join(HERE, "gs_oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(src) > os.path.getmtime(LIB_PATH):
+        subprocess.run(["make", "-C", HERE, "-B" if force else "liboracle.so"], check=True,
+                       capture_output=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB_PATH)
+        CP = ctypes.POINTER(OrcCamera)
+        i, f, d = ctypes.c_int, ctypes.c_float, ctypes.c_double
+        i64 = ctypes.c_int64
+        L.orc_stride.argtypes = [i]
+        L.orc_stride.restype = i
+        L.orc32_preprocess.argtypes = [CP, F32P, i, i, f, f, F32P]
+        L.orc32_bin.argtypes = [F32P, i, i, i, i, i, ctypes.c_void_p, U32P, ctypes.c_void_p, i64]
+        L.orc32_bin.restype = i64
+        L.orc32_forward.argtypes = [F32P, U32P, U32P, i, i, f, f, f, F32P, F32P]
+        L.orc32_loss_grad.argtypes = [F32P, F32P, i, i, f, i, F32P, ctypes.POINTER(d)]
+        L.orc32_backward.argtypes = [F32P, U32P, U32P, F32P, F32P, i, i, f, f, F32P]
+        L.orc32_shape_fd.argtypes = [CP, F32P, i, i, f, f, F32P, F32P]
+        L.orc32_adam.argtypes = [F32P, F32P, F32P, F32P, i, i, i, F32P, f, f, f]
+        L.orc32_step.argtypes = [CP, F32P, F32P, F32P, i, i, F32P, f, i, i, F32P, f, i]
+        L.orc32_step.restype = d
+        L.orc_num_threads.restype = i
+        L.orc_set_threads.argtypes = [i]
+        L.d64_render.argtypes = [CP, F64P, i, i, d, d, d, d, d, F64P, ctypes.POINTER(ctypes.c_uint64)]
+        L.d64_grad.argtypes = [CP, F64P, i, i, d, d, d, d, d, F64P, F64P, ctypes.c_void_p]
+        L.d64_sh_constants.argtypes = [F64P]
+        _lib = L
+    return _lib
+
+
+def camera(cam):
+    """OrcCamera from a trainer camera dict {view[12], fx, fy, cx, cy, width, height}."""
+    c = OrcCamera()
+    for k in range(12):
+        c.view[k] = float(cam["view"][k])
+    c.fx, c.fy, c.cx, c.cy = (float(cam[k]) for k in ("fx", "fy", "cx", "cy"))
+    c.width, c.height = int(cam["width"]), int(cam["height"])
+    return c
+
+
+def stride(degree):
+    return 14 + 3 * ((degree + 1) ** 2 - 1)
+
+
+def preprocess(cam, params, degree, near=0.2, dilation=0.3):
+    params = np.ascontiguousarray(params, np.float32)
+    n = params.shape[0]
+    out = np.zeros((n, 12), np.float32)
+    lib().orc32_preprocess(ctypes.byref(camera(cam)), params.reshape(-1), n, degree, near, dilation,
+                           out.reshape(-1))
+    return out
+
+
+def bin_tiles(splats, width, height, rect_mode=0, cap=0):
+    """Per-tile lists (depth, index order): (list, ranges[tiles, 2], keys)."""
+    splats = np.ascontiguousarray(splats, np.float32)
+    n = splats.shape[0]
+    tiles = ((width + 15) // 16) * ((height + 15) // 16)
+    ranges = np.zeros(tiles * 2, np.uint32)
+    need = -lib().orc32_bin(splats.reshape(-1), n, width, height, rect_mode, cap, None, ranges, None, 0)
+    if need < 0:
+        need = 0
+    lst = np.zeros(max(need, 1), np.uint32)
+    keys = np.zeros(max(need, 1), np.uint64)
+    got = lib().orc32_bin(splats.reshape(-1), n, width, height, rect_mode, cap, lst.ctypes.data, ranges,
+                          keys.ctypes.data, need)
+    assert got == need
+    return lst[:need], ranges.reshape(tiles, 2), keys[:need]
+
+
+def forward(splats, lst, ranges, width, height, amax=0.99, amin=1.0 / 255.0, tmin=1e-4):
+    img = np.zeros((height * width * 3,), np.float32)
+    state = np.zeros((height * width * 2,), np.float32)
+    lst = np.ascontiguousarray(lst if len(lst) else np.zeros(1, np.uint32), np.uint32)
+    lib().orc32_forward(np.ascontiguousarray(splats, np.float32).reshape(-1), lst,
+                        np.ascontiguousarray(ranges, np.uint32).reshape(-1), width, height, amax, amin, tmin,
+                        img, state)
+    return img, state
+
+
+def loss_grad(image, target, width, height, lam, window=0):
+    g = np.zeros(width * height * 3, np.float32)
+    loss = ctypes.c_double(0.0)
+    lib().orc32_loss_grad(np.ascontiguousarray(image, np.float32).reshape(-1),
+                          np.ascontiguousarray(target, np.float32).reshape(-1), width, height, lam, window, g,
+                          ctypes.byref(loss))
+    return g, loss.value
+
+
+def backward(splats, lst, ranges, state, dl, width, height, amax=0.99, amin=1.0 / 255.0):
+    n = splats.shape[0]
+    g = np.zeros(n * 16, np.float32)
+    lst = np.ascontiguousarray(lst if len(lst) else np.zeros(1, np.uint32), np.uint32)
+    lib().orc32_backward(np.ascontiguousarray(splats, np.float32).reshape(-1), lst,
+                         np.ascontiguousarray(ranges, np.uint32).reshape(-1),
+                         np.ascontiguousarray(state, np.float32).reshape(-1),
+                         np.ascontiguousarray(dl, np.float32).reshape(-1), width, height, amax, amin, g)
+    return g.reshape(n, 16)
+
+
+def shape_fd(cam, params, degree, grads16, near=0.2, dilation=0.3):
+    params = np.ascontiguousarray(params, np.float32)
+    n = params.shape[0]
+    out = np.zeros(n * 10, np.float32)
+    lib().orc32_shape_fd(ctypes.byref(camera(cam)), params.reshape(-1), n, degree, near, dilation,
+                         np.ascontiguousarray(grads16, np.float32).reshape(-1), out)
+    return out.reshape(n, 10)
+
+
+def adam(params, grads, m, v, degree, t, lr6, beta1=0.9, beta2=0.999, eps=1e-8):
+    """In place on params, m, v (host records, float32)."""
+    n = params.shape[0]
+    lib().orc32_adam(params.reshape(-1), np.ascontiguousarray(grads, np.float32).reshape(-1), m.reshape(-1),
+                     v.reshape(-1), n, degree, t, np.asarray(lr6, np.float32), beta1, beta2, eps)
+
+
+def step(cam, params, m, v, degree, target, lam, window, t, lr6, near=0.2, cap=1024):
+    """The reference's trainScene step on one view (in place); returns the loss."""
+    n = params.shape[0]
+    return lib().orc32_step(ctypes.byref(camera(cam)), params.reshape(-1), m.reshape(-1), v.reshape(-1), n,
+                            degree, np.ascontiguousarray(target, np.float32).reshape(-1), lam, window, t,
+                            np.asarray(lr6, np.float32), near, cap)
+
+
+def render_ref(cam, params, degree, near=0.2, rect_mode=0, cap=0):
+    """FP32 reference pipeline: splats, tile lists, image, state."""
+    w, h = int(cam["width"]), int(cam["height"])
+    s = preprocess(cam, params, degree, near)
+    lst, ranges, keys = bin_tiles(s, w, h, rect_mode, cap)
+    img, state = forward(s, lst, ranges, w, h)
+    return dict(splats=s, list=lst, ranges=ranges, keys=keys, image=img, state=state)
+
+
+def num_threads():
+    return lib().orc_num_threads()
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+# ---- FP64 ----------------------------------------------------------------------------
+def render64(cam, params, degree, near=0.2, dilation=0.3, amax=0.99, amin=1.0 / 255.0, tmin=1e-4):
+    params = np.ascontiguousarray(params, np.float64)
+    n = params.shape[0]
+    w, h = int(cam["width"]), int(cam["height"])
+    img = np.zeros(w * h * 3, np.float64)
+    sig = ctypes.c_uint64(0)
+    lib().d64_render(ctypes.byref(camera(cam)), params.reshape(-1), n, degree, near, dilation, amax, amin, tmin,
+                     img, ctypes.byref(sig))
+    return img, sig.value
+
+
+def grad64(cam, params, degree, dl, near=0.2, dilation=0.3, amax=0.99, amin=1.0 / 255.0, tmin=1e-4):
+    params = np.ascontiguousarray(params, np.float64)
+    n = params.shape[0]
+    g = np.zeros(params.size, np.float64)
+    s16 = np.zeros(n * 16, np.float64)
+    lib().d64_grad(ctypes.byref(camera(cam)), params.reshape(-1), n, degree, near, dilation, amax, amin, tmin,
+                   np.ascontiguousarray(dl, np.float64).reshape(-1), g, s16.ctypes.data)
+    return g.reshape(params.shape), s16.reshape(n, 16)
+
+
+def sh_constants64():
+    out = np.zeros(15, np.float64)
+    lib().d64_sh_constants(out)
+    return out
