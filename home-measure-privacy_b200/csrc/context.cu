@@ -124,6 +124,7 @@ struct GsContext {
     bool inst_cap_valid = false;
     DevBuf ikeys, ivals, ikeys_alt, ivals_alt;
     DevBuf hist, totals, block_sums;  // radix histograms, digit totals, emission chunk sums
+    DevBuf pair_offsets, block_first_pair;  // emission: per-pair offsets, expansion marks
     // segments: [0, 65) all-pairs segment of c views; [65, 129) pair segment of slot s;
     // [129] batched instance segment; [130, 194) instance segment of slot s
     DevBuf segs, visible, acc, scratch16;
@@ -352,6 +353,7 @@ static int size_pairs(GsContext* c, int views) {
         CKI(ensure(c->sg8, (size_t)pairs * 32, c));
         CKI(ensure(c->sg1, (size_t)pairs * 4, c));
         CKI(ensure(c->block_sums, (size_t)(pairs / emit_chunk_items() + 2) * 4, c));
+        CKI(ensure(c->pair_offsets, (size_t)pairs * 4, c));
         c->pair_cap = pairs;
         const int64_t parts = (std::max(pairs, c->inst_cap) + radix_tile_items() - 1) / radix_tile_items() + 1;
         CKI(ensure(c->hist, (size_t)parts * 256 * 4, c));
@@ -380,6 +382,7 @@ static int size_instances(GsContext* c, int64_t cap) {
     CKI(ensure(c->ivals, (size_t)cap * 4, c));
     CKI(ensure(c->ikeys_alt, (size_t)cap * 4, c));
     CKI(ensure(c->ivals_alt, (size_t)cap * 4, c));
+    CKI(ensure(c->block_first_pair, (size_t)(cap / emit_out_items() + 2) * 4, c));
     c->inst_cap = cap;
     const int64_t parts = (std::max(c->pair_cap, c->inst_cap) + radix_tile_items() - 1) / radix_tile_items() + 1;
     CKI(ensure(c->hist, (size_t)parts * 256 * 4, c));
@@ -497,6 +500,8 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ea.view_first = step_first;  // pair / n_pad is the slot relative to the step's first view
     ea.n_pad = c->n_pad;
     ea.block_sums = c->block_sums.as<uint32_t>();
+    ea.pair_offsets = c->pair_offsets.as<uint32_t>();
+    ea.block_first_pair = c->block_first_pair.as<uint32_t>();
     ea.inst_seg = inst_seg;
     ea.prev_seg = prev_seg;
     ea.inst_keys = c->ikeys.as<uint32_t>();
@@ -505,7 +510,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ea.status = st;
     ea.max_chunks = (int)((int64_t)vcount * c->n_pad / emit_chunk_items() + 1);
     launch_emit(ea, c->stream, c->num_sms);
-    count_launches(c, ST_EMIT, 3);
+    count_launches(c, ST_EMIT, 4);
     // Stable sort by tile id, then the tile ranges.
     CKI(mark(c, ST_SORT_INST));
     RadixSortArgs rb = ra;
@@ -916,6 +921,7 @@ int gs_destroy(GsContext* c) {
                       &c->image, &c->t_final, &c->last, &c->dl, &c->ranges, &c->tile_order, &c->geo0, &c->geo1,
                       &c->rgb, &c->rect, &c->pkeys, &c->pvals, &c->pkeys_alt, &c->pvals_alt, &c->sg8, &c->sg1,
                       &c->ikeys, &c->ivals, &c->ikeys_alt, &c->ivals_alt, &c->hist, &c->totals, &c->block_sums,
+                      &c->pair_offsets, &c->block_first_pair,
                       &c->segs, &c->visible, &c->acc, &c->scratch16, &c->status};
     for (DevBuf* b : bufs) release(*b);
     for (cudaEvent_t e : c->capture_events) cudaEventDestroy(e);

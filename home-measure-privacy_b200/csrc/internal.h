@@ -69,6 +69,8 @@ struct EmitArgs {
     int view_first, n_pad;
     int pair_slot_first;            // slot of the first pair of this segment
     uint32_t* block_sums;           // scratch, >= chunks
+    uint32_t* pair_offsets;         // scratch: first instance of each sorted pair (>= pairs)
+    uint32_t* block_first_pair;     // scratch: pair of every EM_OUT-th instance (>= cap/EM_OUT + 2)
     SegInfo* inst_seg;              // out: instance segment (base, count)
     const SegInfo* prev_seg;        // previous instance segment (plain path) or nullptr
     uint32_t* inst_keys;            // global tile id
@@ -79,6 +81,7 @@ struct EmitArgs {
 };
 void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms);
 int emit_chunk_items();
+int emit_out_items();
 
 // Tile ranges from tile-sorted instances.
 void launch_ranges(const uint32_t* sorted_tiles, const SegInfo* seg, uint2* ranges,

@@ -5,11 +5,13 @@
 // and channel, SSIM and its partials a, b, d by the window mean, mean of squares and
 // mean of products) and LOSS_GRAD (:374-409: each pixel sums a + 2 x b + y d over the
 // windows that cover it, 49 taps each, reading the coefficients back from HBM).  Here
-// one CTA owns a 32 x 16 block of output pixels and keeps everything in shared memory:
+// one CTA owns a 32 x 32 block of output pixels and keeps everything in shared memory:
 // it loads image and target with a 2R halo, forms the five window moments with a
 // separable (horizontal then vertical) filter, turns them into the coefficients
 // a, b, d at every window centre that can reach the block, and filters those
-// coefficients back (again separably) to get each pixel's SSIM gradient.  Windows are
+// coefficients back (again separably) to get each pixel's SSIM gradient.  Every pass
+// gives each thread a short strip of outputs computed from a register window, so one
+// shared-memory load feeds up to 2R + 1 filter taps.  Windows are
 // the reference's: centres whose whole window lies inside the image (7x7 box, R = 3),
 // or the 11-tap Gaussian (sigma 1.5, R = 5) with the same rule.  The kernel also sums
 // |x - y| and the SSIM of the windows centred in its block for the loss value.
@@ -18,8 +20,13 @@
 namespace gs {
 
 constexpr int LB_W = 32;
-constexpr int LB_H = 16;
+constexpr int LB_H = 32;
 constexpr int LB_THREADS = 256;
+// Strip lengths of the four separable passes (outputs per thread task).
+constexpr int S1 = 7;   // horizontal moments
+constexpr int S2 = 4;   // vertical moments -> SSIM coefficients
+constexpr int S3 = 4;   // horizontal coefficients
+constexpr int S4 = 4;   // vertical coefficients -> gradient
 
 struct LossWeights {
     float w[11];
@@ -51,9 +58,10 @@ __device__ __forceinline__ float load_target<float>(const float* t, size_t idx) 
 }
 
 template <int R, typename TT>
-__global__ void __launch_bounds__(LB_THREADS) loss_kernel(LossArgs a, const TT* __restrict__ target,
+__global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const TT* __restrict__ target,
                                                           LossWeights wts) {
     using D = LossDims<R>;
+    constexpr int K = 2 * R + 1;
     extern __shared__ float sm[];
     __shared__ float s_red[2][LB_THREADS / 32];
     const int blk = a.block_first + blockIdx.x;
@@ -69,6 +77,8 @@ __global__ void __launch_bounds__(LB_THREADS) loss_kernel(LossArgs a, const TT* 
     const int winx = W - 2 * R, winy = H - 2 * R;
     const float windows = (winx > 0 && winy > 0) ? (float)winx * (float)winy * 3.0f : 0.0f;
     const bool use_ssim = a.lambda > 0.0f && windows > 0.0f;
+    // Filter taps stay in the kernel-parameter constant bank (FFMA operands).
+    const float* w = wts.w;
     float* X = sm + D::X_OFF;
     float* Y = sm + D::Y_OFF;
     float* HM = sm + D::HM_OFF;
@@ -76,6 +86,10 @@ __global__ void __launch_bounds__(LB_THREADS) loss_kernel(LossArgs a, const TT* 
     float* HC = sm + D::HC_OFF;
     float l1 = 0.f, ssim_sum = 0.f;
     const float C1 = 1e-4f, C2 = 9e-4f;
+    constexpr int NS1 = (D::HW + S1 - 1) / S1;
+    constexpr int NS2 = (D::CH + S2 - 1) / S2;
+    constexpr int NS3 = LB_W / S3;
+    constexpr int NS4 = LB_H / S4;
     for (int c = 0; c < 3; c++) {
         if (use_ssim) {
             for (int idx = threadIdx.x; idx < D::RH * D::RW; idx += LB_THREADS) {
@@ -91,105 +105,141 @@ __global__ void __launch_bounds__(LB_THREADS) loss_kernel(LossArgs a, const TT* 
                 Y[idx] = yv;
             }
             __syncthreads();
-            // Horizontal moments at every region row and centre column.
-            for (int idx = threadIdx.x; idx < D::RH * D::HW; idx += LB_THREADS) {
-                const int r = idx / D::HW, hc = idx % D::HW;
-                float mx = 0.f, my = 0.f, sxx = 0.f, syy = 0.f, sxy = 0.f;
+            // P1: horizontal moments, S1 centre columns per task from a register window.
+            for (int task = threadIdx.x; task < D::RH * NS1; task += LB_THREADS) {
+                const int r = task / NS1, c0 = (task % NS1) * S1;
+                float xs[S1 + 2 * R], ys[S1 + 2 * R];
 #pragma unroll
-                for (int k = 0; k <= 2 * R; k++) {
-                    const float w = wts.w[k];
-                    const float xv = X[r * D::RW + hc + k], yv = Y[r * D::RW + hc + k];
-                    mx += w * xv;
-                    my += w * yv;
-                    sxx += w * xv * xv;
-                    syy += w * yv * yv;
-                    sxy += w * xv * yv;
+                for (int t = 0; t < S1 + 2 * R; t++) {
+                    const int col = c0 + t;
+                    xs[t] = col < D::RW ? X[r * D::RW + col] : 0.f;
+                    ys[t] = col < D::RW ? Y[r * D::RW + col] : 0.f;
                 }
-                HM[0 * D::RH * D::HW + idx] = mx;
-                HM[1 * D::RH * D::HW + idx] = my;
-                HM[2 * D::RH * D::HW + idx] = sxx;
-                HM[3 * D::RH * D::HW + idx] = syy;
-                HM[4 * D::RH * D::HW + idx] = sxy;
-            }
-            __syncthreads();
-            // Vertical pass -> SSIM coefficients at window centres.
-            for (int idx = threadIdx.x; idx < D::CH * D::HW; idx += LB_THREADS) {
-                const int hr = idx / D::HW, hc = idx % D::HW;
-                const int gx = bx0 - R + hc, gy = by0 - R + hr;
-                float ca = 0.f, cb = 0.f, cd = 0.f;
-                if (gx >= R && gy >= R && gx < W - R && gy < H - R) {
-                    float m[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                    for (int k = 0; k <= 2 * R; k++) {
-                        const float w = wts.w[k];
-                        const int row = (hr + k) * D::HW + hc;
+                for (int k = 0; k < S1; k++) {
+                    if (c0 + k >= D::HW) break;
+                    float mx = 0.f, my = 0.f, sxx = 0.f, syy = 0.f, sxy = 0.f;
 #pragma unroll
-                        for (int q = 0; q < 5; q++) m[q] += w * HM[q * D::RH * D::HW + row];
+                    for (int t = 0; t < K; t++) {
+                        const float xv = xs[k + t], yv = ys[k + t], wt = w[t];
+                        mx += wt * xv;
+                        my += wt * yv;
+                        sxx += wt * xv * xv;
+                        syy += wt * yv * yv;
+                        sxy += wt * xv * yv;
                     }
-                    const float mx = m[0], my = m[1], sxx = m[2], syy = m[3], sxy = m[4];
-                    const float a1 = 2.0f * mx * my + C1;
-                    const float a2 = 2.0f * (sxy - mx * my) + C2;
-                    const float b1 = mx * mx + my * my + C1;
-                    const float b2 = (sxx - mx * mx) + (syy - my * my) + C2;
-                    const float ssim = a1 * a2 / (b1 * b2);
-                    ca = ssim * (2.0f * my / a1 - 2.0f * my / a2 - 2.0f * mx / b1 + 2.0f * mx / b2);
-                    cb = -ssim / b2;
-                    cd = 2.0f * ssim / a2;
-                    if (gx >= bx0 && gx < bx0 + LB_W && gy >= by0 && gy < by0 + LB_H) ssim_sum += ssim;
+                    const int o = r * D::HW + c0 + k;
+                    HM[0 * D::RH * D::HW + o] = mx;
+                    HM[1 * D::RH * D::HW + o] = my;
+                    HM[2 * D::RH * D::HW + o] = sxx;
+                    HM[3 * D::RH * D::HW + o] = syy;
+                    HM[4 * D::RH * D::HW + o] = sxy;
                 }
-                CF[0 * D::CH * D::HW + idx] = ca;
-                CF[1 * D::CH * D::HW + idx] = cb;
-                CF[2 * D::CH * D::HW + idx] = cd;
             }
             __syncthreads();
-            // Filter the coefficients back: horizontal ...
-            for (int idx = threadIdx.x; idx < D::CH * LB_W; idx += LB_THREADS) {
-                const int hr = idx / LB_W, oc = idx % LB_W;
-                float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+            // P2: vertical moments at S2 window centres per task -> SSIM coefficients.
+            for (int task = threadIdx.x; task < D::HW * NS2; task += LB_THREADS) {
+                const int hc = task % D::HW, h0 = (task / D::HW) * S2;
+                float m[5][S2 + 2 * R];
 #pragma unroll
-                for (int k = 0; k <= 2 * R; k++) {
-                    const float w = wts.w[k];
-                    const int q = hr * D::HW + oc + k;
-                    s0 += w * CF[0 * D::CH * D::HW + q];
-                    s1 += w * CF[1 * D::CH * D::HW + q];
-                    s2 += w * CF[2 * D::CH * D::HW + q];
+                for (int q = 0; q < 5; q++)
+#pragma unroll
+                    for (int t = 0; t < S2 + 2 * R; t++) {
+                        const int row = h0 + t;
+                        m[q][t] = row < D::RH ? HM[q * D::RH * D::HW + row * D::HW + hc] : 0.f;
+                    }
+#pragma unroll
+                for (int k = 0; k < S2; k++) {
+                    const int hr = h0 + k;
+                    if (hr >= D::CH) break;
+                    const int gx = bx0 - R + hc, gy = by0 - R + hr;
+                    float ca = 0.f, cb = 0.f, cd = 0.f;
+                    if (gx >= R && gy >= R && gx < W - R && gy < H - R) {
+                        float mm[5];
+#pragma unroll
+                        for (int q = 0; q < 5; q++) {
+                            float acc = 0.f;
+#pragma unroll
+                            for (int t = 0; t < K; t++) acc += w[t] * m[q][k + t];
+                            mm[q] = acc;
+                        }
+                        const float mx = mm[0], my = mm[1], sxx = mm[2], syy = mm[3], sxy = mm[4];
+                        const float a1 = 2.0f * mx * my + C1;
+                        const float a2 = 2.0f * (sxy - mx * my) + C2;
+                        const float b1 = mx * mx + my * my + C1;
+                        const float b2 = (sxx - mx * mx) + (syy - my * my) + C2;
+                        const float ssim = a1 * a2 / (b1 * b2);
+                        ca = ssim * (2.0f * my / a1 - 2.0f * my / a2 - 2.0f * mx / b1 + 2.0f * mx / b2);
+                        cb = -ssim / b2;
+                        cd = 2.0f * ssim / a2;
+                        if (gx >= bx0 && gx < bx0 + LB_W && gy >= by0 && gy < by0 + LB_H) ssim_sum += ssim;
+                    }
+                    const int o = hr * D::HW + hc;
+                    CF[0 * D::CH * D::HW + o] = ca;
+                    CF[1 * D::CH * D::HW + o] = cb;
+                    CF[2 * D::CH * D::HW + o] = cd;
                 }
-                HC[0 * D::CH * LB_W + idx] = s0;
-                HC[1 * D::CH * LB_W + idx] = s1;
-                HC[2 * D::CH * LB_W + idx] = s2;
+            }
+            __syncthreads();
+            // P3: filter the coefficients back, horizontal ...
+            for (int task = threadIdx.x; task < D::CH * NS3; task += LB_THREADS) {
+                const int hr = task / NS3, o0 = (task % NS3) * S3;
+                float cf[3][S3 + 2 * R];
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+#pragma unroll
+                    for (int t = 0; t < S3 + 2 * R; t++) cf[q][t] = CF[q * D::CH * D::HW + hr * D::HW + o0 + t];
+#pragma unroll
+                for (int k = 0; k < S3; k++)
+#pragma unroll
+                    for (int q = 0; q < 3; q++) {
+                        float acc = 0.f;
+#pragma unroll
+                        for (int t = 0; t < K; t++) acc += w[t] * cf[q][k + t];
+                        HC[q * D::CH * LB_W + hr * LB_W + o0 + k] = acc;
+                    }
             }
             __syncthreads();
         }
-        // ... and vertical, then the per-pixel gradient.
-        for (int idx = threadIdx.x; idx < LB_W * LB_H; idx += LB_THREADS) {
-            const int oy = idx / LB_W, ox = idx % LB_W;
-            const int gx = bx0 + ox, gy = by0 + oy;
-            if (gx >= W || gy >= H) continue;
-            const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
-            float xv, yv;
+        // P4: ... and vertical, then the per-pixel gradient (with the L1 term).
+        for (int task = threadIdx.x; task < LB_W * NS4; task += LB_THREADS) {
+            const int ox = task % LB_W, oy0 = (task / LB_W) * S4;
+            const int gx = bx0 + ox;
+            float hc[3][S4 + 2 * R];
             if (use_ssim) {
-                xv = X[(oy + 2 * R) * D::RW + ox + 2 * R];
-                yv = Y[(oy + 2 * R) * D::RW + ox + 2 * R];
-            } else {
-                xv = a.image[q];
-                yv = load_target<TT>(target, q);
-            }
-            const float diff = xv - yv;
-            float g = (1.0f - a.lambda) * (float)((diff > 0.f) - (diff < 0.f)) / n;
-            l1 += fabsf(diff);
-            if (use_ssim) {
-                float sa = 0.f, sb = 0.f, sd = 0.f;
 #pragma unroll
-                for (int k = 0; k <= 2 * R; k++) {
-                    const float w = wts.w[k];
-                    const int r = (oy + k) * LB_W + ox;
-                    sa += w * HC[0 * D::CH * LB_W + r];
-                    sb += w * HC[1 * D::CH * LB_W + r];
-                    sd += w * HC[2 * D::CH * LB_W + r];
-                }
-                g -= a.lambda * ((sa + 2.0f * xv * sb + yv * sd) / windows);
+                for (int q = 0; q < 3; q++)
+#pragma unroll
+                    for (int t = 0; t < S4 + 2 * R; t++) hc[q][t] = HC[q * D::CH * LB_W + (oy0 + t) * LB_W + ox];
             }
-            a.dl[q] = g;
+#pragma unroll
+            for (int k = 0; k < S4; k++) {
+                const int oy = oy0 + k, gy = by0 + oy;
+                if (gx >= W || gy >= H) continue;
+                const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
+                float xv, yv;
+                if (use_ssim) {
+                    xv = X[(oy + 2 * R) * D::RW + ox + 2 * R];
+                    yv = Y[(oy + 2 * R) * D::RW + ox + 2 * R];
+                } else {
+                    xv = a.image[q];
+                    yv = load_target<TT>(target, q);
+                }
+                const float diff = xv - yv;
+                float g = (1.0f - a.lambda) * (float)((diff > 0.f) - (diff < 0.f)) / n;
+                l1 += fabsf(diff);
+                if (use_ssim) {
+                    float sa = 0.f, sb = 0.f, sd = 0.f;
+#pragma unroll
+                    for (int t = 0; t < K; t++) {
+                        sa += w[t] * hc[0][k + t];
+                        sb += w[t] * hc[1][k + t];
+                        sd += w[t] * hc[2][k + t];
+                    }
+                    g -= a.lambda * ((sa + 2.0f * xv * sb + yv * sd) / windows);
+                }
+                a.dl[q] = g;
+            }
         }
         __syncthreads();
     }
@@ -207,9 +257,9 @@ __global__ void __launch_bounds__(LB_THREADS) loss_kernel(LossArgs a, const TT* 
     __syncthreads();
     if (threadIdx.x == 0) {
         double t0 = 0.0, t1 = 0.0;
-        for (int w = 0; w < LB_THREADS / 32; w++) {
-            t0 += s_red[0][w];
-            t1 += s_red[1][w];
+        for (int k = 0; k < LB_THREADS / 32; k++) {
+            t0 += s_red[0][k];
+            t1 += s_red[1][k];
         }
         atomicAdd(a.acc + 2 * vi + 0, t0);
         atomicAdd(a.acc + 2 * vi + 1, t1);

@@ -44,8 +44,11 @@ struct TileInfo {
     int width, height;
     int pixel_offset;
     bool inside;
+    float wx0, wx1, wy0, wy1;  // pixel-centre rectangle of this thread's warp
 };
 
+// Thread -> pixel: warp w covers an 8 x 4 block (w & 1, w >> 1) of the 16 x 16 tile,
+// a squarer footprint than two 16-pixel rows, so fewer splats reach each warp.
 __device__ __forceinline__ TileInfo tile_info(const RasterArgs& a, int item) {
     TileInfo ti;
     const int local = a.tile_order ? (int)a.tile_order[item] : item;
@@ -56,12 +59,18 @@ __device__ __forceinline__ TileInfo tile_info(const RasterArgs& a, int item) {
     const ViewDesc& vw = a.views[vi];
     const int lt = ti.g - vw.tile_offset;
     const int tx = lt % vw.tiles_x, ty = lt / vw.tiles_x;
-    ti.x = tx * GS_TILE + (threadIdx.x & (GS_TILE - 1));
-    ti.y = ty * GS_TILE + (threadIdx.x / GS_TILE);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bx = tx * GS_TILE + (w & 1) * 8, by = ty * GS_TILE + (w >> 1) * 4;
+    ti.x = bx + (lane & 7);
+    ti.y = by + (lane >> 3);
     ti.width = vw.width;
     ti.height = vw.height;
     ti.pixel_offset = vw.pixel_offset;
     ti.inside = ti.x < vw.width && ti.y < vw.height;
+    ti.wx0 = (float)bx + 0.5f;
+    ti.wx1 = (float)bx + 7.5f;
+    ti.wy0 = (float)by + 0.5f;
+    ti.wy1 = (float)by + 3.5f;
     return ti;
 }
 
@@ -88,12 +97,49 @@ __device__ __forceinline__ void stage_batch(const RasterArgs& a, uint32_t first,
     cp_async_commit();
 }
 
+// After the batch's copies landed: each staging thread replaces the (unused here) depth
+// of its splats with the culling bound 2 ln(opacity / alpha_min) + slack: a pixel can
+// reach alpha >= alpha_min only where the conic's quadratic form is below it.
+__device__ __forceinline__ void prepare_batch(int cnt, float4* s_g1, float log_amin) {
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const float op = s_g1[t].y;
+        s_g1[t].w = op > 0.f ? 2.0f * (__logf(op) - log_amin) + 1e-3f : -1.0f;
+    }
+}
+
+// Smallest value of the conic's quadratic form A dx^2 + 2 B dx dy + C dy^2 over the box
+// [xl, xh] x [yl, yh] (offsets from the splat centre).  Convex, so: 0 when the centre is
+// inside, else the least of the four edges' clamped 1-D minima.
+__device__ __forceinline__ float qmin_box(float A, float B, float C, float xl, float xh, float yl, float yh) {
+    if (xl <= 0.f && xh >= 0.f && yl <= 0.f && yh >= 0.f) return 0.f;
+    const float iA = 1.0f / A, iC = 1.0f / C;
+    float best, x, y, q;
+    x = xl; y = fminf(fmaxf(-B * x * iC, yl), yh); best = A * x * x + 2.f * B * x * y + C * y * y;
+    x = xh; y = fminf(fmaxf(-B * x * iC, yl), yh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
+    y = yl; x = fminf(fmaxf(-B * y * iA, xl), xh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
+    y = yh; x = fminf(fmaxf(-B * y * iA, xl), xh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
+    return best;
+}
+
+// Can splat (g0, g1) give any pixel centre of the warp's rectangle alpha >= alpha_min?
+// Conservative: the pixels' own tests (bounding box, then alpha) decide; this only
+// skips splats that cannot pass them anywhere in the rectangle.
+__device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1, const TileInfo& ti) {
+    const float r = g1.z;
+    const float xl = fmaxf(ti.wx0, g0.x - r), xh = fminf(ti.wx1, g0.x + r);
+    const float yl = fmaxf(ti.wy0, g0.y - r), yh = fminf(ti.wy1, g0.y + r);
+    if (xl > xh || yl > yh) return false;
+    return qmin_box(g0.z, g0.w, g1.x, xl - g0.x, xh - g0.x, yl - g0.y, yh - g0.y) <= g1.w;
+}
+
 template <int BATCH>
 __global__ void __launch_bounds__(256) raster_fwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
     __shared__ int s_item;
+    const int lane = threadIdx.x & 31;
+    const float log_amin = __logf(a.alpha_min);
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
         const TileInfo ti = tile_info(a, item);
@@ -115,12 +161,20 @@ __global__ void __launch_bounds__(256) raster_fwd_kernel(RasterArgs a) {
             } else {
                 cp_async_wait<0>();
             }
+            prepare_batch(cnt, s_g1[buf], log_amin);
             __syncthreads();
-            if (!done) {
-                const float4* g0s = s_g0[buf];
-                const float4* g1s = s_g1[buf];
-                const float4* cs = s_c[buf];
-                for (int j = 0; j < cnt; j++) {
+            const float4* g0s = s_g0[buf];
+            const float4* g1s = s_g1[buf];
+            const float4* cs = s_c[buf];
+            bool warp_done = __all_sync(FULL_MASK, done);
+            for (int gb = 0; gb < cnt && !warp_done; gb += 32) {
+                const int jl = gb + lane;
+                const bool rel = jl < cnt && warp_reaches(g0s[jl], g1s[jl], ti);
+                uint32_t mask = __ballot_sync(FULL_MASK, rel);
+                while (mask) {
+                    const int j = gb + __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    if (done) continue;
                     const float4 g0 = g0s[j];
                     const float4 g1 = g1s[j];
                     const float dx = pxf - g0.x, dy = pyf - g0.y;
@@ -135,11 +189,9 @@ __global__ void __launch_bounds__(256) raster_fwd_kernel(RasterArgs a) {
                     cb += c.z * alpha * T;
                     T *= 1.0f - alpha;
                     last = b0 + (uint32_t)j + 1u;
-                    if (T <= a.t_min) {
-                        done = true;
-                        break;
-                    }
+                    if (T <= a.t_min) done = true;
                 }
+                warp_done = __all_sync(FULL_MASK, done);
             }
             buf ^= 1;
             // All pixels done: the rest of the list cannot change the tile.
@@ -199,6 +251,7 @@ __global__ void __launch_bounds__(256) raster_bwd_kernel(RasterArgs a) {
     __shared__ int s_item;
     __shared__ unsigned int s_end;
     const int lane = threadIdx.x & 31;
+    const float log_amin = __logf(a.alpha_min);
     float* sg8f = reinterpret_cast<float*>(a.sg8);
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
@@ -218,7 +271,8 @@ __global__ void __launch_bounds__(256) raster_bwd_kernel(RasterArgs a) {
         }
         if (threadIdx.x == 0) s_end = start;
         __syncthreads();
-        // Tile end = largest last of its pixels (BACKWARD_SG, trainer/gpu.js:247-253).
+        // Tile end = largest last of its pixels (BACKWARD_SG, trainer/gpu.js:247-253);
+        // each warp also stops at its own largest last.
         unsigned int wmax = mylast;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) wmax = max(wmax, __shfl_xor_sync(FULL_MASK, wmax, o));
@@ -239,63 +293,72 @@ __global__ void __launch_bounds__(256) raster_bwd_kernel(RasterArgs a) {
             } else {
                 cp_async_wait<0>();
             }
+            prepare_batch(cnt, s_g1[buf], log_amin);
             __syncthreads();
             const float4* g0s = s_g0[buf];
             const float4* g1s = s_g1[buf];
             const float4* cs = s_c[buf];
             const uint32_t* ps = s_pair[buf];
-            // Warp-uniform skip: no pixel of this warp reaches this batch.
-            const bool warp_active = __any_sync(FULL_MASK, ti.inside && bstart < mylast);
-            if (warp_active) {
-                for (int j = 0; j < cnt; j++) {
-                    const uint32_t k = bend - 1 - (uint32_t)j;
-                    float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                    float v8 = 0.f;
-                    bool contrib = false;
-                    if (ti.inside && k < mylast) {
-                        const float4 g0 = g0s[j];
-                        const float4 g1 = g1s[j];
-                        const float dx = pxf - g0.x, dy = pyf - g0.y;
-                        if (fabsf(dx) <= g1.z && fabsf(dy) <= g1.z) {
-                            const float power = -0.5f * (g0.z * dx * dx + g1.x * dy * dy) - g0.w * dx * dy;
-                            if (power <= 0.0f) {
-                                const float alpha = fminf(a.alpha_max, g1.y * expf(power));
-                                if (alpha >= a.alpha_min) {
-                                    contrib = true;
-                                    const float4 c = cs[j];
-                                    const float oma = 1.0f - alpha;
-                                    const float Tk = T / oma;
-                                    v[0] = dlr * alpha * Tk;
-                                    v[1] = dlg * alpha * Tk;
-                                    v[2] = dlb * alpha * Tk;
-                                    const float dA = dlr * (Tk * c.x - br / oma) + dlg * (Tk * c.y - bg / oma) +
-                                                     dlb * (Tk * c.z - bb / oma);
-                                    br += c.x * alpha * Tk;
-                                    bg += c.y * alpha * Tk;
-                                    bb += c.z * alpha * Tk;
-                                    T = Tk;
-                                    if (alpha < a.alpha_max) {
-                                        const float op = g1.y;
-                                        v[3] = dA * (alpha / op) * op * (1.0f - op);
-                                        const float dP = dA * alpha;
-                                        v[4] = dP * (g0.z * dx + g0.w * dy);
-                                        v[5] = dP * (g1.x * dy + g0.w * dx);
-                                        v[6] = dP * -0.5f * dx * dx;
-                                        v[7] = dP * -dx * dy;
-                                        v8 = dP * -0.5f * dy * dy;
+            // Entry j of the batch is list position bend - 1 - j: ascending j walks back to
+            // front.  Warps whose pixels all stopped before this batch skip it.
+            if (bstart < wmax) {
+                for (int gb = 0; gb < cnt; gb += 32) {
+                    const int jl = gb + lane;
+                    const bool rel = jl < cnt && (bend - 1 - (uint32_t)jl) < wmax && warp_reaches(g0s[jl], g1s[jl], ti);
+                    uint32_t mask = __ballot_sync(FULL_MASK, rel);
+                    while (mask) {
+                        const int j = gb + __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const uint32_t k = bend - 1 - (uint32_t)j;
+                        float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                        float v8 = 0.f;
+                        bool contrib = false;
+                        if (ti.inside && k < mylast) {
+                            const float4 g0 = g0s[j];
+                            const float4 g1 = g1s[j];
+                            const float dx = pxf - g0.x, dy = pyf - g0.y;
+                            if (fabsf(dx) <= g1.z && fabsf(dy) <= g1.z) {
+                                const float power = -0.5f * (g0.z * dx * dx + g1.x * dy * dy) - g0.w * dx * dy;
+                                if (power <= 0.0f) {
+                                    const float alpha = fminf(a.alpha_max, g1.y * expf(power));
+                                    if (alpha >= a.alpha_min) {
+                                        contrib = true;
+                                        const float4 c = cs[j];
+                                        const float oma = 1.0f - alpha;
+                                        const float ioma = 1.0f / oma;
+                                        const float Tk = T * ioma;
+                                        v[0] = dlr * alpha * Tk;
+                                        v[1] = dlg * alpha * Tk;
+                                        v[2] = dlb * alpha * Tk;
+                                        const float dA = dlr * (Tk * c.x - br * ioma) + dlg * (Tk * c.y - bg * ioma) +
+                                                         dlb * (Tk * c.z - bb * ioma);
+                                        br += c.x * alpha * Tk;
+                                        bg += c.y * alpha * Tk;
+                                        bb += c.z * alpha * Tk;
+                                        T = Tk;
+                                        if (alpha < a.alpha_max) {
+                                            const float op = g1.y;
+                                            v[3] = dA * alpha * (1.0f - op);
+                                            const float dP = dA * alpha;
+                                            v[4] = dP * (g0.z * dx + g0.w * dy);
+                                            v[5] = dP * (g1.x * dy + g0.w * dx);
+                                            v[6] = dP * -0.5f * dx * dx;
+                                            v[7] = dP * -dx * dy;
+                                            v8 = dP * -0.5f * dy * dy;
+                                        }
                                     }
                                 }
                             }
                         }
-                    }
-                    if (__any_sync(FULL_MASK, contrib)) {
-                        const float s = warp_sum8_transposed(v);
-                        float s8 = v8;
+                        if (__any_sync(FULL_MASK, contrib)) {
+                            const float s = warp_sum8_transposed(v);
+                            float s8 = v8;
 #pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) s8 += __shfl_xor_sync(FULL_MASK, s8, o);
-                        const uint32_t pair = ps[j];
-                        if ((lane & 3) == 0 && s != 0.0f) atomicAdd(sg8f + (size_t)pair * 8 + (lane >> 2), s);
-                        if (lane == 0 && s8 != 0.0f) atomicAdd(a.sg1 + pair, s8);
+                            for (int o = 16; o > 0; o >>= 1) s8 += __shfl_xor_sync(FULL_MASK, s8, o);
+                            const uint32_t pair = ps[j];
+                            if ((lane & 3) == 0 && s != 0.0f) atomicAdd(sg8f + (size_t)pair * 8 + (lane >> 2), s);
+                            if (lane == 0 && s8 != 0.0f) atomicAdd(a.sg1 + pair, s8);
+                        }
                     }
                 }
             }

@@ -234,18 +234,24 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
 }
 
 // ---------------------------------------------------------------------------------
-// Key-instance emission.  Chunks of EM_CHUNK depth-sorted pairs: (1) per-chunk sums of
-// the pairs' tile counts, (2) one block scans the chunk sums and fixes the segment's
-// size (clamped to the capacity, with the overflow flag set), (3) each chunk rescans
-// its counts and expands them: consecutive threads write consecutive instances (a
-// binary search over the chunk's offsets finds the pair), so the writes coalesce even
-// when one splat covers hundreds of tiles.
+// Key-instance emission.  Depth-sorted pairs are taken in chunks of EM_CHUNK:
+// (1) per-chunk sums of the pairs' tile counts; (2) one block scans the chunk sums and
+// fixes the segment's size (clamped to the capacity, with the overflow flag set);
+// (3) each chunk rescans its counts, writes every pair's first-instance offset, and
+// marks, for every EM_OUT-th instance, the pair it belongs to; (4) the expansion walks
+// the instances in equal blocks of EM_OUT: a block reads its first and last pair from
+// the marks, stages their offsets, ids and rectangles in shared memory, and each thread
+// binary-searches its instance's pair there.  Work per block is fixed however many
+// tiles a splat covers (one splat can cover thousands), and consecutive threads write
+// consecutive instances.
 // ---------------------------------------------------------------------------------
 constexpr int EM_THREADS = 256;
 constexpr int EM_ITEMS = 8;
 constexpr int EM_CHUNK = EM_THREADS * EM_ITEMS;
+constexpr int EM_OUT = 2048;
 
 int emit_chunk_items() { return EM_CHUNK; }
+int emit_out_items() { return EM_OUT; }
 
 __device__ __forceinline__ uint32_t rect_count(uint2 r) {
     const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu, y1 = r.y >> 16;
@@ -298,51 +304,73 @@ __global__ void __launch_bounds__(1024) emit_scan(EmitArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(EM_THREADS) emit_write(EmitArgs a) {
-    __shared__ uint32_t s_off[EM_CHUNK + 1];
-    __shared__ uint32_t s_pair[EM_CHUNK];
-    __shared__ uint2 s_rect[EM_CHUNK];
+__global__ void __launch_bounds__(EM_THREADS) emit_offsets(EmitArgs a) {
+    __shared__ uint32_t s_cnt[EM_CHUNK];
     __shared__ uint32_t s_tmp[32];
     const uint32_t M = *a.visible;
     const uint32_t base = a.pair_seg->base;
     const uint32_t chunks = (M + EM_CHUNK - 1) / EM_CHUNK;
-    const uint32_t inst_base = a.inst_seg->base;
-    const unsigned long long limit = a.inst_seg->count;  // instances of this segment that fit
+    const uint32_t total = a.inst_seg->count;
     for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
         const uint32_t first = c * EM_CHUNK;
-        const uint32_t items = min((uint32_t)EM_CHUNK, M - first);
         for (uint32_t j = threadIdx.x; j < EM_CHUNK; j += EM_THREADS) {
-            uint32_t pair = 0;
-            uint2 r = make_uint2(0u, 0u);
-            if (j < items) {
-                pair = __ldg(a.sorted_pairs + base + first + j);
-                r = a.rect[pair];
-            }
-            s_pair[j] = pair;
-            s_rect[j] = r;
+            const uint32_t s = first + j;
+            s_cnt[j] = s < M ? rect_count(a.rect[__ldg(a.sorted_pairs + base + s)]) : 0u;
         }
         __syncthreads();
         uint32_t cnt[EM_ITEMS];
         uint32_t local = 0;
 #pragma unroll
         for (int j = 0; j < EM_ITEMS; j++) {
-            cnt[j] = rect_count(s_rect[threadIdx.x * EM_ITEMS + j]);
+            cnt[j] = s_cnt[threadIdx.x * EM_ITEMS + j];
             local += cnt[j];
         }
         uint32_t tot;
         uint32_t run = block_excl_scan<EM_THREADS>(local, s_tmp, tot) + a.block_sums[c];
 #pragma unroll
         for (int j = 0; j < EM_ITEMS; j++) {
-            s_off[threadIdx.x * EM_ITEMS + j] = run;
+            const uint32_t s = first + threadIdx.x * EM_ITEMS + j;
+            if (s < M) {
+                a.pair_offsets[s] = run;
+                // Instances run, run + 1, ..., run + cnt - 1 belong to pair s: mark the
+                // expansion blocks that start inside that range.
+                uint32_t b = (run + EM_OUT - 1) / EM_OUT;
+                const uint32_t end = min(run + cnt[j], total);
+                for (; (unsigned long long)b * EM_OUT < end; b++) a.block_first_pair[b] = s;
+            }
             run += cnt[j];
         }
-        if (threadIdx.x == 0) s_off[EM_CHUNK] = a.block_sums[c] + tot;
         __syncthreads();
-        const uint32_t o_begin = s_off[0], o_end = s_off[EM_CHUNK];
-        for (uint32_t o = o_begin + threadIdx.x; o < o_end; o += EM_THREADS) {
-            if ((unsigned long long)o >= limit) break;
-            // Largest idx with s_off[idx] <= o among [0, items).
-            uint32_t lo = 0, hi = items - 1;
+    }
+}
+
+__global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
+    __shared__ uint32_t s_off[EM_OUT + 1];
+    __shared__ uint32_t s_pair[EM_OUT + 1];
+    __shared__ uint2 s_rect[EM_OUT + 1];
+    const uint32_t M = *a.visible;
+    const uint32_t base = a.pair_seg->base;
+    const uint32_t inst_base = a.inst_seg->base;
+    const uint32_t total = a.inst_seg->count;
+    const uint32_t blocks = (total + EM_OUT - 1) / EM_OUT;
+    for (uint32_t b = blockIdx.x; b < blocks; b += gridDim.x) {
+        const uint32_t o0 = b * EM_OUT;
+        const uint32_t o1 = min(o0 + EM_OUT, total);
+        const uint32_t p_lo = a.block_first_pair[b];
+        const uint32_t p_hi = (b + 1 < blocks) ? a.block_first_pair[b + 1] : M - 1;
+        // Every pair after p_lo starts after o0 and holds >= 1 instance, so the block
+        // needs at most EM_OUT + 1 pairs (the bound matters for the last block when the
+        // capacity clamped the instance count).
+        const uint32_t np = min(p_hi - p_lo + 1, (uint32_t)EM_OUT + 1);
+        for (uint32_t j = threadIdx.x; j < np; j += EM_THREADS) {
+            const uint32_t pair = __ldg(a.sorted_pairs + base + p_lo + j);
+            s_off[j] = a.pair_offsets[p_lo + j];
+            s_pair[j] = pair;
+            s_rect[j] = a.rect[pair];
+        }
+        __syncthreads();
+        for (uint32_t o = o0 + threadIdx.x; o < o1; o += EM_THREADS) {
+            uint32_t lo = 0, hi = np - 1;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi + 1) >> 1;
                 if (s_off[mid] <= o) lo = mid;
@@ -367,7 +395,8 @@ void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms) {
     if (grid > a.max_chunks) grid = a.max_chunks > 0 ? a.max_chunks : 1;
     emit_reduce<<<grid, EM_THREADS, 0, s>>>(a);
     emit_scan<<<1, 1024, 0, s>>>(a);
-    emit_write<<<grid, EM_THREADS, 0, s>>>(a);
+    emit_offsets<<<grid, EM_THREADS, 0, s>>>(a);
+    emit_expand<<<num_sms * 4, EM_THREADS, 0, s>>>(a);
 }
 
 // ---------------------------------------------------------------------------------
