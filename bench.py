@@ -55,7 +55,7 @@ class Clocks:
             os.close(fd)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -185,6 +185,7 @@ def run_b200(args, rank, local, world, dist):
     tuned = r.autotune()
     clocks = Clocks(device)
     clocks.start()
+    time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
     t_b = timed(r, args.steps, args.warmup)
     res["clocks"] = clocks.stop()
     stages = r.stage_times()
@@ -268,7 +269,7 @@ def roofline(res, peaks):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-plain", action="store_true")
@@ -316,7 +317,9 @@ def main():
             warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True, scaling="weak",
             vs_baseline=None, dtype="f32", data="synthetic",
             config=dict(workload=WORKLOAD, gaussians=res["n"], views=res["V"], pixels=res["pixels"], sh_degree=3,
-                        near=0.01, ssim_lambda=0.2, window="11-tap gaussian", raster_batch=res["tuned"],
+                        near=0.01, ssim_lambda=0.2, window="11-tap gaussian",
+                        raster_variant=dict(fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1]),
+                                            bwd=dict(batch=res["tuned"]["bwd"][0], pixels_per_thread=res["tuned"]["bwd"][1])),
                         l2="inputs larger than L2: params+moments+grads 944 MB, pair records 384 MB per step",
                         parallelism=f"dp{world} over views (own 8 views per GPU)"),
             plain_steps_per_s=round(res["plain"], 4) if res["plain"] else None,

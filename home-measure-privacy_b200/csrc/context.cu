@@ -136,8 +136,8 @@ struct GsContext {
     // last forward
     int last_first = -1, last_count = 0, last_batched = 1;
     bool have_loss = false;
-    // raster tuning
-    int raster_batch = 256;
+    // raster tuning: shared-memory batch and pixels per thread of each kernel
+    int batch_fwd = 256, batch_bwd = 256, ppt_fwd = 1, ppt_bwd = 1;
     int ctas_fwd = 0, ctas_bwd = 0;
     // graphs
     int64_t generation = 0;
@@ -395,7 +395,8 @@ static int size_instances(GsContext* c, int64_t cap) {
 static SegInfo* seg_ptr(GsContext* c, int idx) { return c->segs.as<SegInfo>() + idx; }
 
 static int persistent_ctas(GsContext* c, bool backward) {
-    const int per_sm = raster_max_ctas_per_sm(c->raster_batch, backward);
+    const int per_sm = backward ? raster_max_ctas_per_sm(c->batch_bwd, c->ppt_bwd, true)
+                                : raster_max_ctas_per_sm(c->batch_fwd, c->ppt_fwd, false);
     return c->num_sms * per_sm;
 }
 
@@ -485,7 +486,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ra.end_bit = 31;
     ra.hist = c->hist.as<uint32_t>();
     ra.totals = c->totals.as<uint32_t>();
-    ra.max_parts = (int)(c->hist.bytes / 4 / 256);
+    ra.max_parts = (int)(((int64_t)vcount * c->n_pad + radix_tile_items() - 1) / radix_tile_items());
     launch_radix_sort(ra, c->stream, c->num_sms);
     count_launches(c, ST_SORT_PAIRS, 3 * radix_sort_passes(0, 31));
     // Key instances in depth order.
@@ -522,6 +523,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     rb.seg = inst_seg;
     rb.begin_bit = 0;
     rb.end_bit = c->tile_bits;
+    rb.max_parts = (int)((c->inst_cap + radix_tile_items() - 1) / radix_tile_items());
     launch_radix_sort(rb, c->stream, c->num_sms);
     launch_ranges(c->ikeys.as<uint32_t>(), inst_seg, c->ranges.as<uint2>(), c->stream, c->num_sms);
     count_launches(c, ST_SORT_INST, 3 * radix_sort_passes(0, c->tile_bits) + 1);
@@ -537,7 +539,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
         r.work_counter = &st->work_counter;
     }
     CKI(mark(c, ST_RASTER_FWD));
-    launch_raster_fwd(r, c->raster_batch, batched ? c->ctas_fwd : 0, c->stream);
+    launch_raster_fwd(r, c->batch_fwd, c->ppt_fwd, batched ? c->ctas_fwd : 0, c->stream);
     count_launches(c, ST_RASTER_FWD, 1);
     CK(cudaGetLastError());
     return GS_OK;
@@ -584,7 +586,7 @@ static int enqueue_backward_view(GsContext* c, int first, int step_first, int co
         r.work_counter = &st->work_counter_bwd;
         if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
     }
-    launch_raster_bwd(r, c->raster_batch, batched ? c->ctas_bwd : 0, c->stream);
+    launch_raster_bwd(r, c->batch_bwd, c->ppt_bwd, batched ? c->ctas_bwd : 0, c->stream);
     count_launches(c, ST_RASTER_BWD, 1);
     CKI(mark(c, ST_PROJECT_BWD));
     ProjectBwdArgs pb;
@@ -815,6 +817,7 @@ void gs_config_default(GsConfig* cfg) {
     cfg->device = 0;
     cfg->autotune = 0;
     cfg->raster_batch = 256;
+    cfg->raster_ppt = 1;
     cfg->lpt_order = 1;
 }
 
@@ -866,6 +869,8 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if (cfg.rect_mode < 0 || cfg.rect_mode > 1) return fail(GS_ERR_INVALID_ARG, "rect_mode must be 0 or 1");
     if (cfg.raster_batch != 64 && cfg.raster_batch != 128 && cfg.raster_batch != 256)
         return fail(GS_ERR_INVALID_ARG, "raster_batch must be 64, 128 or 256");
+    if (cfg.raster_ppt == 0) cfg.raster_ppt = 1;
+    if (cfg.raster_ppt != 1 && cfg.raster_ppt != 2) return fail(GS_ERR_INVALID_ARG, "raster_ppt must be 1 or 2");
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) {
@@ -884,7 +889,8 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     c->device_name = prop.name;
     c->degree = cfg.sh_degree;
     c->planes = num_planes(cfg.sh_degree);
-    c->raster_batch = cfg.raster_batch;
+    c->batch_fwd = c->batch_bwd = cfg.raster_batch;
+    c->ppt_fwd = c->ppt_bwd = cfg.raster_ppt;
     int rc = GS_OK;
     auto bail = [&](int r) {
         gs_destroy(c);
@@ -1585,14 +1591,17 @@ int gs_get_stats(GsContext* c, GsStats* out) {
         out->pixels = b.pixel_offset + (int64_t)b.width * b.height - a.pixel_offset;
     }
     out->kernel_launches_per_step = c->last_step_launches;
-    out->raster_batch = c->raster_batch;
-    out->raster_threads = 256;
+    out->raster_batch = c->batch_bwd;
+    out->raster_threads = 256 / c->ppt_bwd;
+    out->raster_variant = c->batch_fwd | (c->ppt_fwd << 12) | (c->batch_bwd << 16) | (c->ppt_bwd << 28);
     out->overflow = (int32_t)c->skipped_steps;
     return GS_OK;
 }
 
-// Raster tuning: times the persistent forward + backward raster for each shared-memory
-// batch size on all training views (after one forward and loss) and keeps the fastest.
+// Raster tuning: times the persistent forward and backward raster kernels, each for every
+// (shared-memory batch, pixels per thread) variant, on all training views after one
+// forward and loss, and keeps the fastest of each.  The choice is cached per device and
+// workload in `cache_path` (lines "key|fwd_batch fwd_ppt bwd_batch bwd_ppt").
 int gs_autotune(GsContext* c, const char* cache_path) {
     CTX_CHECK(c);
     if (c->V < 1 || c->n <= 0) return fail(GS_ERR_STATE, "autotune needs Gaussians and views");
@@ -1601,21 +1610,29 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     char key[256];
     snprintf(key, sizeof key, "%s n=%d views=%d px=%lld deg=%d", c->device_name.c_str(), c->n, c->V,
              (long long)c->total_pixels, c->degree);
+    auto apply = [&](int bf, int pf, int bb, int pb) {
+        c->batch_fwd = bf;
+        c->ppt_fwd = pf;
+        c->batch_bwd = bb;
+        c->ppt_bwd = pb;
+        c->ctas_fwd = persistent_ctas(c, false);
+        c->ctas_bwd = persistent_ctas(c, true);
+        drop_graphs(c);
+    };
     if (cache_path) {
         FILE* f = fopen(cache_path, "r");
         if (f) {
             char line[512];
             while (fgets(line, sizeof line, f)) {
-                int b = 0;
+                int bf, pf, bb, pb;
                 char* bar = strrchr(line, '|');
                 if (!bar) continue;
                 *bar = 0;
-                if (strcmp(line, key) == 0 && sscanf(bar + 1, "%d", &b) == 1 && (b == 64 || b == 128 || b == 256)) {
+                if (strcmp(line, key) == 0 && sscanf(bar + 1, "%d %d %d %d", &bf, &pf, &bb, &pb) == 4 &&
+                    (bf == 64 || bf == 128 || bf == 256) && (bb == 64 || bb == 128 || bb == 256) &&
+                    (pf == 1 || pf == 2) && (pb == 1 || pb == 2)) {
                     fclose(f);
-                    c->raster_batch = b;
-                    c->ctas_fwd = persistent_ctas(c, false);
-                    c->ctas_bwd = persistent_ctas(c, true);
-                    drop_graphs(c);
+                    apply(bf, pf, bb, pb);
                     return GS_OK;
                 }
             }
@@ -1630,45 +1647,54 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     GsLossConfig lc{0.2f, 1};
     CKI(gs_loss(c, &lc, nullptr));
     DevStatus* st = c->status.as<DevStatus>();
-    const int cands[3] = {64, 128, 256};
-    float best = 1e30f;
-    int best_b = c->raster_batch;
-    for (int ci = 0; ci < 3; ci++) {
-        c->raster_batch = cands[ci];
-        const int cf = persistent_ctas(c, false), cb = persistent_ctas(c, true);
-        RasterArgs r = raster_args(c, 0, c->V);
-        if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
-        float total = 0.f;
-        for (int rep = 0; rep < 4; rep++) {
-            CK(cudaMemsetAsync(&st->work_counter, 0, 8, c->stream));
-            CK(cudaMemsetAsync(c->sg8.p, 0, (size_t)c->V * c->n_pad * 32, c->stream));
-            CK(cudaMemsetAsync(c->sg1.p, 0, (size_t)c->V * c->n_pad * 4, c->stream));
-            CK(cudaEventRecord(c->user_events[62], c->stream));
-            r.work_counter = &st->work_counter;
-            launch_raster_fwd(r, c->raster_batch, cf, c->stream);
-            r.work_counter = &st->work_counter_bwd;
-            launch_raster_bwd(r, c->raster_batch, cb, c->stream);
-            CK(cudaEventRecord(c->user_events[63], c->stream));
-            CK(cudaGetLastError());
-            CK(cudaEventSynchronize(c->user_events[63]));
-            float ms = 0.f;
-            CK(cudaEventElapsedTime(&ms, c->user_events[62], c->user_events[63]));
-            if (rep > 0) total += ms;
-        }
-        if (total < best) {
-            best = total;
-            best_b = cands[ci];
-        }
-    }
-    c->raster_batch = best_b;
-    c->ctas_fwd = persistent_ctas(c, false);
-    c->ctas_bwd = persistent_ctas(c, true);
+    const int batches[3] = {64, 128, 256};
+    float best_f = 1e30f, best_b = 1e30f;
+    int bf = c->batch_fwd, pf = c->ppt_fwd, bb = c->batch_bwd, pb = c->ppt_bwd;
+    RasterArgs r = raster_args(c, 0, c->V);
+    if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
+    for (int bi = 0; bi < 3; bi++)
+        for (int ppt = 1; ppt <= 2; ppt++)
+            for (int backward = 0; backward < 2; backward++) {
+                const int ctas = c->num_sms * raster_max_ctas_per_sm(batches[bi], ppt, backward != 0);
+                float total = 0.f;
+                for (int rep = 0; rep < 3; rep++) {
+                    CK(cudaMemsetAsync(&st->work_counter, 0, 8, c->stream));
+                    if (backward) {
+                        CK(cudaMemsetAsync(c->sg8.p, 0, (size_t)c->V * c->n_pad * 32, c->stream));
+                        CK(cudaMemsetAsync(c->sg1.p, 0, (size_t)c->V * c->n_pad * 4, c->stream));
+                    }
+                    CK(cudaEventRecord(c->user_events[62], c->stream));
+                    if (backward) {
+                        r.work_counter = &st->work_counter_bwd;
+                        launch_raster_bwd(r, batches[bi], ppt, ctas, c->stream);
+                    } else {
+                        r.work_counter = &st->work_counter;
+                        launch_raster_fwd(r, batches[bi], ppt, ctas, c->stream);
+                    }
+                    CK(cudaEventRecord(c->user_events[63], c->stream));
+                    CK(cudaGetLastError());
+                    CK(cudaEventSynchronize(c->user_events[63]));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, c->user_events[62], c->user_events[63]));
+                    if (rep > 0) total += ms;
+                }
+                if (backward && total < best_b) {
+                    best_b = total;
+                    bb = batches[bi];
+                    pb = ppt;
+                }
+                if (!backward && total < best_f) {
+                    best_f = total;
+                    bf = batches[bi];
+                    pf = ppt;
+                }
+            }
+    apply(bf, pf, bb, pb);
     c->have_loss = false;
-    drop_graphs(c);
     if (cache_path) {
         FILE* f = fopen(cache_path, "a");
         if (f) {
-            fprintf(f, "%s|%d\n", key, best_b);
+            fprintf(f, "%s|%d %d %d %d\n", key, bf, pf, bb, pb);
             fclose(f);
         }
     }

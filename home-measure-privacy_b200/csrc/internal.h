@@ -110,9 +110,9 @@ struct RasterArgs {
     unsigned int* work_counter;     // persistent queue head (nullptr = one CTA per tile)
     const uint32_t* tile_order;     // optional permutation of the tiles (heavy first)
 };
-void launch_raster_fwd(const RasterArgs& a, int batch, int persistent_ctas, cudaStream_t s);
-void launch_raster_bwd(const RasterArgs& a, int batch, int persistent_ctas, cudaStream_t s);
-int raster_max_ctas_per_sm(int batch, bool backward);
+void launch_raster_fwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s);
+void launch_raster_bwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s);
+int raster_max_ctas_per_sm(int batch, int ppt, bool backward);
 
 // Tiles ordered by descending list length (for the persistent queue).
 void launch_tile_order(const uint2* ranges, int tile_first, int num_tiles, uint32_t* order,

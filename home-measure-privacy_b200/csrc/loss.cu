@@ -76,6 +76,8 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
     const float n = (float)((long long)W * H * 3);
     const int winx = W - 2 * R, winy = H - 2 * R;
     const float windows = (winx > 0 && winy > 0) ? (float)winx * (float)winy * 3.0f : 0.0f;
+    const float l1_scale = (1.0f - a.lambda) / n;
+    const float ssim_scale = windows > 0.0f ? a.lambda / windows : 0.0f;
     const bool use_ssim = a.lambda > 0.0f && windows > 0.0f;
     // Filter taps stay in the kernel-parameter constant bank (FFMA operands).
     const float* w = wts.w;
@@ -168,10 +170,12 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
                         const float a2 = 2.0f * (sxy - mx * my) + C2;
                         const float b1 = mx * mx + my * my + C1;
                         const float b2 = (sxx - mx * mx) + (syy - my * my) + C2;
-                        const float ssim = a1 * a2 / (b1 * b2);
-                        ca = ssim * (2.0f * my / a1 - 2.0f * my / a2 - 2.0f * mx / b1 + 2.0f * mx / b2);
-                        cb = -ssim / b2;
-                        cd = 2.0f * ssim / a2;
+                        const float ia1 = __frcp_rn(a1), ia2 = __frcp_rn(a2);
+                        const float ib1 = __frcp_rn(b1), ib2 = __frcp_rn(b2);
+                        const float ssim = a1 * a2 * ib1 * ib2;
+                        ca = 2.0f * ssim * (my * ia1 - my * ia2 - mx * ib1 + mx * ib2);
+                        cb = -ssim * ib2;
+                        cd = 2.0f * ssim * ia2;
                         if (gx >= bx0 && gx < bx0 + LB_W && gy >= by0 && gy < by0 + LB_H) ssim_sum += ssim;
                     }
                     const int o = hr * D::HW + hc;
@@ -226,7 +230,7 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
                     yv = load_target<TT>(target, q);
                 }
                 const float diff = xv - yv;
-                float g = (1.0f - a.lambda) * (float)((diff > 0.f) - (diff < 0.f)) / n;
+                float g = l1_scale * (float)((diff > 0.f) - (diff < 0.f));
                 l1 += fabsf(diff);
                 if (use_ssim) {
                     float sa = 0.f, sb = 0.f, sd = 0.f;
@@ -236,7 +240,7 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
                         sb += w[t] * hc[1][k + t];
                         sd += w[t] * hc[2][k + t];
                     }
-                    g -= a.lambda * ((sa + 2.0f * xv * sb + yv * sd) / windows);
+                    g -= ssim_scale * (sa + 2.0f * xv * sb + yv * sd);
                 }
                 a.dl[q] = g;
             }

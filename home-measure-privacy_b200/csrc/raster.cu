@@ -38,19 +38,23 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+// Thread -> pixels.  With PPT pixels per thread the CTA has 256 / PPT threads; warp w
+// covers an 8 x (4 PPT) block of the 16 x 16 tile (a squarer footprint than full rows,
+// so fewer splats reach each warp); lane l owns x = l & 7, y = l >> 3 (+ 4 p for its
+// p-th pixel).
+template <int PPT>
 struct TileInfo {
-    int g;               // global tile id
-    int x, y;            // this thread's pixel
+    int g;                     // global tile id
+    int x, y[PPT];             // this thread's pixels
     int width, height;
     int pixel_offset;
-    bool inside;
+    bool inside[PPT];
     float wx0, wx1, wy0, wy1;  // pixel-centre rectangle of this thread's warp
 };
 
-// Thread -> pixel: warp w covers an 8 x 4 block (w & 1, w >> 1) of the 16 x 16 tile,
-// a squarer footprint than two 16-pixel rows, so fewer splats reach each warp.
-__device__ __forceinline__ TileInfo tile_info(const RasterArgs& a, int item) {
-    TileInfo ti;
+template <int PPT>
+__device__ __forceinline__ TileInfo<PPT> tile_info(const RasterArgs& a, int item) {
+    TileInfo<PPT> ti;
     const int local = a.tile_order ? (int)a.tile_order[item] : item;
     ti.g = a.tile_first + local;
     int vi = a.view_first;
@@ -60,17 +64,20 @@ __device__ __forceinline__ TileInfo tile_info(const RasterArgs& a, int item) {
     const int lt = ti.g - vw.tile_offset;
     const int tx = lt % vw.tiles_x, ty = lt / vw.tiles_x;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bx = tx * GS_TILE + (w & 1) * 8, by = ty * GS_TILE + (w >> 1) * 4;
+    const int bx = tx * GS_TILE + (w & 1) * 8, by = ty * GS_TILE + (w >> 1) * 4 * PPT;
     ti.x = bx + (lane & 7);
-    ti.y = by + (lane >> 3);
+#pragma unroll
+    for (int p = 0; p < PPT; p++) {
+        ti.y[p] = by + (lane >> 3) + 4 * p;
+        ti.inside[p] = ti.x < vw.width && ti.y[p] < vw.height;
+    }
     ti.width = vw.width;
     ti.height = vw.height;
     ti.pixel_offset = vw.pixel_offset;
-    ti.inside = ti.x < vw.width && ti.y < vw.height;
     ti.wx0 = (float)bx + 0.5f;
     ti.wx1 = (float)bx + 7.5f;
     ti.wy0 = (float)by + 0.5f;
-    ti.wy1 = (float)by + 3.5f;
+    ti.wy1 = (float)(by + 4 * PPT) - 0.5f;
     return ti;
 }
 
@@ -83,7 +90,6 @@ __device__ __forceinline__ int next_item(unsigned int* counter, int* s_item, int
     return *s_item;
 }
 
-template <int BATCH>
 __device__ __forceinline__ void stage_batch(const RasterArgs& a, uint32_t first, int cnt, bool reverse,
                                             float4* s_g0, float4* s_g1, float4* s_c, uint32_t* s_pair) {
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
@@ -97,14 +103,49 @@ __device__ __forceinline__ void stage_batch(const RasterArgs& a, uint32_t first,
     cp_async_commit();
 }
 
-// After the batch's copies landed: each staging thread replaces the (unused here) depth
-// of its splats with the culling bound 2 ln(opacity / alpha_min) + slack: a pixel can
-// reach alpha >= alpha_min only where the conic's quadratic form is below it.
-__device__ __forceinline__ void prepare_batch(int cnt, float4* s_g1, float log_amin) {
+constexpr float LOG2E = 1.4426950408889634f;
+constexpr float ALPHA_Q_BAND = 1e-4f;  // |q - log2(alpha_min)| below this: reference formula
+
+// After the batch's copies landed, each staging thread derives for its splats:
+// s_g1.w = the culling bound 2 ln(opacity / alpha_min) + slack (a pixel can reach
+// alpha >= alpha_min only where the conic's quadratic form is below it), and
+// s_q = (-A/2, -B, -C/2) log2(e) and log2(opacity), so that alpha = 2^q with
+// q = log2(op) + qa dx^2 + qb dx dy + qc dy^2.
+__device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g1, float4* s_q, float log_amin) {
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-        const float op = s_g1[t].y;
+        const float4 g0 = s_g0[t];
+        const float4 g1 = s_g1[t];
+        const float op = g1.y;
         s_g1[t].w = op > 0.f ? 2.0f * (__logf(op) - log_amin) + 1e-3f : -1.0f;
+        s_q[t] = make_float4(-0.5f * LOG2E * g0.z, -LOG2E * g0.w, -0.5f * LOG2E * g1.x,
+                             op > 0.f ? __log2f(op) : -1e30f);
     }
+}
+
+// alpha of splat (g0, g1, q) at offset (dx, dy), or 0 when the pixel skips it:
+// alphaAt (trainer/gpu.js:91-103).  2^q by the fast exp2; within ALPHA_Q_BAND of the
+// alpha_min threshold the reference expression min(0.99, op exp(power)) decides, so
+// skip decisions match the reference's.  Explicit rounding intrinsics keep forward and
+// backward bit-identical.
+__device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, float dx, float dy,
+                                          float amax, float amin, float qlo, float qhi) {
+    if (fabsf(dx) > g1.z || fabsf(dy) > g1.z) return 0.f;
+    const float t = __fmaf_rn(q.y, dy, __fmul_rn(q.x, dx));
+    float e = __fmaf_rn(dx, t, q.w);
+    e = __fmaf_rn(__fmul_rn(q.z, dy), dy, e);
+    if (e < qlo) return 0.f;
+    float alpha;
+    if (e < qhi) {
+        const float power = __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(__fmul_rn(__fmul_rn(g0.z, dx), dx),
+                                                                 __fmul_rn(__fmul_rn(g1.x, dy), dy))),
+                                      __fmul_rn(__fmul_rn(g0.w, dx), dy));
+        if (power > 0.f) return 0.f;
+        alpha = __fmul_rn(g1.y, expf(power));
+        if (alpha < amin) return 0.f;
+    } else {
+        alpha = exp2f(e);
+    }
+    return fminf(amax, alpha);
 }
 
 // Smallest value of the conic's quadratic form A dx^2 + 2 B dx dy + C dy^2 over the box
@@ -124,7 +165,8 @@ __device__ __forceinline__ float qmin_box(float A, float B, float C, float xl, f
 // Can splat (g0, g1) give any pixel centre of the warp's rectangle alpha >= alpha_min?
 // Conservative: the pixels' own tests (bounding box, then alpha) decide; this only
 // skips splats that cannot pass them anywhere in the rectangle.
-__device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1, const TileInfo& ti) {
+template <int PPT>
+__device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1, const TileInfo<PPT>& ti) {
     const float r = g1.z;
     const float xl = fmaxf(ti.wx0, g0.x - r), xh = fminf(ti.wx1, g0.x + r);
     const float yl = fmaxf(ti.wy0, g0.y - r), yh = fminf(ti.wy1, g0.y + r);
@@ -132,81 +174,103 @@ __device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1,
     return qmin_box(g0.z, g0.w, g1.x, xl - g0.x, xh - g0.x, yl - g0.y, yh - g0.y) <= g1.w;
 }
 
-template <int BATCH>
-__global__ void __launch_bounds__(256) raster_fwd_kernel(RasterArgs a) {
+template <int BATCH, int PPT>
+__global__ void __launch_bounds__(256 / PPT) raster_fwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
+    __shared__ __align__(16) float4 s_q[2][BATCH];
     __shared__ int s_item;
     const int lane = threadIdx.x & 31;
     const float log_amin = __logf(a.alpha_min);
+    const float qthr = __log2f(a.alpha_min);
+    const float qlo = qthr - ALPHA_Q_BAND, qhi = qthr + ALPHA_Q_BAND;
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
-        const TileInfo ti = tile_info(a, item);
+        const TileInfo<PPT> ti = tile_info<PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x, end = rg.y;
-        const float pxf = (float)ti.x + 0.5f, pyf = (float)ti.y + 0.5f;
-        float T = 1.0f, cr = 0.f, cg = 0.f, cb = 0.f;
-        uint32_t last = start;
-        bool done = !ti.inside;
+        const float pxf = (float)ti.x + 0.5f;
+        float pyf[PPT], T[PPT], cr[PPT], cg[PPT], cb[PPT];
+        uint32_t last[PPT];
+        bool done[PPT];
+#pragma unroll
+        for (int p = 0; p < PPT; p++) {
+            pyf[p] = (float)ti.y[p] + 0.5f;
+            T[p] = 1.0f;
+            cr[p] = cg[p] = cb[p] = 0.f;
+            last[p] = start;
+            done[p] = !ti.inside[p];
+        }
         int buf = 0;
-        if (start < end) stage_batch<BATCH>(a, start, min((uint32_t)BATCH, end - start), false, s_g0[0], s_g1[0], s_c[0], nullptr);
+        if (start < end) stage_batch(a, start, min((uint32_t)BATCH, end - start), false, s_g0[0], s_g1[0], s_c[0], nullptr);
         for (uint32_t b0 = start; b0 < end; b0 += BATCH) {
             const int cnt = (int)min((uint32_t)BATCH, end - b0);
             const uint32_t nb = b0 + BATCH;
             if (nb < end) {
-                stage_batch<BATCH>(a, nb, min((uint32_t)BATCH, end - nb), false, s_g0[buf ^ 1], s_g1[buf ^ 1],
-                                   s_c[buf ^ 1], nullptr);
+                stage_batch(a, nb, min((uint32_t)BATCH, end - nb), false, s_g0[buf ^ 1], s_g1[buf ^ 1], s_c[buf ^ 1],
+                            nullptr);
                 cp_async_wait<1>();
             } else {
                 cp_async_wait<0>();
             }
-            prepare_batch(cnt, s_g1[buf], log_amin);
+            prepare_batch(cnt, s_g0[buf], s_g1[buf], s_q[buf], log_amin);
             __syncthreads();
             const float4* g0s = s_g0[buf];
             const float4* g1s = s_g1[buf];
             const float4* cs = s_c[buf];
-            bool warp_done = __all_sync(FULL_MASK, done);
+            const float4* qs = s_q[buf];
+            bool all_done = true;
+#pragma unroll
+            for (int p = 0; p < PPT; p++) all_done = all_done && done[p];
+            bool warp_done = __all_sync(FULL_MASK, all_done);
             for (int gb = 0; gb < cnt && !warp_done; gb += 32) {
                 const int jl = gb + lane;
-                const bool rel = jl < cnt && warp_reaches(g0s[jl], g1s[jl], ti);
+                const bool rel = jl < cnt && warp_reaches<PPT>(g0s[jl], g1s[jl], ti);
                 uint32_t mask = __ballot_sync(FULL_MASK, rel);
                 while (mask) {
                     const int j = gb + __ffs(mask) - 1;
                     mask &= mask - 1;
-                    if (done) continue;
                     const float4 g0 = g0s[j];
                     const float4 g1 = g1s[j];
-                    const float dx = pxf - g0.x, dy = pyf - g0.y;
-                    if (fabsf(dx) > g1.z || fabsf(dy) > g1.z) continue;
-                    const float power = -0.5f * (g0.z * dx * dx + g1.x * dy * dy) - g0.w * dx * dy;
-                    if (power > 0.0f) continue;
-                    const float alpha = fminf(a.alpha_max, g1.y * expf(power));
-                    if (alpha < a.alpha_min) continue;
-                    const float4 c = cs[j];
-                    cr += c.x * alpha * T;
-                    cg += c.y * alpha * T;
-                    cb += c.z * alpha * T;
-                    T *= 1.0f - alpha;
-                    last = b0 + (uint32_t)j + 1u;
-                    if (T <= a.t_min) done = true;
+                    const float4 q = qs[j];
+                    const float dx = pxf - g0.x;
+#pragma unroll
+                    for (int p = 0; p < PPT; p++) {
+                        if (done[p]) continue;
+                        const float alpha = alpha_at(g0, g1, q, dx, pyf[p] - g0.y, a.alpha_max, a.alpha_min, qlo, qhi);
+                        if (alpha == 0.f) continue;
+                        const float4 c = cs[j];
+                        const float w = alpha * T[p];
+                        cr[p] += c.x * w;
+                        cg[p] += c.y * w;
+                        cb[p] += c.z * w;
+                        T[p] *= 1.0f - alpha;
+                        last[p] = b0 + (uint32_t)j + 1u;
+                        if (T[p] <= a.t_min) done[p] = true;
+                    }
                 }
-                warp_done = __all_sync(FULL_MASK, done);
+                all_done = true;
+#pragma unroll
+                for (int p = 0; p < PPT; p++) all_done = all_done && done[p];
+                warp_done = __all_sync(FULL_MASK, all_done);
             }
             buf ^= 1;
             // All pixels done: the rest of the list cannot change the tile.
-            if (__syncthreads_count(done) == (int)blockDim.x) {
+            if (__syncthreads_count(all_done) == (int)blockDim.x) {
                 cp_async_wait<0>();
                 break;
             }
         }
-        if (ti.inside) {
-            const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y * ti.width + ti.x;
-            a.image[pix * 3 + 0] = cr;
-            a.image[pix * 3 + 1] = cg;
-            a.image[pix * 3 + 2] = cb;
-            a.t_final[pix] = T;
-            a.last[pix] = last;
+#pragma unroll
+        for (int p = 0; p < PPT; p++) {
+            if (!ti.inside[p]) continue;
+            const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x;
+            a.image[pix * 3 + 0] = cr[p];
+            a.image[pix * 3 + 1] = cg[p];
+            a.image[pix * 3 + 2] = cb[p];
+            a.t_final[pix] = T[p];
+            a.last[pix] = last[p];
         }
         if (!a.work_counter) break;
         item = next_item(a.work_counter, &s_item, 0);
@@ -242,112 +306,122 @@ __device__ __forceinline__ float warp_sum8_transposed(float v[8]) {
     return v[0];
 }
 
-template <int BATCH>
-__global__ void __launch_bounds__(256) raster_bwd_kernel(RasterArgs a) {
+template <int BATCH, int PPT>
+__global__ void __launch_bounds__(256 / PPT) raster_bwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
+    __shared__ __align__(16) float4 s_q[2][BATCH];
     __shared__ uint32_t s_pair[2][BATCH];
     __shared__ int s_item;
     __shared__ unsigned int s_end;
     const int lane = threadIdx.x & 31;
     const float log_amin = __logf(a.alpha_min);
+    const float qthr = __log2f(a.alpha_min);
+    const float qlo = qthr - ALPHA_Q_BAND, qhi = qthr + ALPHA_Q_BAND;
     float* sg8f = reinterpret_cast<float*>(a.sg8);
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
-        const TileInfo ti = tile_info(a, item);
+        const TileInfo<PPT> ti = tile_info<PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
-        const float pxf = (float)ti.x + 0.5f, pyf = (float)ti.y + 0.5f;
-        float T = 0.f, dlr = 0.f, dlg = 0.f, dlb = 0.f;
-        uint32_t mylast = start;
-        if (ti.inside) {
-            const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y * ti.width + ti.x;
-            T = a.t_final[pix];
-            mylast = a.last[pix];
-            dlr = a.dl[pix * 3 + 0];
-            dlg = a.dl[pix * 3 + 1];
-            dlb = a.dl[pix * 3 + 2];
+        const float pxf = (float)ti.x + 0.5f;
+        float pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], br[PPT], bg[PPT], bb[PPT];
+        uint32_t mylast[PPT];
+        unsigned int tmax = start;
+#pragma unroll
+        for (int p = 0; p < PPT; p++) {
+            pyf[p] = (float)ti.y[p] + 0.5f;
+            T[p] = 0.f;
+            dlr[p] = dlg[p] = dlb[p] = 0.f;
+            br[p] = bg[p] = bb[p] = 0.f;  // colour of the splats behind, "behind"
+            mylast[p] = start;
+            if (ti.inside[p]) {
+                const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x;
+                T[p] = a.t_final[pix];
+                mylast[p] = a.last[pix];
+                dlr[p] = a.dl[pix * 3 + 0];
+                dlg[p] = a.dl[pix * 3 + 1];
+                dlb[p] = a.dl[pix * 3 + 2];
+            }
+            tmax = max(tmax, mylast[p]);
         }
         if (threadIdx.x == 0) s_end = start;
         __syncthreads();
         // Tile end = largest last of its pixels (BACKWARD_SG, trainer/gpu.js:247-253);
         // each warp also stops at its own largest last.
-        unsigned int wmax = mylast;
+        unsigned int wmax = tmax;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) wmax = max(wmax, __shfl_xor_sync(FULL_MASK, wmax, o));
         if (lane == 0) atomicMax(&s_end, wmax);
         __syncthreads();
         const uint32_t end = s_end;
-        float br = 0.f, bg = 0.f, bb = 0.f;  // colour of the splats behind, "behind"
         int buf = 0;
         if (end > start)
-            stage_batch<BATCH>(a, end, min((uint32_t)BATCH, end - start), true, s_g0[0], s_g1[0], s_c[0], s_pair[0]);
+            stage_batch(a, end, min((uint32_t)BATCH, end - start), true, s_g0[0], s_g1[0], s_c[0], s_pair[0]);
         for (uint32_t bend = end; bend > start;) {
             const uint32_t bstart = (bend - start > (uint32_t)BATCH) ? bend - BATCH : start;
             const int cnt = (int)(bend - bstart);
             if (bstart > start) {
-                stage_batch<BATCH>(a, bstart, min((uint32_t)BATCH, bstart - start), true, s_g0[buf ^ 1],
-                                   s_g1[buf ^ 1], s_c[buf ^ 1], s_pair[buf ^ 1]);
+                stage_batch(a, bstart, min((uint32_t)BATCH, bstart - start), true, s_g0[buf ^ 1], s_g1[buf ^ 1],
+                            s_c[buf ^ 1], s_pair[buf ^ 1]);
                 cp_async_wait<1>();
             } else {
                 cp_async_wait<0>();
             }
-            prepare_batch(cnt, s_g1[buf], log_amin);
+            prepare_batch(cnt, s_g0[buf], s_g1[buf], s_q[buf], log_amin);
             __syncthreads();
             const float4* g0s = s_g0[buf];
             const float4* g1s = s_g1[buf];
             const float4* cs = s_c[buf];
+            const float4* qs = s_q[buf];
             const uint32_t* ps = s_pair[buf];
             // Entry j of the batch is list position bend - 1 - j: ascending j walks back to
             // front.  Warps whose pixels all stopped before this batch skip it.
             if (bstart < wmax) {
                 for (int gb = 0; gb < cnt; gb += 32) {
                     const int jl = gb + lane;
-                    const bool rel = jl < cnt && (bend - 1 - (uint32_t)jl) < wmax && warp_reaches(g0s[jl], g1s[jl], ti);
+                    const bool rel = jl < cnt && (bend - 1 - (uint32_t)jl) < wmax && warp_reaches<PPT>(g0s[jl], g1s[jl], ti);
                     uint32_t mask = __ballot_sync(FULL_MASK, rel);
                     while (mask) {
                         const int j = gb + __ffs(mask) - 1;
                         mask &= mask - 1;
                         const uint32_t k = bend - 1 - (uint32_t)j;
+                        const float4 g0 = g0s[j];
+                        const float4 g1 = g1s[j];
+                        const float4 q = qs[j];
+                        const float dx = pxf - g0.x;
                         float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                         float v8 = 0.f;
                         bool contrib = false;
-                        if (ti.inside && k < mylast) {
-                            const float4 g0 = g0s[j];
-                            const float4 g1 = g1s[j];
-                            const float dx = pxf - g0.x, dy = pyf - g0.y;
-                            if (fabsf(dx) <= g1.z && fabsf(dy) <= g1.z) {
-                                const float power = -0.5f * (g0.z * dx * dx + g1.x * dy * dy) - g0.w * dx * dy;
-                                if (power <= 0.0f) {
-                                    const float alpha = fminf(a.alpha_max, g1.y * expf(power));
-                                    if (alpha >= a.alpha_min) {
-                                        contrib = true;
-                                        const float4 c = cs[j];
-                                        const float oma = 1.0f - alpha;
-                                        const float ioma = 1.0f / oma;
-                                        const float Tk = T * ioma;
-                                        v[0] = dlr * alpha * Tk;
-                                        v[1] = dlg * alpha * Tk;
-                                        v[2] = dlb * alpha * Tk;
-                                        const float dA = dlr * (Tk * c.x - br * ioma) + dlg * (Tk * c.y - bg * ioma) +
-                                                         dlb * (Tk * c.z - bb * ioma);
-                                        br += c.x * alpha * Tk;
-                                        bg += c.y * alpha * Tk;
-                                        bb += c.z * alpha * Tk;
-                                        T = Tk;
-                                        if (alpha < a.alpha_max) {
-                                            const float op = g1.y;
-                                            v[3] = dA * alpha * (1.0f - op);
-                                            const float dP = dA * alpha;
-                                            v[4] = dP * (g0.z * dx + g0.w * dy);
-                                            v[5] = dP * (g1.x * dy + g0.w * dx);
-                                            v[6] = dP * -0.5f * dx * dx;
-                                            v[7] = dP * -dx * dy;
-                                            v8 = dP * -0.5f * dy * dy;
-                                        }
-                                    }
-                                }
+#pragma unroll
+                        for (int p = 0; p < PPT; p++) {
+                            if (!(k < mylast[p])) continue;
+                            const float dy = pyf[p] - g0.y;
+                            const float alpha = alpha_at(g0, g1, q, dx, dy, a.alpha_max, a.alpha_min, qlo, qhi);
+                            if (alpha == 0.f) continue;
+                            contrib = true;
+                            const float4 c = cs[j];
+                            const float ioma = __frcp_rn(1.0f - alpha);
+                            const float Tk = T[p] * ioma;
+                            const float at = alpha * Tk;
+                            v[0] += dlr[p] * at;
+                            v[1] += dlg[p] * at;
+                            v[2] += dlb[p] * at;
+                            const float dA = dlr[p] * (Tk * c.x - br[p] * ioma) + dlg[p] * (Tk * c.y - bg[p] * ioma) +
+                                             dlb[p] * (Tk * c.z - bb[p] * ioma);
+                            br[p] += c.x * at;
+                            bg[p] += c.y * at;
+                            bb[p] += c.z * at;
+                            T[p] = Tk;
+                            if (alpha < a.alpha_max) {
+                                const float dP = dA * alpha;
+                                v[3] += dP * (1.0f - g1.y);
+                                v[4] += dP * (g0.z * dx + g0.w * dy);
+                                v[5] += dP * (g1.x * dy + g0.w * dx);
+                                v[6] += dP * -0.5f * dx * dx;
+                                v[7] += dP * -dx * dy;
+                                v8 += dP * -0.5f * dy * dy;
                             }
                         }
                         if (__any_sync(FULL_MASK, contrib)) {
@@ -371,53 +445,58 @@ __global__ void __launch_bounds__(256) raster_bwd_kernel(RasterArgs a) {
     }
 }
 
-template <int BATCH>
-static void fwd_dispatch(const RasterArgs& a, int ctas, cudaStream_t s) {
-    raster_fwd_kernel<BATCH><<<ctas, 256, 0, s>>>(a);
+// Variant = (shared-memory batch, pixels per thread); the autotuner picks one.
+static const int kBatches[3] = {64, 128, 256};
+
+template <int BATCH, int PPT>
+static void fwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
+    raster_fwd_kernel<BATCH, PPT><<<ctas, 256 / PPT, 0, s>>>(a);
 }
-template <int BATCH>
-static void bwd_dispatch(const RasterArgs& a, int ctas, cudaStream_t s) {
-    raster_bwd_kernel<BATCH><<<ctas, 256, 0, s>>>(a);
+template <int BATCH, int PPT>
+static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
+    raster_bwd_kernel<BATCH, PPT><<<ctas, 256 / PPT, 0, s>>>(a);
 }
 
-void launch_raster_fwd(const RasterArgs& a, int batch, int persistent_ctas, cudaStream_t s) {
+#define RASTER_SWITCH(FN, batch, ppt, ...)                   \
+    do {                                                     \
+        if ((ppt) == 2) {                                    \
+            switch (batch) {                                 \
+                case 64: FN<64, 2>(__VA_ARGS__); break;      \
+                case 128: FN<128, 2>(__VA_ARGS__); break;    \
+                default: FN<256, 2>(__VA_ARGS__); break;     \
+            }                                                \
+        } else {                                             \
+            switch (batch) {                                 \
+                case 64: FN<64, 1>(__VA_ARGS__); break;      \
+                case 128: FN<128, 1>(__VA_ARGS__); break;    \
+                default: FN<256, 1>(__VA_ARGS__); break;     \
+            }                                                \
+        }                                                    \
+    } while (0)
+
+void launch_raster_fwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
     const int ctas = a.work_counter ? persistent_ctas : a.num_tiles;
     if (ctas <= 0 || a.num_tiles <= 0) return;
-    switch (batch) {
-        case 64: fwd_dispatch<64>(a, ctas, s); break;
-        case 128: fwd_dispatch<128>(a, ctas, s); break;
-        default: fwd_dispatch<256>(a, ctas, s); break;
-    }
+    RASTER_SWITCH(fwd_launch, batch, ppt, a, ctas, s);
 }
 
-void launch_raster_bwd(const RasterArgs& a, int batch, int persistent_ctas, cudaStream_t s) {
+void launch_raster_bwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
     const int ctas = a.work_counter ? persistent_ctas : a.num_tiles;
     if (ctas <= 0 || a.num_tiles <= 0) return;
-    switch (batch) {
-        case 64: bwd_dispatch<64>(a, ctas, s); break;
-        case 128: bwd_dispatch<128>(a, ctas, s); break;
-        default: bwd_dispatch<256>(a, ctas, s); break;
-    }
+    RASTER_SWITCH(bwd_launch, batch, ppt, a, ctas, s);
 }
 
-int raster_max_ctas_per_sm(int batch, bool backward) {
+template <int BATCH, int PPT>
+static void occ(int* n, bool backward) {
+    if (backward) cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_bwd_kernel<BATCH, PPT>, 256 / PPT, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_fwd_kernel<BATCH, PPT>, 256 / PPT, 0);
+}
+
+int raster_max_ctas_per_sm(int batch, int ppt, bool backward) {
     int n = 0;
-    cudaError_t e;
-    if (!backward) {
-        switch (batch) {
-            case 64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_fwd_kernel<64>, 256, 0); break;
-            case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_fwd_kernel<128>, 256, 0); break;
-            default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_fwd_kernel<256>, 256, 0); break;
-        }
-    } else {
-        switch (batch) {
-            case 64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_bwd_kernel<64>, 256, 0); break;
-            case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_bwd_kernel<128>, 256, 0); break;
-            default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, raster_bwd_kernel<256>, 256, 0); break;
-        }
-    }
-    if (e != cudaSuccess || n < 1) n = 1;
-    return n;
+    RASTER_SWITCH(occ, batch, ppt, &n, backward);
+    cudaGetLastError();
+    return n < 1 ? 1 : n;
 }
 
 // ---------------------------------------------------------------------------------

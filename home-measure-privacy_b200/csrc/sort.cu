@@ -24,13 +24,14 @@ constexpr unsigned FULL = 0xffffffffu;
 
 int radix_tile_items() { return RS_TILE; }
 
+// 8-bit digits; an even number of passes so the result lands back in the input buffers
+// (keys above end_bit are zero, so an extra pass over them keeps the order).
 static void pass_plan(int begin_bit, int end_bit, int& passes, int& step) {
     const int bits = end_bit - begin_bit;
     passes = (bits + 7) / 8;
     if (passes < 1) passes = 1;
-    if (passes & 1) passes += 1;  // even: the result lands back in the input buffers
-    step = (bits + passes - 1) / passes;
-    if (step < 1) step = 1;
+    if (passes & 1) passes += 1;
+    step = 8;
 }
 
 int radix_sort_passes(int begin_bit, int end_bit) {
@@ -68,25 +69,46 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_tmp,
     return prefix + x - v;
 }
 
+// Lanes (among `valid` ones) holding the same 8-bit digit as this lane: one ballot per
+// digit bit, unrolled.
+__device__ __forceinline__ uint32_t warp_peers(uint32_t d, bool valid) {
+    uint32_t peers = __ballot_sync(FULL, valid);
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const uint32_t bal = __ballot_sync(FULL, (d >> b) & 1u);
+        peers &= ((d >> b) & 1u) ? bal : ~bal;
+    }
+    return peers;
+}
+
 __global__ void __launch_bounds__(RS_THREADS) radix_upsweep(const uint32_t* __restrict__ keys,
                                                             const SegInfo* seg, int shift, int bits,
                                                             uint32_t* __restrict__ hist) {
     __shared__ uint32_t wh[RS_WARPS][256];
     const uint32_t base = seg->base, n = seg->count;
     const uint32_t P = (n + RS_TILE - 1) / RS_TILE;
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t mask = (1u << bits) - 1u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
     for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
         for (int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS) (&wh[0][0])[d] = 0u;
         __syncthreads();
-        const uint32_t start = p * RS_TILE;
-#pragma unroll 4
+        const uint32_t start = p * RS_TILE + warp * (RS_ITEMS * 32);
+        uint32_t kk[RS_ITEMS];
+#pragma unroll
         for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = start + j * RS_THREADS + threadIdx.x;
-            if (idx < n) {
-                const uint32_t k = __ldg(keys + base + idx);
-                atomicAdd(&wh[warp][(k >> shift) & mask], 1u);
-            }
+            const uint32_t idx = start + j * 32 + lane;
+            kk[j] = idx < n ? __ldg(keys + base + idx) : 0u;  // all loads in flight together
+        }
+#pragma unroll
+        for (int j = 0; j < RS_ITEMS; j++) {
+            const uint32_t idx = start + j * 32 + lane;
+            const bool valid = idx < n;
+            const uint32_t d = valid ? (kk[j] >> shift) & mask : 0u;
+            // The lowest lane of each group of equal digits adds the group's size to the
+            // warp's histogram: one plain shared-memory update per distinct digit.
+            const uint32_t peers = warp_peers(d, valid);
+            if (valid && (peers & lt_mask) == 0u) wh[warp][d] += __popc(peers);
         }
         __syncthreads();
         for (int d = threadIdx.x; d < 256; d += RS_THREADS) {
@@ -118,7 +140,7 @@ __global__ void __launch_bounds__(1024) radix_scan(const SegInfo* seg, uint32_t*
     if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) radix_downsweep(
+__global__ void __launch_bounds__(RS_THREADS, 3) radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift,
     int bits, const uint32_t* __restrict__ hist, const uint32_t* __restrict__ totals) {
@@ -145,25 +167,19 @@ __global__ void __launch_bounds__(RS_THREADS) radix_downsweep(
         __syncthreads();
         const uint32_t part_start = p * RS_TILE;
         const uint32_t warp_start = part_start + warp * (RS_ITEMS * 32);
-        uint32_t k[RS_ITEMS], v[RS_ITEMS], rank[RS_ITEMS];
+        const uint32_t my_hist = hist[(size_t)threadIdx.x * P + p];  // digit threadIdx.x
+        uint32_t k[RS_ITEMS], rank[RS_ITEMS];
 #pragma unroll
         for (int j = 0; j < RS_ITEMS; j++) {
             const uint32_t idx = warp_start + j * 32 + lane;
-            const bool valid = idx < n;
-            k[j] = valid ? __ldg(keys_in + base + idx) : 0xffffffffu;
-            v[j] = valid ? (vals_in ? __ldg(vals_in + base + idx) : base + idx) : 0u;
+            k[j] = idx < n ? __ldg(keys_in + base + idx) : 0xffffffffu;
         }
 #pragma unroll
         for (int j = 0; j < RS_ITEMS; j++) {
             const uint32_t idx = warp_start + j * 32 + lane;
             const bool valid = idx < n;
             const uint32_t d = (k[j] >> shift) & mask;
-            uint32_t peers = __ballot_sync(FULL, valid);
-            for (int b = 0; b < bits; b++) {
-                const bool bit = (d >> b) & 1u;
-                const uint32_t bal = __ballot_sync(FULL, bit);
-                peers &= bit ? bal : ~bal;
-            }
+            const uint32_t peers = warp_peers(d, valid);
             uint32_t prev = 0;
             if (valid) {
                 prev = s_warp[warp][d];
@@ -186,18 +202,30 @@ __global__ void __launch_bounds__(RS_THREADS) radix_downsweep(
             uint32_t tot;
             const uint32_t ex = block_excl_scan<RS_THREADS>(s, s_tmp, tot);
             s_digit_start[d] = ex;
-            s_global[d] = s_total_excl[d] + hist[(size_t)d * P + p];
+            s_global[d] = s_total_excl[d] + my_hist;
         }
         __syncthreads();
+        // Keys to their block-sorted slots; then all values are loaded at once (no load
+        // waits behind a shared-memory store) and follow the keys.
 #pragma unroll
         for (int j = 0; j < RS_ITEMS; j++) {
             const uint32_t idx = warp_start + j * 32 + lane;
             if (idx < n) {
                 const uint32_t d = (k[j] >> shift) & mask;
-                const uint32_t pos = s_digit_start[d] + s_warp[warp][d] + rank[j];
-                s_keys[pos] = k[j];
-                s_vals[pos] = v[j];
+                rank[j] += s_digit_start[d] + s_warp[warp][d];
+                s_keys[rank[j]] = k[j];
             }
+        }
+        uint32_t v[RS_ITEMS];
+#pragma unroll
+        for (int j = 0; j < RS_ITEMS; j++) {
+            const uint32_t idx = warp_start + j * 32 + lane;
+            v[j] = (idx < n) ? (vals_in ? __ldg(vals_in + base + idx) : base + idx) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < RS_ITEMS; j++) {
+            const uint32_t idx = warp_start + j * 32 + lane;
+            if (idx < n) s_vals[rank[j]] = v[j];
         }
         __syncthreads();
         const uint32_t cnt = min((uint32_t)RS_TILE, n - part_start);
@@ -215,16 +243,17 @@ __global__ void __launch_bounds__(RS_THREADS) radix_downsweep(
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
     int passes, step;
     pass_plan(a.begin_bit, a.end_bit, passes, step);
-    const int grid_up = num_sms * 4;
-    const int grid_down = num_sms * 3;
+    // One block per partition of the largest segment this buffer can hold; blocks past
+    // the segment's live partitions exit at once.  (Persistent blocks walking many
+    // partitions left the loads' latency exposed.)
+    const int grid_up = a.max_parts > 0 ? a.max_parts : num_sms;
+    const int grid_down = grid_up;
     uint32_t* kb[2] = {a.keys, a.keys_alt};
     uint32_t* vb[2] = {a.vals, a.vals_alt};
     for (int p = 0; p < passes; p++) {
         const int in = p & 1, out = in ^ 1;
         const int shift = a.begin_bit + p * step;
-        int bits = a.end_bit - shift;
-        if (bits > step) bits = step;
-        if (bits < 1) bits = 1;
+        const int bits = 8;
         radix_upsweep<<<grid_up, RS_THREADS, 0, s>>>(kb[in], a.seg, shift, bits, a.hist);
         radix_scan<<<256, 1024, 0, s>>>(a.seg, a.hist, a.totals);
         radix_downsweep<<<grid_down, RS_THREADS, 0, s>>>(kb[in], (p == 0 && a.iota) ? nullptr : vb[in],
@@ -315,7 +344,9 @@ __global__ void __launch_bounds__(EM_THREADS) emit_offsets(EmitArgs a) {
         const uint32_t first = c * EM_CHUNK;
         for (uint32_t j = threadIdx.x; j < EM_CHUNK; j += EM_THREADS) {
             const uint32_t s = first + j;
-            s_cnt[j] = s < M ? rect_count(a.rect[__ldg(a.sorted_pairs + base + s)]) : 0u;
+            uint32_t cnt = 0;
+            if (s < M) cnt = rect_count(a.rect[__ldg(a.sorted_pairs + base + s)]);
+            s_cnt[j] = cnt;
         }
         __syncthreads();
         uint32_t cnt[EM_ITEMS];
@@ -344,10 +375,41 @@ __global__ void __launch_bounds__(EM_THREADS) emit_offsets(EmitArgs a) {
     }
 }
 
+// Inclusive max-scan over a block of NT threads.
+template <int NT>
+__device__ __forceinline__ uint32_t block_incl_max(uint32_t v, uint32_t* s_tmp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = NT / 32;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    if (lane == 31) s_tmp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t t = lane < NW ? s_tmp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(FULL, t, o);
+            if (lane >= o) t = max(t, y);
+        }
+        if (lane < NW) s_tmp[lane] = t;
+    }
+    __syncthreads();
+    const uint32_t prefix = warp > 0 ? s_tmp[warp - 1] : 0u;
+    __syncthreads();
+    return max(prefix, x);
+}
+
 __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
+    constexpr int PER = EM_OUT / EM_THREADS;  // instances per thread
     __shared__ uint32_t s_off[EM_OUT + 1];
     __shared__ uint32_t s_pair[EM_OUT + 1];
-    __shared__ uint2 s_rect[EM_OUT + 1];
+    __shared__ uint2 s_geom[EM_OUT + 1];     // first tile of the rectangle, tiles_x | width << 16
+    __shared__ uint32_t s_head[EM_OUT];
+    __shared__ uint32_t s_tmp[32];
     const uint32_t M = *a.visible;
     const uint32_t base = a.pair_seg->base;
     const uint32_t inst_base = a.inst_seg->base;
@@ -362,59 +424,112 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
         // needs at most EM_OUT + 1 pairs (the bound matters for the last block when the
         // capacity clamped the instance count).
         const uint32_t np = min(p_hi - p_lo + 1, (uint32_t)EM_OUT + 1);
+        for (uint32_t j = threadIdx.x; j < EM_OUT; j += EM_THREADS) s_head[j] = 0u;
         for (uint32_t j = threadIdx.x; j < np; j += EM_THREADS) {
             const uint32_t pair = __ldg(a.sorted_pairs + base + p_lo + j);
+            const uint2 r = a.rect[pair];
+            const ViewDesc& vw = a.views[a.view_first + pair / (uint32_t)a.n_pad];
+            const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu;
             s_off[j] = a.pair_offsets[p_lo + j];
             s_pair[j] = pair;
-            s_rect[j] = a.rect[pair];
+            s_geom[j] = make_uint2((uint32_t)vw.tile_offset + y0 * (uint32_t)vw.tiles_x + x0,
+                                   (uint32_t)vw.tiles_x | ((x1 - x0) << 16));
         }
         __syncthreads();
-        for (uint32_t o = o0 + threadIdx.x; o < o1; o += EM_THREADS) {
-            uint32_t lo = 0, hi = np - 1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (s_off[mid] <= o) lo = mid;
-                else hi = mid - 1;
-            }
-            const uint32_t pair = s_pair[lo];
-            const uint2 r = s_rect[lo];
-            const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu;
-            const uint32_t w = x1 - x0;
-            const uint32_t t = o - s_off[lo];
-            const uint32_t tx = x0 + t % w, ty = y0 + t / w;
-            const ViewDesc& vw = a.views[a.view_first + pair / (uint32_t)a.n_pad];
-            a.inst_keys[inst_base + o] = (uint32_t)vw.tile_offset + ty * (uint32_t)vw.tiles_x + tx;
-            a.inst_vals[inst_base + o] = pair;
+        // Head flags: the instance where each pair starts gets the pair's local index;
+        // a running max then gives every instance its pair.
+        for (uint32_t j = 1 + threadIdx.x; j < np; j += EM_THREADS) {
+            const uint32_t pos = s_off[j] - o0;
+            if (pos < (uint32_t)EM_OUT) s_head[pos] = j;
         }
+        __syncthreads();
+        uint32_t run = 0, loc[PER];
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            run = max(run, s_head[threadIdx.x * PER + k]);
+            loc[k] = run;
+        }
+        const uint32_t prefix = block_incl_max<EM_THREADS>(run, s_tmp);
+        const uint32_t carry = __shfl_up_sync(FULL, prefix, 1);
+        // Exclusive prefix of this thread = inclusive max of the threads before it.
+        uint32_t before = 0;
+        {
+            const int lane = threadIdx.x & 31;
+            before = lane > 0 ? carry : 0u;
+            if (lane == 0 && threadIdx.x > 0) before = s_tmp[(threadIdx.x >> 5) - 1];
+        }
+        __syncthreads();
+        // Tile of each instance into shared memory (s_head holds tiles now), then
+        // striped, coalesced stores.
+        uint32_t jj[PER];
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t ol = threadIdx.x * PER + k;
+            const uint32_t j = max(before, loc[k]);
+            jj[k] = j;
+            const uint2 gm = s_geom[j];
+            const uint32_t tx = gm.y & 0xffffu, w = gm.y >> 16;
+            const uint32_t t = o0 + ol - s_off[j];
+            const uint32_t row = t / max(w, 1u);
+            s_head[ol] = gm.x + row * tx + (t - row * w);
+        }
+        __syncthreads();
+        for (uint32_t ol = threadIdx.x; ol < o1 - o0; ol += EM_THREADS) a.inst_keys[inst_base + o0 + ol] = s_head[ol];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; k++) s_head[threadIdx.x * PER + k] = s_pair[jj[k]];
+        __syncthreads();
+        for (uint32_t ol = threadIdx.x; ol < o1 - o0; ol += EM_THREADS) a.inst_vals[inst_base + o0 + ol] = s_head[ol];
         __syncthreads();
     }
 }
 
 void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms) {
-    int grid = num_sms * 4;
-    if (grid > a.max_chunks) grid = a.max_chunks > 0 ? a.max_chunks : 1;
+    // One block per chunk / output block of the capacity; idle blocks exit at once.
+    const int grid = a.max_chunks > 0 ? a.max_chunks : 1;
+    const int grid_out = (int)(a.capacity / EM_OUT + 1);
+    (void)num_sms;
     emit_reduce<<<grid, EM_THREADS, 0, s>>>(a);
     emit_scan<<<1, 1024, 0, s>>>(a);
     emit_offsets<<<grid, EM_THREADS, 0, s>>>(a);
-    emit_expand<<<num_sms * 4, EM_THREADS, 0, s>>>(a);
+    emit_expand<<<grid_out, EM_THREADS, 0, s>>>(a);
 }
+
 
 // ---------------------------------------------------------------------------------
 // Tile ranges: each tile's [first, last + 1) in the tile-sorted instances (absolute
 // indices).  Tiles without instances keep the zeroed (0, 0).
 // ---------------------------------------------------------------------------------
-__global__ void ranges_kernel(const uint32_t* __restrict__ tiles, const SegInfo* seg, uint2* ranges) {
+constexpr int RG_ITEMS = 16;
+
+// Each thread takes RG_ITEMS consecutive sorted keys and compares neighbours in
+// registers (one extra load for the key before its chunk).
+__global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict__ tiles, const SegInfo* seg,
+                                                    uint2* ranges) {
     const uint32_t base = seg->base, n = seg->count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t t = tiles[base + i];
-        if (i == 0 || tiles[base + i - 1] != t) ranges[t].x = base + i;
-        if (i == n - 1 || tiles[base + i + 1] != t) ranges[t].y = base + i + 1;
+    const uint32_t chunks = (n + RG_ITEMS - 1) / RG_ITEMS;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < chunks; c += gridDim.x * blockDim.x) {
+        const uint32_t i0 = c * RG_ITEMS;
+        uint32_t t[RG_ITEMS];
+#pragma unroll
+        for (int k = 0; k < RG_ITEMS; k++) t[k] = (i0 + k < n) ? __ldg(tiles + base + i0 + k) : 0xffffffffu;
+        uint32_t prev = i0 > 0 ? __ldg(tiles + base + i0 - 1) : 0xffffffffu;
+        const uint32_t next = (i0 + RG_ITEMS < n) ? __ldg(tiles + base + i0 + RG_ITEMS) : 0xffffffffu;
+#pragma unroll
+        for (int k = 0; k < RG_ITEMS; k++) {
+            const uint32_t i = i0 + k;
+            if (i >= n) break;
+            const uint32_t nx = (k + 1 < RG_ITEMS) ? t[k + 1] : next;
+            if (t[k] != prev) ranges[t[k]].x = base + i;
+            if (i + 1 == n || nx != t[k]) ranges[t[k]].y = base + i + 1;
+            prev = t[k];
+        }
     }
 }
 
 void launch_ranges(const uint32_t* sorted_tiles, const SegInfo* seg, uint2* ranges, cudaStream_t s,
                    int num_sms) {
-    ranges_kernel<<<num_sms * 8, 256, 0, s>>>(sorted_tiles, seg, ranges);
+    ranges_kernel<<<num_sms * 16, 256, 0, s>>>(sorted_tiles, seg, ranges);
 }
 
 }  // namespace gs

@@ -63,7 +63,7 @@ class Renderer:
     """createRenderer() result.  One CUDA context (device, stream, buffers)."""
 
     def __init__(self, gpuTiles=True, sh_degree=0, near=0.2, batched=True, use_graph=True, device=0,
-                 raster_batch=256, lpt_order=True, rect_mode=None, instance_capacity=0):
+                 raster_batch=256, lpt_order=True, rect_mode=None, instance_capacity=0, raster_ppt=1):
         self.lib = N.load()
         cfg = N.GsConfig()
         self.lib.gs_config_default(ctypes.byref(cfg))
@@ -75,6 +75,7 @@ class Renderer:
         cfg.raster_batch = int(raster_batch)
         cfg.lpt_order = 1 if lpt_order else 0
         cfg.instance_capacity = int(instance_capacity)
+        cfg.raster_ppt = int(raster_ppt)
         # gpuTiles=False is the reference's CPU tileLists path (trainer/gpu.js:703, :799-806):
         # here the binning always runs on the GPU, with tileLists' tile rectangle.
         cfg.rect_mode = int(rect_mode) if rect_mode is not None else (0 if gpuTiles else 1)
@@ -278,7 +279,7 @@ class Renderer:
     def stats(self):
         s = N.GsStats()
         N.check(self.lib.gs_get_stats(self.ctx, ctypes.byref(s)))
-        return {f: getattr(s, f) for f, _ in N.GsStats._fields_ if f != "reserved"}
+        return {f: getattr(s, f) for f, _ in N.GsStats._fields_}
 
     def step_count(self):
         t = ctypes.c_int32(0)
@@ -289,8 +290,10 @@ class Renderer:
         N.check(self.lib.gs_synchronize(self.ctx))
 
     def autotune(self, cache_path=None):
+        """Picks the raster variants; returns {fwd: (batch, ppt), bwd: (batch, ppt)}."""
         N.check(self.lib.gs_autotune(self.ctx, cache_path.encode() if cache_path else None))
-        return self.stats()["raster_batch"]
+        v = self.stats()["raster_variant"]
+        return dict(fwd=(v & 0xfff, (v >> 12) & 0xf), bwd=((v >> 16) & 0xfff, (v >> 28) & 0xf))
 
     def stage_times(self):
         ms = np.zeros(N.GS_NUM_STAGES, np.float64)

@@ -73,7 +73,9 @@ typedef struct GsConfig {
     int32_t instance_capacity; /* initial key-instance capacity; 0 = measured by a first
                               forward.  A step that overflows skips its update, the
                               buffer grows and a synchronous step is redone.           */
-    int32_t reserved[3];
+    int32_t raster_ppt;    /* pixels per raster thread: 1 (256 threads per 16 x 16
+                              tile) or 2 (128 threads); 0 = 1                           */
+    int32_t reserved[2];
 } GsConfig;
 
 /* Adam settings.  The per-group learning rates are the reference's (trainer/gpu.js:846,
@@ -261,7 +263,7 @@ typedef struct GsStats {
     int32_t raster_batch;
     int32_t raster_threads;
     int32_t overflow;
-    int32_t reserved;
+    int32_t raster_variant;  /* fwd batch | fwd ppt << 12 | bwd batch << 16 | bwd ppt << 28 */
 } GsStats;
 GS_API int gs_get_stats(GsContext* ctx, GsStats* out);
 
@@ -280,9 +282,10 @@ GS_API int gs_get_tile_lists(GsContext* ctx, int32_t view, uint32_t* list_out,
  * depth, r, g, b, valid. */
 GS_API int gs_get_splats(GsContext* ctx, int32_t view, float* splats12_out);
 
-/* Raster tuning: measures the raster kernels' candidate variants on the current views
- * and keeps the fastest (tile batch and threads per tile).  cache_path (optional): a
- * text file that records the choice per device and workload. */
+/* Raster tuning: measures the raster kernels' candidate variants (splats per shared-
+ * memory batch, pixels per thread) on the current views and keeps the fastest forward
+ * and backward.  cache_path (optional): a text file that records the choice per device
+ * and workload. */
 GS_API int gs_autotune(GsContext* ctx, const char* cache_path);
 
 #ifdef __cplusplus
