@@ -108,6 +108,7 @@ SIGNATURES = {
     "gs_get_tile_lists": (ctypes.c_int, [CTX, c_int32, VP, VP, VP, c_int64, ctypes.POINTER(c_int64)]),
     "gs_get_splats": (ctypes.c_int, [CTX, c_int32, VP]),
     "gs_autotune": (ctypes.c_int, [CTX, ctypes.c_char_p]),
+    "gs_loss_gradient_noalloc": (ctypes.c_int, [VP, VP, c_int32, c_int32, c_int32, c_float, c_int32, VP, VP, VP]),
 }
 
 _lib = None

@@ -288,6 +288,31 @@ GS_API int gs_get_splats(GsContext* ctx, int32_t view, float* splats12_out);
  * and workload. */
 GS_API int gs_autotune(GsContext* ctx, const char* cache_path);
 
+/* ---- loss gradient without allocation ------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device memory: an
+ * engine that hands out all GPU memory from its own pool, code being recorded into a
+ * CUDA graph by the caller (a cudaMalloc would end the capture), or a real-time loop
+ * that must not wait on the allocator.  Same result as gs_loss_gradient for each image,
+ * but image, target, grad and loss are caller-owned DEVICE buffers and the call only
+ * queues work on `stream` (a cudaStream_t; NULL = the legacy default stream): read the
+ * outputs after synchronising it.  num_images images of width x height (RGB floats,
+ * concatenated) are processed in one launch; loss (optional) gets one mean loss per
+ * image.  The kernels' scratch (view descriptors, per-image loss sums) lives in one
+ * static device array of GS_NOALLOC_SCRATCH_BYTES that every GPU loading the library
+ * keeps until exit, sized for at most GS_NOALLOC_MAX_IMAGES images: more images return
+ * GS_ERR_CAPACITY.  Nothing is allocated: no cudaMalloc, cudaFree or allocating library
+ * call.  The first call on a device looks up the array's address on that device (and
+ * raises the loss kernel's shared-memory limit), so make the first call on each device
+ * outside any stream capture.  All calls share the array and it keeps the last call's
+ * contents; each call clears the sums it accumulates, and calls that overlap on the GPU
+ * (other streams or host threads on the same device) race on it.  Returns GS_OK or a
+ * status code; it does not set gs_last_error. */
+#define GS_NOALLOC_MAX_IMAGES 8
+#define GS_NOALLOC_SCRATCH_BYTES 4096
+GS_API int gs_loss_gradient_noalloc(const float* image, const float* target, int32_t num_images,
+                                    int32_t width, int32_t height, float ssim_lambda, int32_t window,
+                                    float* grad, float* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
