@@ -118,7 +118,7 @@ struct GsContext {
     DevBuf views_d, target_u8, target_f32, image, t_final, last, dl, ranges, tile_order;
     // pairs
     int64_t pair_cap = 0;
-    DevBuf geo0, geo1, rgb, rect, pkeys, pvals, pkeys_alt, pvals_alt, sg8, sg1;
+    DevBuf geo0, geo1, rgb, rect, pkeys, pvals, pkeys_alt, pvals_alt, sg8, sg1, pcount, spans;
     // instances
     int64_t inst_cap = 0;
     bool inst_cap_valid = false;
@@ -346,6 +346,8 @@ static int size_pairs(GsContext* c, int views) {
         CKI(ensure(c->geo1, (size_t)pairs * 16, c));
         CKI(ensure(c->rgb, (size_t)pairs * 16, c));
         CKI(ensure(c->rect, (size_t)pairs * 8, c));
+        CKI(ensure(c->pcount, (size_t)pairs * 4, c));
+        CKI(ensure(c->spans, (size_t)pairs * 16, c));
         CKI(ensure(c->pkeys, (size_t)pairs * 4, c));
         CKI(ensure(c->pvals, (size_t)pairs * 4, c));
         CKI(ensure(c->pkeys_alt, (size_t)pairs * 4, c));
@@ -471,6 +473,10 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     pa.rect = c->rect.as<uint2>();
     pa.keys = c->pkeys.as<uint32_t>();
     pa.visible = visible;
+    pa.tile_cull = c->cfg.tile_cull;
+    pa.alpha_min = c->cfg.alpha_min;
+    pa.pcount = c->pcount.as<uint32_t>();
+    pa.spans = c->spans.as<uint4>();
     launch_project_fwd(pa, c->stream);
     count_launches(c, ST_PROJECT, 1);
     // Depth sort of the pairs (31 bits: depths are positive, the sentinel is 0x7fffffff).
@@ -497,6 +503,8 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ea.pair_seg = pair_seg;
     ea.visible = visible;
     ea.rect = c->rect.as<uint2>();
+    ea.pcount = c->pcount.as<uint32_t>();
+    ea.spans = c->spans.as<uint4>();
     ea.views = c->views_d.as<ViewDesc>();
     ea.view_first = step_first;  // pair / n_pad is the slot relative to the step's first view
     ea.n_pad = c->n_pad;
@@ -818,6 +826,7 @@ void gs_config_default(GsConfig* cfg) {
     cfg->autotune = 0;
     cfg->raster_batch = 256;
     cfg->raster_ppt = 1;
+    cfg->tile_cull = 1;
     cfg->lpt_order = 1;
 }
 
@@ -899,6 +908,7 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(GS_ERR_CUDA, "cudaStreamCreate failed"));
     if (loss_prepare() != cudaSuccess) return bail(fail(GS_ERR_CUDA, "loss kernel attributes"));
+    if (radix_prepare() != cudaSuccess) return bail(fail(GS_ERR_CUDA, "radix kernel attributes"));
     if ((rc = ensure(c->status, sizeof(DevStatus), c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->visible, sizeof(unsigned) * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->acc, sizeof(double) * 2 * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
@@ -925,7 +935,7 @@ int gs_destroy(GsContext* c) {
     drop_graphs(c);
     DevBuf* bufs[] = {&c->params, &c->grads, &c->mom1, &c->mom2, &c->views_d, &c->target_u8, &c->target_f32,
                       &c->image, &c->t_final, &c->last, &c->dl, &c->ranges, &c->tile_order, &c->geo0, &c->geo1,
-                      &c->rgb, &c->rect, &c->pkeys, &c->pvals, &c->pkeys_alt, &c->pvals_alt, &c->sg8, &c->sg1,
+                      &c->rgb, &c->rect, &c->pcount, &c->spans, &c->pkeys, &c->pvals, &c->pkeys_alt, &c->pvals_alt, &c->sg8, &c->sg1,
                       &c->ikeys, &c->ivals, &c->ikeys_alt, &c->ivals_alt, &c->hist, &c->totals, &c->block_sums,
                       &c->pair_offsets, &c->block_first_pair,
                       &c->segs, &c->visible, &c->acc, &c->scratch16, &c->status};

@@ -249,6 +249,36 @@ __host__ __device__ __forceinline__ void tile_rect(float u, float v, float r, in
     if (y1 < y0) y1 = y0;
 }
 
+// Smallest value of the conic's quadratic form A dx^2 + 2 B dx dy + C dy^2 over the box
+// [xl, xh] x [yl, yh] (offsets from the splat centre).  Convex, so: 0 when the centre is
+// inside, else the least of the four edges' clamped 1-D minima.
+__host__ __device__ __forceinline__ float conic_qmin_box(float A, float B, float C, float xl, float xh, float yl,
+                                                         float yh) {
+    if (xl <= 0.f && xh >= 0.f && yl <= 0.f && yh >= 0.f) return 0.f;
+    const float iA = 1.0f / A, iC = 1.0f / C;
+    float best, x, y, q;
+    x = xl; y = fminf(fmaxf(-B * x * iC, yl), yh); best = A * x * x + 2.f * B * x * y + C * y * y;
+    x = xh; y = fminf(fmaxf(-B * x * iC, yl), yh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
+    y = yl; x = fminf(fmaxf(-B * y * iA, xl), xh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
+    y = yh; x = fminf(fmaxf(-B * y * iA, xl), xh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
+    return best;
+}
+
+// Can a splat (centre u, v; conic A, B, C; radius r; culling bound thr = 2 ln(op /
+// alpha_min) + slack) give any pixel centre in [px0, px1] x [py0, py1] alpha >=
+// alpha_min?  Conservative: a pixel passes only inside the square |dx|, |dy| <= r and
+// where the quadratic form is below thr.
+__host__ __device__ __forceinline__ bool splat_reaches_box(float u, float v, float A, float B, float C, float r,
+                                                           float thr, float px0, float px1, float py0, float py1) {
+    const float xl = fmaxf(px0, u - r), xh = fminf(px1, u + r);
+    const float yl = fmaxf(py0, v - r), yh = fminf(py1, v + r);
+    if (xl > xh || yl > yh) return false;
+    return conic_qmin_box(A, B, C, xl - u, xh - u, yl - v, yh - v) <= thr;
+}
+
+#define GS_SPAN_ROWS 8            // pairs up to this many tile rows get per-row tile spans
+#define GS_PCOUNT_RECT 0x80000000u  // pcount flag: instances are the whole rectangle
+
 // ---------------------------------------------------------------------------------
 // Real spherical harmonics up to degree 3 (Condon-Shortley phase).  Coefficient k of a
 // band l >= 1 uses index k = l^2 + l + m; constants are K_l^m = sqrt((2l+1)/(4 pi) *

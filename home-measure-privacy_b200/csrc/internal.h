@@ -21,6 +21,10 @@ struct ProjectArgs {
     uint2* rect;
     uint32_t* keys;          // depth key, GS_KEY_SENTINEL when the pair covers no tile
     unsigned int* visible;   // optional counter of pairs with >= 1 tile
+    int tile_cull;           // 1: only tiles the alpha >= alpha_min ellipse reaches
+    float alpha_min;
+    uint32_t* pcount;        // instances of the pair (| GS_PCOUNT_RECT: whole rectangle)
+    uint4* spans;            // per rectangle row r < 8: tiles [xs, xe) as bytes (xs | xe << 8) << 16 * (r & 1)
 };
 void launch_project_fwd(const ProjectArgs& a, cudaStream_t s);
 
@@ -58,6 +62,7 @@ struct RadixSortArgs {
 int radix_sort_passes(int begin_bit, int end_bit);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms);
 int radix_tile_items();
+cudaError_t radix_prepare();
 
 // Emission of key instances from the depth-sorted pairs.
 struct EmitArgs {
@@ -65,6 +70,8 @@ struct EmitArgs {
     const SegInfo* pair_seg;        // pair segment: base into sorted_pairs, count
     const unsigned int* visible;    // number of visible pairs in the segment
     const uint2* rect;
+    const uint32_t* pcount;
+    const uint4* spans;
     const ViewDesc* views;
     int view_first, n_pad;
     int pair_slot_first;            // slot of the first pair of this segment

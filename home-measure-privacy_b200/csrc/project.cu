@@ -59,7 +59,56 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
             tile_rect(p.u, p.v, p.radius, vw.tiles_x, vw.tiles_y, a.rect_mode, x0, x1, y0, y1);
         else
             p.ok = false;
-        const bool covers = p.ok && x1 > x0 && y1 > y0;
+        uint32_t count = (p.ok && x1 > x0 && y1 > y0) ? (uint32_t)((x1 - x0) * (y1 - y0)) : 0u;
+        uint32_t sp[4] = {0u, 0u, 0u, 0u};
+        if (count && a.tile_cull) {
+            if (y1 - y0 <= GS_SPAN_ROWS && x1 - x0 < 256) {
+                // Per rectangle row, the tiles the ellipse A dx^2 + 2B dx dy + C dy^2 <= thr
+                // reaches inside the row's pixel band (and the |d| <= r square, and the
+                // image): the band's x-extent of the ellipse is contiguous, its right edge
+                // concave and its left edge convex in dy, so each extreme sits at its
+                // stationary point dy* = -/+ B sqrt(thr / (det C)) clamped to the band.
+                const float thr = 2.0f * (logf(opacity) - logf(a.alpha_min)) + 1e-3f;
+                const float A = p.a, B = p.b, C = p.c;
+                const float det = fmaxf(A * C - B * B, 1e-30f);
+                const float ymax = sqrtf(fmaxf(thr, 0.f) * A / det);
+                const float ystat = B * sqrtf(fmaxf(thr, 0.f) / (det * C));
+                const float iA = 1.0f / A;
+                const float H1 = (float)vw.height - 0.5f, W1 = (float)vw.width - 0.5f;
+                const float xlo_lim = fmaxf(p.u - p.radius, 0.5f), xhi_lim = fminf(p.u + p.radius, W1);
+                count = 0;
+                for (int ty = y0; ty < y1; ty++) {
+                    float yl = fmaxf(fmaxf((float)(ty * GS_TILE) + 0.5f, p.v - p.radius), p.v - ymax) - p.v;
+                    float yh = fminf(fminf(fminf((float)(ty * GS_TILE) + 15.5f, H1), p.v + p.radius), p.v + ymax) - p.v;
+                    int xs = 0, xe = 0;
+                    if (thr > 0.f && yl <= yh) {
+                        const float dr = fminf(fmaxf(-ystat, yl), yh);   // right edge maximiser
+                        const float dl = fminf(fmaxf(ystat, yl), yh);    // left edge minimiser
+                        const float sr = sqrtf(fmaxf(A * thr - det * dr * dr, 0.f));
+                        const float sl = sqrtf(fmaxf(A * thr - det * dl * dl, 0.f));
+                        const float slack = 1e-3f * (1.0f + p.radius);
+                        const float xhi = fminf(p.u + (-B * dr + sr) * iA + slack, xhi_lim);
+                        const float xlo = fmaxf(p.u + (-B * dl - sl) * iA - slack, xlo_lim);
+                        if (xlo <= xhi) {
+                            // Tile tx holds pixel centres [16 tx + 0.5, 16 tx + 15.5].
+                            xs = max(x0, (int)ceilf((xlo - 15.5f) * 0.0625f));
+                            xe = min(x1, (int)floorf((xhi - 0.5f) * 0.0625f) + 1);
+                            if (xe < xs) xe = xs;
+                        }
+                    }
+                    const int r = ty - y0;
+                    if (xe > xs) {
+                        sp[r >> 1] |= ((uint32_t)(xs - x0) | ((uint32_t)(xe - x0) << 8)) << (16 * (r & 1));
+                        count += (uint32_t)(xe - xs);
+                    }
+                }
+            } else {
+                count |= GS_PCOUNT_RECT;
+            }
+        } else if (count) {
+            count |= GS_PCOUNT_RECT;
+        }
+        const bool covers = (count & ~GS_PCOUNT_RECT) != 0u;
         float r = 0.f, g = 0.f, b = 0.f;
         if (p.ok) {
             r = dc[0]; g = dc[1]; b = dc[2];
@@ -83,6 +132,8 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
         a.rgb[pair] = make_float4(r, g, b, p.ok ? 1.0f : 0.0f);
         a.rect[pair] = make_uint2((unsigned)x0 | ((unsigned)x1 << 16), (unsigned)y0 | ((unsigned)y1 << 16));
         a.keys[pair] = covers ? __float_as_uint(p.depth) : GS_KEY_SENTINEL;
+        a.pcount[pair] = covers ? count : 0u;
+        a.spans[pair] = make_uint4(sp[0], sp[1], sp[2], sp[3]);
         my_visible += covers ? 1u : 0u;
     }
     if (a.visible) {

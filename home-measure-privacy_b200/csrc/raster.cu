@@ -148,30 +148,12 @@ __device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, co
     return fminf(amax, alpha);
 }
 
-// Smallest value of the conic's quadratic form A dx^2 + 2 B dx dy + C dy^2 over the box
-// [xl, xh] x [yl, yh] (offsets from the splat centre).  Convex, so: 0 when the centre is
-// inside, else the least of the four edges' clamped 1-D minima.
-__device__ __forceinline__ float qmin_box(float A, float B, float C, float xl, float xh, float yl, float yh) {
-    if (xl <= 0.f && xh >= 0.f && yl <= 0.f && yh >= 0.f) return 0.f;
-    const float iA = 1.0f / A, iC = 1.0f / C;
-    float best, x, y, q;
-    x = xl; y = fminf(fmaxf(-B * x * iC, yl), yh); best = A * x * x + 2.f * B * x * y + C * y * y;
-    x = xh; y = fminf(fmaxf(-B * x * iC, yl), yh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
-    y = yl; x = fminf(fmaxf(-B * y * iA, xl), xh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
-    y = yh; x = fminf(fmaxf(-B * y * iA, xl), xh); q = A * x * x + 2.f * B * x * y + C * y * y; best = fminf(best, q);
-    return best;
-}
-
 // Can splat (g0, g1) give any pixel centre of the warp's rectangle alpha >= alpha_min?
 // Conservative: the pixels' own tests (bounding box, then alpha) decide; this only
 // skips splats that cannot pass them anywhere in the rectangle.
 template <int PPT>
 __device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1, const TileInfo<PPT>& ti) {
-    const float r = g1.z;
-    const float xl = fmaxf(ti.wx0, g0.x - r), xh = fminf(ti.wx1, g0.x + r);
-    const float yl = fmaxf(ti.wy0, g0.y - r), yh = fminf(ti.wy1, g0.y + r);
-    if (xl > xh || yl > yh) return false;
-    return qmin_box(g0.z, g0.w, g1.x, xl - g0.x, xh - g0.x, yl - g0.y, yh - g0.y) <= g1.w;
+    return splat_reaches_box(g0.x, g0.y, g0.z, g0.w, g1.x, g1.z, g1.w, ti.wx0, ti.wx1, ti.wy0, ti.wy1);
 }
 
 template <int BATCH, int PPT>

@@ -262,6 +262,7 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
     }
 }
 
+
 // ---------------------------------------------------------------------------------
 // Key-instance emission.  Depth-sorted pairs are taken in chunks of EM_CHUNK:
 // (1) per-chunk sums of the pairs' tile counts; (2) one block scans the chunk sums and
@@ -282,9 +283,8 @@ constexpr int EM_OUT = 2048;
 int emit_chunk_items() { return EM_CHUNK; }
 int emit_out_items() { return EM_OUT; }
 
-__device__ __forceinline__ uint32_t rect_count(uint2 r) {
-    const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu, y1 = r.y >> 16;
-    return (x1 > x0 && y1 > y0) ? (x1 - x0) * (y1 - y0) : 0u;
+__device__ __forceinline__ uint32_t pair_count(const EmitArgs& a, uint32_t pair) {
+    return a.pcount[pair] & ~GS_PCOUNT_RECT;
 }
 
 __global__ void __launch_bounds__(EM_THREADS) emit_reduce(EmitArgs a) {
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(EM_THREADS) emit_reduce(EmitArgs a) {
 #pragma unroll
         for (int j = 0; j < EM_ITEMS; j++) {
             const uint32_t sidx = c * EM_CHUNK + j * EM_THREADS + threadIdx.x;
-            if (sidx < M) sum += rect_count(a.rect[__ldg(a.sorted_pairs + base + sidx)]);
+            if (sidx < M) sum += pair_count(a, __ldg(a.sorted_pairs + base + sidx));
         }
         uint32_t tot;
         block_excl_scan<EM_THREADS>(sum, s_tmp, tot);
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(EM_THREADS) emit_offsets(EmitArgs a) {
         for (uint32_t j = threadIdx.x; j < EM_CHUNK; j += EM_THREADS) {
             const uint32_t s = first + j;
             uint32_t cnt = 0;
-            if (s < M) cnt = rect_count(a.rect[__ldg(a.sorted_pairs + base + s)]);
+            if (s < M) cnt = pair_count(a, __ldg(a.sorted_pairs + base + s));
             s_cnt[j] = cnt;
         }
         __syncthreads();
@@ -403,12 +403,16 @@ __device__ __forceinline__ uint32_t block_incl_max(uint32_t v, uint32_t* s_tmp) 
     return max(prefix, x);
 }
 
+constexpr size_t EM_EXPAND_SMEM = (size_t)(EM_OUT + 1) * (4 + 4 + 8 + 16) + (size_t)EM_OUT * 4;
+
 __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
     constexpr int PER = EM_OUT / EM_THREADS;  // instances per thread
-    __shared__ uint32_t s_off[EM_OUT + 1];
-    __shared__ uint32_t s_pair[EM_OUT + 1];
-    __shared__ uint2 s_geom[EM_OUT + 1];     // first tile of the rectangle, tiles_x | width << 16
-    __shared__ uint32_t s_head[EM_OUT];
+    extern __shared__ __align__(16) unsigned char em_smem[];
+    uint4* s_span = reinterpret_cast<uint4*>(em_smem);                               // rows' tile spans
+    uint2* s_geom = reinterpret_cast<uint2*>(s_span + (EM_OUT + 1));                 // first tile, tiles_x | width << 16 | rect flag
+    uint32_t* s_off = reinterpret_cast<uint32_t*>(s_geom + (EM_OUT + 1));
+    uint32_t* s_pair = s_off + (EM_OUT + 1);
+    uint32_t* s_head = s_pair + (EM_OUT + 1);
     __shared__ uint32_t s_tmp[32];
     const uint32_t M = *a.visible;
     const uint32_t base = a.pair_seg->base;
@@ -430,10 +434,12 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
             const uint2 r = a.rect[pair];
             const ViewDesc& vw = a.views[a.view_first + pair / (uint32_t)a.n_pad];
             const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu;
+            const uint32_t whole = (a.pcount[pair] & GS_PCOUNT_RECT) ? 1u : 0u;
             s_off[j] = a.pair_offsets[p_lo + j];
             s_pair[j] = pair;
             s_geom[j] = make_uint2((uint32_t)vw.tile_offset + y0 * (uint32_t)vw.tiles_x + x0,
-                                   (uint32_t)vw.tiles_x | ((x1 - x0) << 16));
+                                   (uint32_t)vw.tiles_x | ((x1 - x0) << 16) | (whole << 31));
+            s_span[j] = a.spans[pair];
         }
         __syncthreads();
         // Head flags: the instance where each pair starts gets the pair's local index;
@@ -468,10 +474,29 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
             const uint32_t j = max(before, loc[k]);
             jj[k] = j;
             const uint2 gm = s_geom[j];
-            const uint32_t tx = gm.y & 0xffffu, w = gm.y >> 16;
-            const uint32_t t = o0 + ol - s_off[j];
-            const uint32_t row = t / max(w, 1u);
-            s_head[ol] = gm.x + row * tx + (t - row * w);
+            const uint32_t tx = gm.y & 0xffffu, w = (gm.y >> 16) & 0x7fffu;
+            uint32_t t = o0 + ol - s_off[j];
+            uint32_t tile;
+            if (gm.y >> 31) {
+                const uint32_t row = t / max(w, 1u);
+                tile = gm.x + row * tx + (t - row * w);
+            } else {
+                // Walk the rows' spans (at most GS_SPAN_ROWS).
+                const uint4 sp = s_span[j];
+                const uint32_t words[4] = {sp.x, sp.y, sp.z, sp.w};
+                tile = gm.x;
+#pragma unroll
+                for (int r = 0; r < GS_SPAN_ROWS; r++) {
+                    const uint32_t h = (words[r >> 1] >> (16 * (r & 1))) & 0xffffu;
+                    const uint32_t xs = h & 0xffu, len = (h >> 8) - xs;
+                    if (t < len) {
+                        tile = gm.x + (uint32_t)r * tx + xs + t;
+                        break;
+                    }
+                    t -= len;
+                }
+            }
+            s_head[ol] = tile;
         }
         __syncthreads();
         for (uint32_t ol = threadIdx.x; ol < o1 - o0; ol += EM_THREADS) a.inst_keys[inst_base + o0 + ol] = s_head[ol];
@@ -492,7 +517,7 @@ void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms) {
     emit_reduce<<<grid, EM_THREADS, 0, s>>>(a);
     emit_scan<<<1, 1024, 0, s>>>(a);
     emit_offsets<<<grid, EM_THREADS, 0, s>>>(a);
-    emit_expand<<<grid_out, EM_THREADS, 0, s>>>(a);
+    emit_expand<<<grid_out, EM_THREADS, EM_EXPAND_SMEM, s>>>(a);
 }
 
 
@@ -530,6 +555,10 @@ __global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict_
 void launch_ranges(const uint32_t* sorted_tiles, const SegInfo* seg, uint2* ranges, cudaStream_t s,
                    int num_sms) {
     ranges_kernel<<<num_sms * 16, 256, 0, s>>>(sorted_tiles, seg, ranges);
+}
+
+cudaError_t radix_prepare() {
+    return cudaFuncSetAttribute(emit_expand, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EM_EXPAND_SMEM);
 }
 
 }  // namespace gs

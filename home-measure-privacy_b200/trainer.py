@@ -63,7 +63,8 @@ class Renderer:
     """createRenderer() result.  One CUDA context (device, stream, buffers)."""
 
     def __init__(self, gpuTiles=True, sh_degree=0, near=0.2, batched=True, use_graph=True, device=0,
-                 raster_batch=256, lpt_order=True, rect_mode=None, instance_capacity=0, raster_ppt=1):
+                 raster_batch=256, lpt_order=True, rect_mode=None, instance_capacity=0, raster_ppt=1,
+                 tile_cull=True):
         self.lib = N.load()
         cfg = N.GsConfig()
         self.lib.gs_config_default(ctypes.byref(cfg))
@@ -76,6 +77,7 @@ class Renderer:
         cfg.lpt_order = 1 if lpt_order else 0
         cfg.instance_capacity = int(instance_capacity)
         cfg.raster_ppt = int(raster_ppt)
+        cfg.tile_cull = 1 if tile_cull else 0
         # gpuTiles=False is the reference's CPU tileLists path (trainer/gpu.js:703, :799-806):
         # here the binning always runs on the GPU, with tileLists' tile rectangle.
         cfg.rect_mode = int(rect_mode) if rect_mode is not None else (0 if gpuTiles else 1)

@@ -75,7 +75,11 @@ typedef struct GsConfig {
                               buffer grows and a synchronous step is redone.           */
     int32_t raster_ppt;    /* pixels per raster thread: 1 (256 threads per 16 x 16
                               tile) or 2 (128 threads); 0 = 1                           */
-    int32_t reserved[2];
+    int32_t tile_cull;     /* 1 (default) = a tile list holds only splats whose
+                              alpha >= alpha_min ellipse reaches the tile: same images
+                              and gradients, fewer entries; 0 = the reference's
+                              rectangle lists (rect_mode), whose keys match BIN + SORT  */
+    int32_t reserved[1];
 } GsConfig;
 
 /* Adam settings.  The per-group learning rates are the reference's (trainer/gpu.js:846,

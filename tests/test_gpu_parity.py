@@ -55,7 +55,7 @@ def test_projection_records_bit_exact(hmp, oracle, degree):
 @pytest.mark.parametrize("rect_mode", [0, 1])
 def test_tile_lists_and_keys_bit_exact(hmp, oracle, rect_mode):
     rec, cam = scene0(hmp)
-    with make(hmp, 0, rect_mode=rect_mode) as r:
+    with make(hmp, 0, rect_mode=rect_mode, tile_cull=False) as r:
         r.set_gaussians(rec)
         r.set_views([cam])
         r.forward(0, 1, images=False)
@@ -72,7 +72,7 @@ def test_tile_lists_many_views_batched(hmp, oracle):
     """Three uneven views in one batched forward: each view's lists equal the oracle's."""
     rec = hmp.synthetic_scene(30_000, 1, 7, "normal", (-4.0, 0.6), (0.0, 1.5))
     cams = hmp.ring_cameras([(333, 250), (480, 270), (200, 411)], 4.0)
-    with make(hmp, 1) as r:
+    with make(hmp, 1, tile_cull=False) as r:
         r.set_gaussians(rec)
         r.set_views(cams)
         r.forward(0, 3, images=False)
@@ -84,17 +84,53 @@ def test_tile_lists_many_views_batched(hmp, oracle):
             assert np.array_equal(keys, ref_keys)
 
 
+def test_culled_tile_lists_are_subsequences_with_identical_results(hmp, oracle):
+    """tile_cull drops only splats whose alpha >= 1/255 ellipse misses the tile: each list
+    is an order-preserving subsequence of the reference list, images are bit-identical
+    and gradients agree."""
+    rec = hmp.synthetic_scene(40_000, 3, 5, "normal", (-4.5, 0.7), (0.0, 1.5))
+    cams = hmp.ring_cameras([(640, 480), (512, 300)], 4.0)
+    dl = None
+    out = {}
+    for cull in (False, True):
+        with make(hmp, 3, tile_cull=cull) as r:
+            r.set_gaussians(rec)
+            r.set_views(cams)
+            img = r.forward(0, 2)
+            lists = [r.tile_lists(v) for v in range(2)]
+            if dl is None:
+                dl = np.random.default_rng(0).standard_normal(img.size).astype(np.float32) * 1e-3
+            g = r.backward(dl)
+            out[cull] = (img, lists, g)
+    assert np.array_equal(out[True][0], out[False][0])
+    for v in range(2):
+        full_l, full_r, _ = out[False][1][v]
+        cul_l, cul_r, _ = out[True][1][v]
+        assert len(cul_l) < len(full_l)
+        for t in range(full_r.shape[0]):
+            a = full_l[full_r[t, 0]:full_r[t, 1]]
+            b = cul_l[cul_r[t, 0]:cul_r[t, 1]]
+            it = iter(a.tolist())
+            assert all(x in it for x in b.tolist()), t  # subsequence, same order
+    assert rel_err(out[True][2], out[False][2]) < 1e-4
+
+
 # ------------------------------------------------------------------------------- forward
 def test_render_matches_oracle(hmp, oracle):
     rec, cam = scene0(hmp)
-    with make(hmp, 0) as r:
-        img, state = r.render(rec, cam, state=True)
     ref = oracle.render_ref(cam, rec, 0, near=0.2)
+    # Reference lists: image, final transmittance and list position (state) all match.
+    with make(hmp, 0, tile_cull=False) as r:
+        img, state = r.render(rec, cam, state=True)
     assert np.abs(img - ref["image"]).max() < IMG_TOL
-    # final transmittance and list position
     assert np.abs(state[0::2] - ref["state"][0::2]).max() < 1e-4
     agree = np.mean(state[1::2] == ref["state"][1::2])
     assert agree > 0.999
+    # Culled lists: the same image and transmittance (list positions count fewer entries).
+    with make(hmp, 0) as r:
+        img_c, state_c = r.render(rec, cam, state=True)
+    assert np.array_equal(img_c, img)
+    assert np.array_equal(state_c[0::2], state[0::2])
 
 
 def test_render_reference_scene(hmp, oracle):
