@@ -134,6 +134,8 @@ def run_b200(args, rank, local, world, dist):
     hmp = importlib.import_module("home-measure-privacy_b200")
     from importlib import import_module
     N = import_module("home-measure-privacy_b200._native")
+    DP = import_module("home-measure-privacy_b200.data_parallel")
+    dp = dist is not None
     device = local
     c, cams = workload(hmp, rank, world)
     targets = make_targets(hmp, c, cams, device)
@@ -156,18 +158,38 @@ def run_b200(args, rank, local, world, dist):
             off += px
         return r
 
-    def timed(r, steps, warmup, host=None):
-        for _ in range(warmup):
-            r.train_step(ad, lam, window, loss=False, host_targets=host)
+    trainer = {}
+
+    def one_step(r, host, want_loss):
+        if dp:
+            # data parallel: gradients of this rank's views, one NCCL all-reduce of the
+            # gradient buffer on the library's stream, the same Adam update on every rank
+            if host is not None:
+                off = 0
+                for v, cm in enumerate(cams):
+                    px = cm["width"] * cm["height"] * 3
+                    r.set_target(v, host[off:off + px])
+                    off += px
+            tr = trainer.setdefault(id(r), DP.DataParallelTrainer(r, first=0, count=V))
+            return tr.step(ad, lam, window, wait=want_loss)
+        return r.train_step(ad, lam, window, loss=want_loss, host_targets=host)
+
+    def sync_all(r):
         r.synchronize()
-        r.stage_times_reset()
         if dist:
             dist.barrier()
         r.synchronize()
+
+    def timed(r, steps, warmup, host=None):
+        for _ in range(warmup):
+            one_step(r, host, False)
+        r.synchronize()
+        r.stage_times_reset()
+        sync_all(r)
         lib, ctx = r.lib, r.ctx
         N.check(lib.gs_event_record(ctx, 0))
         for _ in range(steps):
-            r.train_step(ad, lam, window, loss=host is not None, host_targets=host)
+            one_step(r, host, host is not None)
         N.check(lib.gs_event_record(ctx, 1))
         ms = ctypes.c_float(0.0)
         N.check(lib.gs_event_elapsed(ctx, 0, 1, ctypes.byref(ms)))
@@ -175,7 +197,7 @@ def run_b200(args, rank, local, world, dist):
         t = ms.value
         if dist:
             import torch
-            x = torch.tensor([t], dtype=torch.float64)
+            x = torch.tensor([t], dtype=torch.float64, device=f"cuda:{device}")
             dist.all_reduce(x, op=dist.ReduceOp.MAX)
             t = float(x.item())
         return t
@@ -196,17 +218,20 @@ def run_b200(args, rank, local, world, dist):
     # ---- e2e through the public API: pinned host targets in, loss out, every step
     e2e = None
     if not args.no_e2e:
-        host = ctypes.c_void_p()
-        N.check(r.lib.gs_host_alloc(targets.nbytes, ctypes.byref(host)))
-        ctypes.memmove(host.value, targets.ctypes.data, targets.nbytes)
-        t_e = timed(r, args.steps, 2, host=host)
-        N.check(r.lib.gs_host_free(host))
+        if dp:
+            t_e = timed(r, args.steps, 2, host=targets)
+        else:
+            host = ctypes.c_void_p()
+            N.check(r.lib.gs_host_alloc(targets.nbytes, ctypes.byref(host)))
+            ctypes.memmove(host.value, targets.ctypes.data, targets.nbytes)
+            t_e = timed(r, args.steps, 2, host=host)
+            N.check(r.lib.gs_host_free(host))
         e2e = dict(value=world * 1000.0 / (t_e / args.steps), unit="steps/s", h2d_bytes_per_step=int(targets.nbytes),
                    d2h_bytes_per_step=int(ctypes.sizeof(ctypes.c_float) * 0 + 64))
     r.close()
     # ---- plain: one view per launch per stage, same step
     plain = None
-    if not args.no_plain:
+    if not args.no_plain and not dp:
         rp = setup(False)
         t_p = timed(rp, max(3, args.steps // 2), 2)
         plain = 1000.0 / (t_p / max(3, args.steps // 2))
@@ -217,10 +242,39 @@ def run_b200(args, rank, local, world, dist):
     return res
 
 
-def cpu_baseline(hmp, sample_seconds=20.0):
+def profile_case(args):
+    """Small case for ncu captures (one kernel, few launches, ~2 GB on the device): the
+    benchmark scene (1M Gaussians, SH3) seen by its three largest views, raster variants
+    fixed at batch 256, 2 pixels per thread (the tuned backward variant), three
+    graph-replayed training steps."""
+    hmp = importlib.import_module("home-measure-privacy_b200")
+    c = hmp.config(3)
+    cams = c["cameras"][-3:]
+    targets = make_targets(hmp, c, cams, 0)
+    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=256, raster_ppt=2,
+                            device=0) as r:
+        r.set_gaussians(c["records"])
+        r.set_views(cams)
+        off = 0
+        for v, cm in enumerate(cams):
+            px = cm["width"] * cm["height"] * 3
+            r.set_target(v, targets[off:off + px])
+            off += px
+        ad = hmp.adam_config()
+        for _ in range(3):
+            loss = r.train_step(ad, c["ssim_lambda"], c["window"])
+        st = r.stats()
+        print(json.dumps(dict(case="profile", views=len(cams), pixels=int(st["pixels"]),
+                              instances=int(st["instances"]), loss=float(loss),
+                              stages_ms=r.stage_times()["ms"])), flush=True)
+
+
+def cpu_baseline(hmp, steps=1, warmup=0, budget_s=150.0):
     """The reference's step restated in C (FP32, OpenMP, all host threads) on a bounded
-    sample: one full step of view 0 (640x480) with all 1M Gaussians; the 8-view step time
-    is that view's time scaled by the views' pixel counts."""
+    sample: each step is one full step of view 0 (640x480) with all 1M Gaussians, and the
+    8-view step time is that view's time scaled by the views' pixel counts.  Runs
+    `warmup` untimed and then `steps` timed samples, fewer when they would exceed
+    budget_s (the count timed is in `sample`)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
     O.build()
@@ -232,16 +286,24 @@ def cpu_baseline(hmp, sample_seconds=20.0):
     v = np.zeros_like(rec)
     tgt = np.zeros(cam["width"] * cam["height"] * 3, np.float32) + 0.5
     lr = [0.025, 0.05, 0.002, 0.005, 0.001, 0.025 / 20]
-    t0 = time.perf_counter()
-    O.step(cam, rec, m, v, 3, tgt, 0.2, 1, 1, lr, near=c["near"], cap=1024)
-    dt = time.perf_counter() - t0
+    for _ in range(warmup):
+        O.step(cam, rec, m, v, 3, tgt, 0.2, 1, 1, lr, near=c["near"], cap=1024)
+    times = []
+    t_start = time.perf_counter()
+    for k in range(max(1, steps)):
+        t0 = time.perf_counter()
+        O.step(cam, rec, m, v, 3, tgt, 0.2, 1, k + 1, lr, near=c["near"], cap=1024)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start + times[-1] > budget_s:
+            break
+    dt = statistics.mean(times)
     px0 = cam["width"] * cam["height"]
     total = sum(cm["width"] * cm["height"] for cm in cams)
     step_s = dt * total / px0
     return dict(value=1.0 / step_s, unit="steps/s", cores=O.num_threads(), kind="port",
-                sample=f"one reference step (FP32 C restatement, cap 1024) on view 0 (640x480) with all "
-                       f"1,000,000 Gaussians took {dt:.2f} s; 8-view step time scaled by pixel count "
-                       f"({total}/{px0})")
+                sample=f"{len(times)} timed reference steps (FP32 C restatement, per-tile cap 1024) on view 0 "
+                       f"(640x480) with all 1,000,000 Gaussians, mean {dt:.3f} s; 8-view step time scaled by "
+                       f"pixel count ({total}/{px0})", samples=len(times))
 
 
 def roofline(res, peaks):
@@ -275,15 +337,25 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--dp", action="store_true",
+                    help="use the data-parallel step (gradients, NCCL all-reduce, update) even on one GPU")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run the small ncu capture case instead of the benchmark")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args)
+        return
     args.warmup = max(3, args.warmup)
     rank, local, world = env_rank()
     dist = None
-    if world > 1:
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0 alone
+    if (world > 1 or args.dp) and args.impl != "reference":
         import torch
         import torch.distributed as tdist
         from datetime import timedelta
-        tdist.init_process_group("gloo", timeout=timedelta(seconds=300))
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(f"cuda:{local}"))
         dist = tdist
     hmp = importlib.import_module("home-measure-privacy_b200")
     peaks = {}
@@ -293,17 +365,14 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            cb = cpu_baseline(hmp)
-            line = dict(metric=METRIC, value=cb["value"], unit="steps/s", n_gpus=args.gpus, steps=1,
-                        warmup=0, ms_per_step=1000.0 / cb["value"], higher_is_better=True, scaling="weak",
+            cb = cpu_baseline(hmp, args.steps, args.warmup)
+            line = dict(metric=METRIC, value=cb["value"], unit="steps/s", n_gpus=args.gpus, steps=cb["samples"],
+                        warmup=args.warmup, ms_per_step=1000.0 / cb["value"], higher_is_better=True, scaling="weak",
                         vs_baseline=None, dtype="f32", data="synthetic", impl="reference",
                         config=dict(workload=WORKLOAD, gaussians=1_000_000, views=8, sh_degree=3),
                         cpu_baseline=cb,
                         e2e=dict(value=cb["value"], unit="steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
             print(json.dumps(line), flush=True)
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
         return
 
     res = run_b200(args, rank, local, world, dist)
@@ -321,7 +390,8 @@ def main():
                         raster_variant=dict(fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1]),
                                             bwd=dict(batch=res["tuned"]["bwd"][0], pixels_per_thread=res["tuned"]["bwd"][1])),
                         l2="inputs larger than L2: params+moments+grads 944 MB, pair records 384 MB per step",
-                        parallelism=f"dp{world} over views (own 8 views per GPU)"),
+                        parallelism=(f"dp{world}: 8 own views per GPU, gradients summed by one NCCL all-reduce "
+                                     f"per step" if dist else "dp1: one GPU, 8 views")),
             plain_steps_per_s=round(res["plain"], 4) if res["plain"] else None,
             batched_over_plain=round(value / world / res["plain"], 4) if res["plain"] else None,
             instances_per_step=int(res["stats"]["instances"]),
@@ -335,7 +405,7 @@ def main():
             ps = res["plain_stages"]
             line["plain_stages_ms_per_step"] = {k: round(v / max(1, ps["steps"]), 4) for k, v in ps["ms"].items()}
         if not args.no_cpu and world == 1:
-            line["cpu_baseline"] = cpu_baseline(hmp)
+            line["cpu_baseline"] = cpu_baseline(hmp, steps=3, warmup=0)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -64,6 +64,8 @@ VP = ctypes.c_void_p
 CTX = ctypes.c_void_p
 
 # name -> (restype, argtypes)
+GRAD_TAIL_FLOATS = 64  # GS_GRAD_TAIL_FLOATS
+
 SIGNATURES = {
     "gs_config_default": (None, [ctypes.POINTER(GsConfig)]),
     "gs_adam_default": (None, [ctypes.POINTER(GsAdamConfig)]),
@@ -95,6 +97,12 @@ SIGNATURES = {
                                           c_int32, c_int32, VP, ctypes.POINTER(c_float)]),
     "gs_train": (ctypes.c_int, [CTX, c_int32, ctypes.POINTER(GsAdamConfig), VP]),
     "gs_get_step": (ctypes.c_int, [CTX, ctypes.POINTER(c_int32)]),
+    "gs_step_gradients": (ctypes.c_int, [CTX, ctypes.POINTER(GsLossConfig), c_int32, c_int32,
+                                         ctypes.POINTER(ctypes.POINTER(c_float)), ctypes.POINTER(ctypes.c_int64)]),
+    "gs_step_apply": (ctypes.c_int, [CTX, ctypes.POINTER(GsAdamConfig), ctypes.POINTER(c_float),
+                                     ctypes.POINTER(c_int32)]),
+    "gs_get_stream": (ctypes.c_int, [CTX, ctypes.POINTER(VP)]),
+    "gs_get_blend_count": (ctypes.c_int, [CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "gs_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(VP)]),
     "gs_host_free": (ctypes.c_int, [VP]),
     "gs_synchronize": (ctypes.c_int, [CTX]),

@@ -8,12 +8,15 @@
 // through every plane (parameters, gradient, both moments), so each warp streams
 // 512-byte rows.  A step whose key instances overflowed their buffer (its tile lists
 // are truncated) skips the update.
+#include "../../include/gsb200.h"
 #include "internal.h"
 
 namespace gs {
 
 __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
-    if (a.status->overflow) return;
+    // Skip the update when this step's instances overflowed -- on every replica at once
+    // when the gradients were reduced across replicas (the tail's overflow count).
+    if (a.skip ? (*a.skip > 0.f) : (a.status->overflow != 0u)) return;
     const int i4 = blockIdx.x * blockDim.x + threadIdx.x;  // group of 4 Gaussians
     const int i = i4 * 4;
     if (i >= a.n_pad) return;
@@ -114,6 +117,40 @@ void launch_step_end(DevStatus* status, const double* acc, const ViewDesc* views
 void launch_loss_from_acc(DevStatus* status, const double* acc, const ViewDesc* views, int view_first,
                           int num_views, float lambda, int window, cudaStream_t s) {
     step_end_kernel<<<1, 1, 0, s>>>(status, acc, views, view_first, num_views, lambda, window, 0);
+}
+
+// Tail of the gradient buffer after the gradients-only phase: [0] sum over this replica's
+// views of their mean losses, [1] 1 if its instances overflowed, [2] its view count.
+// Reduced (summed) across replicas together with the gradients.
+__global__ void grad_tail_kernel(const DevStatus* st, const double* acc, const ViewDesc* views, int view_first,
+                                 int num_views, float lambda, int window, float* tail) {
+    const int t = threadIdx.x;
+    if (t == 0) tail[0] = step_loss(acc, views, view_first, num_views, lambda, window) * (float)num_views;
+    else if (t == 1) tail[1] = st->overflow ? 1.f : 0.f;
+    else if (t == 2) tail[2] = (float)num_views;
+    else if (t < GS_GRAD_TAIL_FLOATS) tail[t] = 0.f;
+}
+
+void launch_grad_tail(const DevStatus* status, const double* acc, const ViewDesc* views, int view_first,
+                      int num_views, float lambda, int window, float* tail, cudaStream_t s) {
+    grad_tail_kernel<<<1, GS_GRAD_TAIL_FLOATS, 0, s>>>(status, acc, views, view_first, num_views, lambda, window,
+                                                       tail);
+}
+
+// Book-keeping after the update from a reduced tail: loss = mean over all replicas'
+// views, skipped when any replica overflowed.
+__global__ void reduced_step_end_kernel(DevStatus* st, const float* tail) {
+    const float views = fmaxf(tail[2], 1.f);
+    const float loss = tail[0] / views;
+    const bool skip = tail[1] > 0.f;
+    st->loss = loss;
+    st->nonfinite = isfinite(loss) ? 0 : 1;
+    st->skipped = skip ? 1 : 0;
+    if (!skip) st->step_t += 1;
+}
+
+void launch_reduced_step_end(DevStatus* status, const float* tail, cudaStream_t s) {
+    reduced_step_end_kernel<<<1, 1, 0, s>>>(status, tail);
 }
 
 // Screen gradients of one view in the reference's 16-float per-Gaussian layout

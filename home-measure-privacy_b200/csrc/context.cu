@@ -94,6 +94,7 @@ struct TimingSlot {
 
 struct GraphKey {
     int first, count, batched, window, kind, loss_lambda_bits;
+    int phase;  // 0 = whole step, 1 = gradients only (data-parallel split)
     GsAdamConfig adam;
     bool operator<(const GraphKey& o) const { return memcmp(this, &o, sizeof(GraphKey)) < 0; }
 };
@@ -106,7 +107,8 @@ struct GsContext {
     std::string device_name;
     // scene
     int n = 0, n_pad = 0, degree = 0, planes = 14;
-    DevBuf params, grads, mom1, mom2;
+    DevBuf params, grads, mom1, mom2;   // grads: planes x n_pad, then GS_GRAD_TAIL_FLOATS
+    bool grads_pending = false;         // gs_step_gradients queued, gs_step_apply not yet
     // views: training views [0, V) plus one scratch view at index V for render /
     // gradients / loss-gradient calls on arbitrary cameras or images
     std::vector<GsCamera> cams;
@@ -629,8 +631,28 @@ static void fill_lrs(GsContext* c, const GsAdamConfig& ad, float* lr) {
 }
 
 // The whole training step (no host synchronisation inside).
+static float* grad_tail(GsContext* c) { return c->grads.as<float>() + (size_t)c->planes * c->n_pad; }
+
+static void fill_adam_args(GsContext* c, const GsAdamConfig& ad, AdamArgs& aa) {
+    memset(&aa, 0, sizeof aa);
+    aa.params = c->params.as<float>();
+    aa.grads = c->grads.as<float>();
+    aa.m = c->mom1.as<float>();
+    aa.v = c->mom2.as<float>();
+    aa.n = c->n;
+    aa.n_pad = c->n_pad;
+    aa.planes = c->planes;
+    fill_lrs(c, ad, aa.lr);
+    aa.beta1 = ad.beta1;
+    aa.beta2 = ad.beta2;
+    aa.eps = ad.eps;
+    aa.status = c->status.as<DevStatus>();
+}
+
+// phase 0: the whole step; phase 1: forward, loss and backward only, then the gradient
+// buffer's tail (loss sum, overflow, views) for a cross-replica reduction.
 static int enqueue_step(GsContext* c, const GsAdamConfig& ad, const GsLossConfig& lc, int first, int count,
-                        bool batched, int kind) {
+                        bool batched, int kind, int phase = 0) {
     CK(cudaMemsetAsync(c->acc.p, 0, sizeof(double) * 2 * (GS_MAX_VIEWS + 1), c->stream));
     if (batched) {
         CKI(enqueue_forward(c, first, count, true));
@@ -645,21 +667,16 @@ static int enqueue_step(GsContext* c, const GsAdamConfig& ad, const GsLossConfig
             CKI(enqueue_backward_view(c, v, first, 1, false, v > first));
         }
     }
+    if (phase == 1) {
+        launch_grad_tail(c->status.as<DevStatus>(), c->acc.as<double>(), c->views_d.as<ViewDesc>(), first, count,
+                         lc.ssim_lambda, lc.window, grad_tail(c), c->stream);
+        count_launches(c, ST_PROJECT_BWD, 1);
+        CK(cudaGetLastError());
+        return GS_OK;
+    }
     CKI(mark(c, ST_ADAM));
     AdamArgs aa;
-    memset(&aa, 0, sizeof aa);
-    aa.params = c->params.as<float>();
-    aa.grads = c->grads.as<float>();
-    aa.m = c->mom1.as<float>();
-    aa.v = c->mom2.as<float>();
-    aa.n = c->n;
-    aa.n_pad = c->n_pad;
-    aa.planes = c->planes;
-    fill_lrs(c, ad, aa.lr);
-    aa.beta1 = ad.beta1;
-    aa.beta2 = ad.beta2;
-    aa.eps = ad.eps;
-    aa.status = c->status.as<DevStatus>();
+    fill_adam_args(c, ad, aa);
     launch_adam(aa, c->stream);
     launch_step_end(c->status.as<DevStatus>(), c->acc.as<double>(), c->views_d.as<ViewDesc>(), first, count,
                     lc.ssim_lambda, lc.window, 1, c->stream);
@@ -684,7 +701,7 @@ static void drop_graphs(GsContext* c) {
 }
 
 static int capture_step(GsContext* c, StepGraph& g, const GsAdamConfig& ad, const GsLossConfig& lc, int first,
-                        int count, bool batched, int kind) {
+                        int count, bool batched, int kind, int phase = 0) {
     drop_graph(g);
     // Events used by the capture are created before it starts.
     while (c->capture_events.size() < 1024) {
@@ -699,7 +716,7 @@ static int capture_step(GsContext* c, StepGraph& g, const GsAdamConfig& ad, cons
         c->capturing = false;
         return fail(GS_ERR_CUDA, "cudaStreamBeginCapture failed: %s", cudaGetErrorString(e));
     }
-    int rc = enqueue_step(c, ad, lc, first, count, batched, kind);
+    int rc = enqueue_step(c, ad, lc, first, count, batched, kind, phase);
     if (rc == GS_OK) rc = end_record(c);
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(c->stream, &graph);
@@ -959,11 +976,11 @@ static int upload_planes(GsContext* c, int n, const std::vector<float>& planes_h
     if (c->n_pad == 0) c->n_pad = 128;
     const size_t bytes = (size_t)c->planes * c->n_pad * 4;
     CKI(ensure(c->params, bytes, c));
-    CKI(ensure(c->grads, bytes, c));
+    CKI(ensure(c->grads, bytes + GS_GRAD_TAIL_FLOATS * 4, c));
     CKI(ensure(c->mom1, bytes, c));
     CKI(ensure(c->mom2, bytes, c));
     CK(cudaMemcpyAsync(c->params.p, planes_host.data(), bytes, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(c->grads.p, 0, bytes, c->stream));
+    CK(cudaMemsetAsync(c->grads.p, 0, bytes + GS_GRAD_TAIL_FLOATS * 4, c->stream));
     CK(cudaMemsetAsync(c->mom1.p, 0, bytes, c->stream));
     CK(cudaMemsetAsync(c->mom2.p, 0, bytes, c->stream));
     CK(cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream));
@@ -1487,6 +1504,79 @@ int gs_train_step_host(GsContext* c, const GsAdamConfig* adam, const GsLossConfi
     return train_step_impl(c, adam, loss, first, count, targets_u8, loss_out);
 }
 
+int gs_step_gradients(GsContext* c, const GsLossConfig* lc, int32_t first, int32_t count, float** grads_device,
+                      int64_t* num_floats) {
+    CTX_CHECK(c);
+    CKI(check_loss(lc));
+    CKI(check_range(c, first, count, false));
+    if (!grads_device || !num_floats) return fail(GS_ERR_INVALID_ARG, "null output pointer");
+    int kind;
+    CKI(targets_kind(c, first, count, &kind));
+    CKI(size_pairs(c, count));
+    CKI(poll_status(c, false));
+    CKI(ensure_capacity(c, first, count));
+    const bool batched = c->cfg.batched != 0;
+    const GsAdamConfig ad = {};
+    if (c->cfg.use_graph) {
+        GraphKey key;
+        memset(&key, 0, sizeof key);
+        key.first = first;
+        key.count = count;
+        key.batched = batched;
+        key.window = lc->window;
+        key.kind = kind;
+        key.phase = 1;
+        memcpy(&key.loss_lambda_bits, &lc->ssim_lambda, 4);
+        StepGraph& g = c->graphs[key];
+        if (!g.exec || g.generation != c->generation) CKI(capture_step(c, g, ad, *lc, first, count, batched, kind, 1));
+        CKI(launch_graph(c, g));
+    } else {
+        CKI(begin_record(c));
+        CKI(enqueue_step(c, ad, *lc, first, count, batched, kind, 1));
+        CKI(end_record(c));
+    }
+    c->last_first = first;
+    c->last_count = count;
+    c->last_batched = batched;
+    c->have_loss = true;
+    c->grads_pending = true;
+    *grads_device = c->grads.as<float>();
+    *num_floats = (int64_t)c->planes * c->n_pad + GS_GRAD_TAIL_FLOATS;
+    return GS_OK;
+}
+
+int gs_step_apply(GsContext* c, const GsAdamConfig* ad, float* loss_out, int32_t* skipped_out) {
+    CTX_CHECK(c);
+    CKI(check_adam(ad));
+    if (!c->grads_pending) return fail(GS_ERR_STATE, "gs_step_apply without gs_step_gradients");
+    c->grads_pending = false;
+    AdamArgs aa;
+    fill_adam_args(c, *ad, aa);
+    aa.skip = grad_tail(c) + 1;
+    launch_adam(aa, c->stream);
+    launch_reduced_step_end(c->status.as<DevStatus>(), grad_tail(c), c->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->status_host, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->status_event, c->stream));
+    c->status_pending = true;
+    if (!loss_out && !skipped_out) return GS_OK;
+    const DevStatus* h = c->status_host;
+    CK(cudaEventSynchronize(c->status_event));
+    const float loss = h->loss;
+    const int skipped = h->skipped;
+    CKI(poll_status(c, true));
+    if (loss_out) *loss_out = loss;
+    if (skipped_out) *skipped_out = skipped;
+    return GS_OK;
+}
+
+int gs_get_stream(GsContext* c, void** stream_out) {
+    CTX_CHECK(c);
+    if (!stream_out) return fail(GS_ERR_INVALID_ARG, "stream_out is null");
+    *stream_out = (void*)c->stream;
+    return GS_OK;
+}
+
 int gs_train(GsContext* c, int32_t steps, const GsAdamConfig* adam, float* losses_out) {
     CTX_CHECK(c);
     if (steps < 0) return fail(GS_ERR_INVALID_ARG, "steps < 0");
@@ -1605,6 +1695,25 @@ int gs_get_stats(GsContext* c, GsStats* out) {
     out->raster_threads = 256 / c->ppt_bwd;
     out->raster_variant = c->batch_fwd | (c->ppt_fwd << 12) | (c->batch_bwd << 16) | (c->ppt_bwd << 28);
     out->overflow = (int32_t)c->skipped_steps;
+    return GS_OK;
+}
+
+int gs_get_blend_count(GsContext* c, uint64_t* blends_out) {
+    CTX_CHECK(c);
+    if (!blends_out) return fail(GS_ERR_INVALID_ARG, "blends_out is null");
+    if (c->last_first < 0 || c->last_count < 1) return fail(GS_ERR_STATE, "no forward yet");
+    int maxpx = 0;
+    for (int v = c->last_first; v < c->last_first + c->last_count; v++)
+        maxpx = std::max(maxpx, c->vdesc[v].width * c->vdesc[v].height);
+    CKI(ensure(c->scratch16, 64, c));
+    CK(cudaMemsetAsync(c->scratch16.p, 0, 8, c->stream));
+    launch_blend_count(c->views_d.as<ViewDesc>(), c->last_first, c->last_count, maxpx, c->ranges.as<uint2>(),
+                       c->last.as<uint32_t>(), c->scratch16.as<unsigned long long>(), c->stream);
+    CK(cudaGetLastError());
+    unsigned long long n = 0;
+    CK(cudaMemcpyAsync(&n, c->scratch16.p, 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *blends_out = (uint64_t)n;
     return GS_OK;
 }
 

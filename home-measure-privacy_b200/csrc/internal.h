@@ -121,6 +121,10 @@ void launch_raster_fwd(const RasterArgs& a, int batch, int ppt, int persistent_c
 void launch_raster_bwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s);
 int raster_max_ctas_per_sm(int batch, int ppt, bool backward);
 
+// Blends (pixel, splat evaluations) of the last forward, added to *out.
+void launch_blend_count(const ViewDesc* views, int view_first, int num_views, int max_pixels, const uint2* ranges,
+                        const uint32_t* last, unsigned long long* out, cudaStream_t s);
+
 // Tiles ordered by descending list length (for the persistent queue).
 void launch_tile_order(const uint2* ranges, int tile_first, int num_tiles, uint32_t* order,
                        uint32_t* scratch, cudaStream_t s);
@@ -153,8 +157,14 @@ struct AdamArgs {
     float lr[GS_MAX_PLANES];
     float beta1, beta2, eps;
     DevStatus* status;
+    const float* skip;              // reduced overflow count (nullptr: this replica's status)
 };
 void launch_adam(const AdamArgs& a, cudaStream_t s);
+
+// Data-parallel split: the gradient buffer's tail and the step's end from a reduced tail.
+void launch_grad_tail(const DevStatus* status, const double* acc, const ViewDesc* views, int view_first,
+                      int num_views, float lambda, int window, float* tail, cudaStream_t s);
+void launch_reduced_step_end(DevStatus* status, const float* tail, cudaStream_t s);
 
 // Finishes a step: loss from the accumulators, skip flag, Adam step counter.
 void launch_step_end(DevStatus* status, const double* acc, const ViewDesc* views,

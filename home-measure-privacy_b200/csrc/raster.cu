@@ -521,4 +521,30 @@ void launch_tile_order(const uint2* ranges, int tile_first, int num_tiles, uint3
     tile_order_kernel<<<1, 1024, 0, s>>>(ranges, tile_first, num_tiles, order);
 }
 
+// Blends of the last forward: sum over pixels of (last contributor + 1 - tile start),
+// the (pixel, splat) evaluations the per-pixel blend of trainer/gpu.js:114-136 makes
+// before the pixel stops; the backward replays the same pairs.
+__global__ void blend_count_kernel(const ViewDesc* views, int view_first, const uint2* ranges,
+                                   const uint32_t* last, unsigned long long* out) {
+    const ViewDesc& vw = views[view_first + blockIdx.y];
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long n = 0;
+    if (px < vw.width * vw.height) {
+        const int x = px % vw.width, y = px / vw.width;
+        const int tile = vw.tile_offset + (y / GS_TILE) * vw.tiles_x + x / GS_TILE;
+        const uint32_t start = ranges[tile].x, l = last[(size_t)vw.pixel_offset + px];
+        n = l > start ? (unsigned long long)(l - start) : 0ull;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(out, n);
+}
+
+void launch_blend_count(const ViewDesc* views, int view_first, int num_views, int max_pixels, const uint2* ranges,
+                        const uint32_t* last, unsigned long long* out, cudaStream_t s) {
+    if (num_views <= 0 || max_pixels <= 0) return;
+    dim3 grid((max_pixels + 255) / 256, num_views);
+    blend_count_kernel<<<grid, 256, 0, s>>>(views, view_first, ranges, last, out);
+}
+
 }  // namespace gs

@@ -278,10 +278,65 @@ class Renderer:
             N.check(self.lib.gs_train_step(self.ctx, ctypes.byref(ad), ctypes.byref(lc), first, count, lp))
         return v.value if loss else None
 
+    # ---- data-parallel split (one replica per GPU; see data_parallel.py)
+    def step_gradients(self, ssim=0.2, window=1, first=0, count=None):
+        """Forward, loss and backward of views [first, first+count) without the update.
+        Returns (device address, float count) of the gradient buffer: num_params x n_pad
+        floats, then GRAD_TAIL_FLOATS floats [loss sum, overflow, view count, 0...]."""
+        count = len(self._views) - first if count is None else count
+        lc = N.GsLossConfig(float(ssim), int(window))
+        ptr = ctypes.POINTER(ctypes.c_float)()
+        n = ctypes.c_int64(0)
+        N.check(self.lib.gs_step_gradients(self.ctx, ctypes.byref(lc), first, count, ctypes.byref(ptr),
+                                           ctypes.byref(n)))
+        self._grad_buf = (ctypes.cast(ptr, ctypes.c_void_p).value, int(n.value))
+        return self._grad_buf
+
+    def gradient_tensor(self):
+        """torch tensor aliasing the gradient buffer of the last step_gradients (no copy)."""
+        import torch
+
+        addr, n = self._grad_buf
+
+        class _Buf:
+            __cuda_array_interface__ = dict(shape=(n,), typestr="<f4", data=(addr, False), version=3,
+                                            strides=None)
+
+        return torch.as_tensor(_Buf(), device=f"cuda:{self.device}")
+
+    def stream_handle(self):
+        """The context's cudaStream_t as an integer."""
+        st = ctypes.c_void_p()
+        N.check(self.lib.gs_get_stream(self.ctx, ctypes.byref(st)))
+        return st.value or 0
+
+    def torch_stream(self):
+        import torch
+
+        return torch.cuda.ExternalStream(self.stream_handle(), device=f"cuda:{self.device}")
+
+    def step_apply(self, adam=None, wait=True):
+        """Adam update from the (reduced) gradient buffer.  wait: return (mean loss over
+        the reduced views, skipped); otherwise None without waiting."""
+        ad = adam if adam is not None else adam_config()
+        if not wait:
+            N.check(self.lib.gs_step_apply(self.ctx, ctypes.byref(ad), None, None))
+            return None
+        v = ctypes.c_float(0.0)
+        sk = ctypes.c_int32(0)
+        N.check(self.lib.gs_step_apply(self.ctx, ctypes.byref(ad), ctypes.byref(v), ctypes.byref(sk)))
+        return v.value, bool(sk.value)
+
     def stats(self):
         s = N.GsStats()
         N.check(self.lib.gs_get_stats(self.ctx, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in N.GsStats._fields_}
+
+    def blend_count(self):
+        """(pixel, splat) blends of the last forward."""
+        n = ctypes.c_uint64(0)
+        N.check(self.lib.gs_get_blend_count(self.ctx, ctypes.byref(n)))
+        return int(n.value)
 
     def step_count(self):
         t = ctypes.c_int32(0)

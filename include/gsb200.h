@@ -226,6 +226,34 @@ GS_API int gs_train_step_host(GsContext* ctx, const GsAdamConfig* adam, const Gs
  * L1 (the reference reads the image back every step). */
 GS_API int gs_train(GsContext* ctx, int32_t steps, const GsAdamConfig* adam, float* losses_out);
 
+/* Data-parallel split of gs_train_step, for replicas that hold the same Gaussians and
+ * train on different views (one process per GPU).  The reference trains on one device
+ * and has no counterpart; the pair replaces trainScene's step (trainer/gpu.js:915-933)
+ * when its views are spread over several GPUs.
+ *
+ * gs_step_gradients queues forward, loss and backward of views [first, first+count) on
+ * the context's stream and leaves the parameter gradients in the context's gradient
+ * buffer: num_params x n_pad floats (plane-major, n_pad = n rounded up to 128) followed
+ * by GS_GRAD_TAIL_FLOATS floats: [0] the sum over these views of their mean losses,
+ * [1] 1 if the step's key instances overflowed their buffer, [2] the view count, rest 0.
+ * *grads_device gets the buffer's device address and *num_floats its length.  Sum the
+ * whole buffer across replicas (e.g. an NCCL all-reduce on gs_get_stream's stream),
+ * then call gs_step_apply.  The address stays valid until the scene changes size. */
+#define GS_GRAD_TAIL_FLOATS 64
+GS_API int gs_step_gradients(GsContext* ctx, const GsLossConfig* loss, int32_t first_view, int32_t num_views,
+                             float** grads_device, int64_t* num_floats);
+
+/* Adam update from the (reduced) gradient buffer, queued on the context's stream.  The
+ * update is skipped on every replica when the reduced overflow count is non-zero; the
+ * instance buffer of the replica that overflowed grows before its next step, so the
+ * caller repeats the step.  loss_out (nullable, waits for the step) gets the mean loss
+ * over all reduced views; skipped_out (nullable, waits) gets 1 for a skipped update. */
+GS_API int gs_step_apply(GsContext* ctx, const GsAdamConfig* adam, float* loss_out, int32_t* skipped_out);
+
+/* The context's CUDA stream (a cudaStream_t), for work the caller orders with the
+ * library's: a collective over gs_step_gradients' buffer, a copy, an event. */
+GS_API int gs_get_stream(GsContext* ctx, void** stream_out);
+
 /* Step counter t (number of Adam updates applied since gs_set_gaussians). */
 GS_API int gs_get_step(GsContext* ctx, int32_t* t_out);
 
@@ -270,6 +298,11 @@ typedef struct GsStats {
     int32_t raster_variant;  /* fwd batch | fwd ppt << 12 | bwd batch << 16 | bwd ppt << 28 */
 } GsStats;
 GS_API int gs_get_stats(GsContext* ctx, GsStats* out);
+
+/* Blends of the last forward: the sum over its pixels of the splats each pixel walked
+ * through in its tile list until it stopped (the (pixel, splat) pairs of the blend loop,
+ * trainer/gpu.js:114-136, which the backward replays).  Waits for the stream. */
+GS_API int gs_get_blend_count(GsContext* ctx, uint64_t* blends_out);
 
 /* Sorted tile lists of the last forward for one view, in the reference's terms
  * (tileLists, trainer/gpu.js:450-481): list_out gets the splat indices of every tile
