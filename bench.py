@@ -113,21 +113,41 @@ def make_targets(hmp, c, cams, device):
     return np.round(np.clip(imgs, 0.0, 1.0) * 255.0).astype(np.uint8)
 
 
-def algorithmic_bytes(st, n, planes, views, pixels):
-    """Bytes each stage must move per step (the roofline numerators)."""
+def algorithmic_bytes(st, n, planes, views, pixels, tiles):
+    """Bytes each stage must move per step (the roofline numerators): N Gaussians of P
+    bytes, N x V pairs, I key instances, M visible pairs, px pixels."""
     P = planes * 4
     pairs = n * views
     inst = st["instances"]
+    vis = st["visible_pairs"]
     passes_pairs, passes_inst = 4, 2
     return {
         "project": n * P + pairs * (48 + 8 + 4),
         "sort_pairs": passes_pairs * pairs * (4 + 8 + 8),
         "emit": pairs * (4 + 8) * 2 + inst * 8,
         "sort_instances": passes_inst * inst * (4 + 8 + 8) + inst * 4,
+        # instance list, tile ranges, splat records of the visible pairs, per-pixel image / state
+        "raster_fwd": inst * 4 + tiles * 8 + vis * 48 + pixels * (12 + 4 + 4),
         "loss": pixels * (12 + 3 + 12),
+        # + dL/dpixel in, screen-space gradients (36 B per visible pair) out
+        "raster_bwd": inst * 4 + tiles * 8 + vis * (48 + 36) + pixels * (12 + 4 + 4),
         "project_bwd": 2 * n * P + pairs * 36,
         "adam": 7 * n * P,
     }
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` on the benchmark workload, from the committed
+    ncu summary profiles/<kernel>_1M_sh3_8views_dram.md (line 'traffic per launch: B
+    bytes'); None when there is none."""
+    path = os.path.join(REPO, "profiles", f"{kernel}_1M_sh3_8views_dram.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic per launch:"):
+                return int(line.split(":")[1].split()[0])
+    except OSError:
+        pass
+    return None
 
 
 def run_b200(args, rank, local, world, dist):
@@ -204,7 +224,7 @@ def run_b200(args, rank, local, world, dist):
 
     # ---- batched (headline)
     r = setup(True)
-    tuned = r.autotune()
+    tuned = r.autotune(args.autotune_cache)
     clocks = Clocks(device)
     clocks.start()
     time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
@@ -212,6 +232,7 @@ def run_b200(args, rank, local, world, dist):
     res["clocks"] = clocks.stop()
     stages = r.stage_times()
     st = r.stats()
+    res["blends"] = r.blend_count()
     res["stats"] = st
     res["stages"] = stages
     ms_step = t_b / args.steps
@@ -238,7 +259,7 @@ def run_b200(args, rank, local, world, dist):
         res["plain_stages"] = rp.stage_times()
         rp.close()
     res.update(ms_step=ms_step, plain=plain, e2e=e2e, tuned=tuned, n=n, V=V, pixels=pixels)
-    res["bytes"] = algorithmic_bytes(st, n, hmp.stride(c["degree"]), V, pixels)
+    res["bytes"] = algorithmic_bytes(st, n, hmp.stride(c["degree"]), V, pixels, int(st["tiles"]))
     return res
 
 
@@ -307,25 +328,33 @@ def cpu_baseline(hmp, steps=1, warmup=0, budget_s=150.0):
 
 
 def roofline(res, peaks):
-    """Roofline object of the dominant HBM-bound stage (largest time among the stages
-    with an algorithmic byte count)."""
+    """Roofline of the dominant kernel (the stage with the largest device time: the
+    raster backward, one launch per step) against the measured HBM copy bandwidth, with
+    its blends per second; and the same ratio for every stage with an algorithmic byte
+    count."""
     stages = res["stages"]
     steps = max(1, stages["steps"])
     hbm = peaks.get("hbm_gbs", 6650.0)
-    best = None
+    src = "measured" if "hbm_gbs" in peaks else "fallback"
+    per = {}
     for name, b in res["bytes"].items():
         ms = stages["ms"].get(name, 0.0) / steps
-        if ms <= 0:
-            continue
-        gbs = b / (ms * 1e-3) / 1e9
-        if best is None or ms > best[1]:
-            best = (name, ms, gbs, b)
-    if best is None:
-        return None
-    name, ms, gbs, b = best
-    return dict(kernel=name, bound="hbm", achieved=round(gbs, 1), peak=hbm, unit="GB/s",
-                frac=round(gbs / hbm, 4), traffic=None, bytes_per_launch=int(b), ms_per_launch=round(ms, 4),
-                peak_source="measured" if "hbm_gbs" in peaks else "fallback")
+        if ms > 0:
+            per[name] = dict(ms=round(ms, 4), bytes=int(b), gbs=round(b / (ms * 1e-3) / 1e9, 1),
+                             frac=round(b / (ms * 1e-3) / 1e9 / hbm, 4))
+    if not per:
+        return None, per
+    name = max(per, key=lambda k: per[k]["ms"])
+    d = per[name]
+    traffic = profiled_traffic(name)
+    out = dict(kernel=name, bound="hbm", achieved=d["gbs"], peak=hbm, unit="GB/s", frac=d["frac"],
+               traffic=traffic, bytes_per_launch=d["bytes"], ms_per_launch=d["ms"], peak_source=src)
+    if name.startswith("raster") and res.get("blends"):
+        out["blends_per_launch"] = int(res["blends"])
+        out["blends_per_s"] = float(f"{res['blends'] / (d['ms'] * 1e-3):.4g}")
+        out["note"] = ("issue-bound FP32/ALU kernel (per-pixel alpha blending and its adjoint), "
+                       "not bandwidth-bound: see profiles/raster_bwd_1M_sh3_3views_full.md")
+    return out, per
 
 
 def main():
@@ -339,6 +368,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--dp", action="store_true",
                     help="use the data-parallel step (gradients, NCCL all-reduce, update) even on one GPU")
+    ap.add_argument("--autotune-cache", default=None,
+                    help="file caching the raster variant choice (a profiled run then uses the unprofiled choice)")
     ap.add_argument("--profile-case", action="store_true",
                     help="run the small ncu capture case instead of the benchmark")
     args = ap.parse_args()
@@ -381,6 +412,7 @@ def main():
         value = world * 1000.0 / ms
         launches = res["stages"]["launches"]
         steps = max(1, res["stages"]["steps"])
+        rl, per_stage = roofline(res, peaks)
         line = dict(
             metric=METRIC, value=round(value, 4), unit="steps/s", n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True, scaling="weak",
@@ -398,7 +430,8 @@ def main():
             stages_ms_per_step={k: round(v / steps, 4) for k, v in res["stages"]["ms"].items()},
             gpu_launches=int(sum(launches.values()) * args.steps / steps),
             clocks=res["clocks"],
-            roofline=roofline(res, peaks),
+            roofline=rl,
+            stage_rooflines=per_stage,
             e2e=res["e2e"],
         )
         if res.get("plain_stages"):

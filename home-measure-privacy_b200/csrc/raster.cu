@@ -104,6 +104,21 @@ __device__ __forceinline__ void stage_batch(const RasterArgs& a, uint32_t first,
 }
 
 constexpr float LOG2E = 1.4426950408889634f;
+
+// 2^e by the PTX ex2.approx instruction (relative error about 2^-22; e here lies in
+// [log2(1/255), 0], far from the subnormal range the .ftz qualifier flushes).
+__device__ __forceinline__ float ex2_approx(float e) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
+    return r;
+}
+
+// 1/x by the PTX rcp.approx instruction, for x = 1 - alpha in [0.01, 1].
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 constexpr float ALPHA_Q_BAND = 1e-4f;  // |q - log2(alpha_min)| below this: reference formula
 
 // After the batch's copies landed, each staging thread derives for its splats:
@@ -143,7 +158,7 @@ __device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, co
         alpha = __fmul_rn(g1.y, expf(power));
         if (alpha < amin) return 0.f;
     } else {
-        alpha = exp2f(e);
+        alpha = ex2_approx(e);
     }
     return fminf(amax, alpha);
 }
@@ -302,13 +317,23 @@ __global__ void __launch_bounds__(256 / PPT) raster_bwd_kernel(RasterArgs a) {
     const float qthr = __log2f(a.alpha_min);
     const float qlo = qthr - ALPHA_Q_BAND, qhi = qthr + ALPHA_Q_BAND;
     float* sg8f = reinterpret_cast<float*>(a.sg8);
+    // Selector constants of this lane's reduced value g = lane / 4 (see the reduction):
+    // (k0, kop, kA, kC) and kB.
+    float4 sel;
+    float sel_b;
+    {
+        const int g = lane >> 2;
+        sel = make_float4(g < 4 ? 1.f : (g == 6 ? -0.5f : (g == 7 ? -1.f : 0.f)), g == 3 ? -1.f : 0.f,
+                          g == 4 ? 1.f : 0.f, g == 5 ? 1.f : 0.f);
+        sel_b = (g == 4 || g == 5) ? 1.f : 0.f;
+    }
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
         const TileInfo<PPT> ti = tile_info<PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
         const float pxf = (float)ti.x + 0.5f;
-        float pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], br[PPT], bg[PPT], bb[PPT];
+        float pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
         uint32_t mylast[PPT];
         unsigned int tmax = start;
 #pragma unroll
@@ -316,7 +341,7 @@ __global__ void __launch_bounds__(256 / PPT) raster_bwd_kernel(RasterArgs a) {
             pyf[p] = (float)ti.y[p] + 0.5f;
             T[p] = 0.f;
             dlr[p] = dlg[p] = dlb[p] = 0.f;
-            br[p] = bg[p] = bb[p] = 0.f;  // colour of the splats behind, "behind"
+            bd[p] = 0.f;  // dL . (colour of the splats behind), "behind"
             mylast[p] = start;
             if (ti.inside[p]) {
                 const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x;
@@ -373,6 +398,10 @@ __global__ void __launch_bounds__(256 / PPT) raster_bwd_kernel(RasterArgs a) {
                         const float4 g1 = g1s[j];
                         const float4 q = qs[j];
                         const float dx = pxf - g0.x;
+                        // Per pixel: colour terms and the moments of dP = dL/dpower over the
+                        // offsets (sum dP, dP dx, dP dy, dP dx^2, dP dx dy, dP dy^2); the
+                        // splat's conic and opacity turn the warp sums into the gradients of
+                        // (opacity logit, u, v, A, B, C) after the reduction.
                         float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                         float v8 = 0.f;
                         bool contrib = false;
@@ -384,33 +413,42 @@ __global__ void __launch_bounds__(256 / PPT) raster_bwd_kernel(RasterArgs a) {
                             if (alpha == 0.f) continue;
                             contrib = true;
                             const float4 c = cs[j];
-                            const float ioma = __frcp_rn(1.0f - alpha);
+                            const float ioma = rcp_approx(1.0f - alpha);
                             const float Tk = T[p] * ioma;
                             const float at = alpha * Tk;
                             v[0] += dlr[p] * at;
                             v[1] += dlg[p] * at;
                             v[2] += dlb[p] * at;
-                            const float dA = dlr[p] * (Tk * c.x - br[p] * ioma) + dlg[p] * (Tk * c.y - bg[p] * ioma) +
-                                             dlb[p] * (Tk * c.z - bb[p] * ioma);
-                            br[p] += c.x * at;
-                            bg[p] += c.y * at;
-                            bb[p] += c.z * at;
+                            // dL/dalpha = dL.(c T_k - behind / (1 - alpha)); only dL.behind is
+                            // kept per pixel.
+                            const float dlc = dlr[p] * c.x + dlg[p] * c.y + dlb[p] * c.z;
+                            const float dA = Tk * dlc - ioma * bd[p];
+                            bd[p] += dlc * at;
                             T[p] = Tk;
                             if (alpha < a.alpha_max) {
                                 const float dP = dA * alpha;
-                                v[3] += dP * (1.0f - g1.y);
-                                v[4] += dP * (g0.z * dx + g0.w * dy);
-                                v[5] += dP * (g1.x * dy + g0.w * dx);
-                                v[6] += dP * -0.5f * dx * dx;
-                                v[7] += dP * -dx * dy;
-                                v8 += dP * -0.5f * dy * dy;
+                                const float dPx = dP * dx, dPy = dP * dy;
+                                v[3] += dP;
+                                v[4] += dPx;
+                                v[5] += dPy;
+                                v[6] += dPx * dx;
+                                v[7] += dPx * dy;
+                                v8 += dPy * dy;
                             }
                         }
                         if (__any_sync(FULL_MASK, contrib)) {
-                            const float s = warp_sum8_transposed(v);
+                            float s = warp_sum8_transposed(v);
                             float s8 = v8;
 #pragma unroll
                             for (int o = 16; o > 0; o >>= 1) s8 += __shfl_xor_sync(FULL_MASK, s8, o);
+                            // lane 4g holds sum g: 3 -> opacity logit (x (1 - op)), 4/5 -> u/v
+                            // (A Sx + B Sy, C Sy + B Sx), 6/7 -> A/B (-Sxx/2, -Sxy), C = -Syy/2.
+                            // Branch-free: s = s (k0 + kop op + kA A + kC C) + other kB B with the
+                            // lane's selector constants.
+                            const float other = __shfl_xor_sync(FULL_MASK, s, 4);
+                            const float m0 = fmaf(sel.w, g1.x, fmaf(sel.z, g0.z, fmaf(sel.y, g1.y, sel.x)));
+                            s = fmaf(s, m0, other * (sel_b * g0.w));
+                            s8 *= -0.5f;
                             const uint32_t pair = ps[j];
                             if ((lane & 3) == 0 && s != 0.0f) atomicAdd(sg8f + (size_t)pair * 8 + (lane >> 2), s);
                             if (lane == 0 && s8 != 0.0f) atomicAdd(a.sg1 + pair, s8);
