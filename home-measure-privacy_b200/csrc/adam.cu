@@ -171,8 +171,8 @@ void launch_screen_grads16(const float4* sg8, const float* sg1, int n, float* ou
 }
 
 // Splat records in the reference's 12-float layout (trainer/gpu.js:7).
-__global__ void splats12_kernel(const float4* geo0, const float4* geo1, const float4* rgb, const uint2* rect,
-                                const uint32_t* keys, int n, float* out) {
+__global__ void splats12_kernel(const float4* geo0, const float4* geo1, const float4* rgb, const uint32_t* keys,
+                                int n, float* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 g0 = geo0[i], g1 = geo1[i], c = rgb[i];
@@ -180,13 +180,12 @@ __global__ void splats12_kernel(const float4* geo0, const float4* geo1, const fl
     o[0] = g0.x; o[1] = g0.y; o[2] = g0.z; o[3] = g0.w;
     o[4] = g1.x; o[5] = g1.y; o[6] = g1.z; o[7] = g1.w;
     o[8] = c.x; o[9] = c.y; o[10] = c.z; o[11] = c.w;
-    (void)rect;
     (void)keys;
 }
 
-void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb, const uint2* rect,
-                     const uint32_t* keys, int n, float* out12, cudaStream_t s) {
-    if (n > 0) splats12_kernel<<<(n + 255) / 256, 256, 0, s>>>(geo0, geo1, rgb, rect, keys, n, out12);
+void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb, const uint32_t* keys, int n,
+                     float* out12, cudaStream_t s) {
+    if (n > 0) splats12_kernel<<<(n + 255) / 256, 256, 0, s>>>(geo0, geo1, rgb, keys, n, out12);
 }
 
 }  // namespace gs

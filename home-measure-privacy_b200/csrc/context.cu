@@ -120,7 +120,7 @@ struct GsContext {
     DevBuf views_d, target_u8, target_f32, image, t_final, last, dl, ranges, tile_order;
     // pairs
     int64_t pair_cap = 0;
-    DevBuf geo0, geo1, rgb, rect, pkeys, pvals, pkeys_alt, pvals_alt, sg8, sg1, pcount, spans;
+    DevBuf geo0, geo1, rgb, erec, pkeys, pvals, pkeys_alt, pvals_alt, sg8, sg1, pcount;
     // instances
     int64_t inst_cap = 0;
     bool inst_cap_valid = false;
@@ -347,9 +347,8 @@ static int size_pairs(GsContext* c, int views) {
         CKI(ensure(c->geo0, (size_t)pairs * 16, c));
         CKI(ensure(c->geo1, (size_t)pairs * 16, c));
         CKI(ensure(c->rgb, (size_t)pairs * 16, c));
-        CKI(ensure(c->rect, (size_t)pairs * 8, c));
+        CKI(ensure(c->erec, (size_t)pairs * sizeof(EmitRec), c));
         CKI(ensure(c->pcount, (size_t)pairs * 4, c));
-        CKI(ensure(c->spans, (size_t)pairs * 16, c));
         CKI(ensure(c->pkeys, (size_t)pairs * 4, c));
         CKI(ensure(c->pvals, (size_t)pairs * 4, c));
         CKI(ensure(c->pkeys_alt, (size_t)pairs * 4, c));
@@ -472,13 +471,12 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     pa.geo0 = c->geo0.as<float4>();
     pa.geo1 = c->geo1.as<float4>();
     pa.rgb = c->rgb.as<float4>();
-    pa.rect = c->rect.as<uint2>();
     pa.keys = c->pkeys.as<uint32_t>();
     pa.visible = visible;
     pa.tile_cull = c->cfg.tile_cull;
     pa.alpha_min = c->cfg.alpha_min;
     pa.pcount = c->pcount.as<uint32_t>();
-    pa.spans = c->spans.as<uint4>();
+    pa.erec = c->erec.as<EmitRec>();
     launch_project_fwd(pa, c->stream);
     count_launches(c, ST_PROJECT, 1);
     // Depth sort of the pairs (31 bits: depths are positive, the sentinel is 0x7fffffff).
@@ -504,9 +502,8 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ea.sorted_pairs = c->pvals.as<uint32_t>();
     ea.pair_seg = pair_seg;
     ea.visible = visible;
-    ea.rect = c->rect.as<uint2>();
     ea.pcount = c->pcount.as<uint32_t>();
-    ea.spans = c->spans.as<uint4>();
+    ea.erec = c->erec.as<EmitRec>();
     ea.views = c->views_d.as<ViewDesc>();
     ea.view_first = step_first;  // pair / n_pad is the slot relative to the step's first view
     ea.n_pad = c->n_pad;
@@ -952,7 +949,7 @@ int gs_destroy(GsContext* c) {
     drop_graphs(c);
     DevBuf* bufs[] = {&c->params, &c->grads, &c->mom1, &c->mom2, &c->views_d, &c->target_u8, &c->target_f32,
                       &c->image, &c->t_final, &c->last, &c->dl, &c->ranges, &c->tile_order, &c->geo0, &c->geo1,
-                      &c->rgb, &c->rect, &c->pcount, &c->spans, &c->pkeys, &c->pvals, &c->pkeys_alt, &c->pvals_alt, &c->sg8, &c->sg1,
+                      &c->rgb, &c->erec, &c->pcount, &c->pkeys, &c->pvals, &c->pkeys_alt, &c->pvals_alt, &c->sg8, &c->sg1,
                       &c->ikeys, &c->ivals, &c->ikeys_alt, &c->ivals_alt, &c->hist, &c->totals, &c->block_sums,
                       &c->pair_offsets, &c->block_first_pair,
                       &c->segs, &c->visible, &c->acc, &c->scratch16, &c->status};
@@ -1253,7 +1250,7 @@ int gs_get_splats(GsContext* c, int32_t view, float* out12) {
     CKI(ensure(c->scratch16, (size_t)c->n_pad * 64, c));
     const size_t off = (size_t)slot * c->n_pad;
     launch_splats12(c->geo0.as<float4>() + off, c->geo1.as<float4>() + off, c->rgb.as<float4>() + off,
-                    c->rect.as<uint2>() + off, c->pkeys.as<uint32_t>() + off, c->n, c->scratch16.as<float>(), c->stream);
+                    c->pkeys.as<uint32_t>() + off, c->n, c->scratch16.as<float>(), c->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out12, c->scratch16.p, (size_t)c->n * 48, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));

@@ -6,6 +6,17 @@
 
 namespace gs {
 
+// What the instance emission gathers for one (view, Gaussian) pair, in one 32-byte
+// sector: the global tile of the rectangle's corner (x0, y0), tiles_x | (x1 - x0) << 16
+// | whole-rectangle flag << 31, the instance count, and the per-row tile spans.
+struct __align__(32) EmitRec {
+    uint32_t first_tile;
+    uint32_t geom;
+    uint32_t count;
+    uint32_t pad;
+    uint4 spans;             // row r < 8: tiles [xs, xe) as bytes (xs | xe << 8) << 16 * (r & 1), x0-relative
+};
+
 // Projection forward over view slots [0, num_views) of views[view_first + slot].
 struct ProjectArgs {
     const float* params;     // [planes][n_pad]
@@ -18,13 +29,12 @@ struct ProjectArgs {
     float4* geo0;            // [num_views * n_pad]
     float4* geo1;
     float4* rgb;
-    uint2* rect;
     uint32_t* keys;          // depth key, GS_KEY_SENTINEL when the pair covers no tile
     unsigned int* visible;   // optional counter of pairs with >= 1 tile
     int tile_cull;           // 1: only tiles the alpha >= alpha_min ellipse reaches
     float alpha_min;
-    uint32_t* pcount;        // instances of the pair (| GS_PCOUNT_RECT: whole rectangle)
-    uint4* spans;            // per rectangle row r < 8: tiles [xs, xe) as bytes (xs | xe << 8) << 16 * (r & 1)
+    uint32_t* pcount;        // instances of the pair (0 when it covers no tile)
+    EmitRec* erec;           // written for pairs that cover >= 1 tile
 };
 void launch_project_fwd(const ProjectArgs& a, cudaStream_t s);
 
@@ -69,9 +79,8 @@ struct EmitArgs {
     const uint32_t* sorted_pairs;   // pairs in depth order (first `visible` are real)
     const SegInfo* pair_seg;        // pair segment: base into sorted_pairs, count
     const unsigned int* visible;    // number of visible pairs in the segment
-    const uint2* rect;
     const uint32_t* pcount;
-    const uint4* spans;
+    const EmitRec* erec;
     const ViewDesc* views;
     int view_first, n_pad;
     int pair_slot_first;            // slot of the first pair of this segment
@@ -177,7 +186,7 @@ void launch_loss_from_acc(DevStatus* status, const double* acc, const ViewDesc* 
 // ---- layout conversion -----------------------------------------------------------------
 void launch_screen_grads16(const float4* sg8, const float* sg1, int n, float* out16,
                            cudaStream_t s);
-void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb, const uint2* rect,
+void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb,
                      const uint32_t* keys, int n, float* out12, cudaStream_t s);
 
 }  // namespace gs

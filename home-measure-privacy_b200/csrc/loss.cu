@@ -46,6 +46,12 @@ struct LossDims {
     static constexpr int FLOATS = C_OFF + 3 * CH * HW;
 };
 
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <typename TT>
 __device__ __forceinline__ float load_target(const TT* t, size_t idx);
 template <>
@@ -110,12 +116,16 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
             // P1: horizontal moments, S1 centre columns per task from a register window.
             for (int task = threadIdx.x; task < D::RH * NS1; task += LB_THREADS) {
                 const int r = task / NS1, c0 = (task % NS1) * S1;
-                float xs[S1 + 2 * R], ys[S1 + 2 * R];
+                // Products formed once per window element, not once per tap.
+                float xs[S1 + 2 * R], ys[S1 + 2 * R], xx[S1 + 2 * R], yy[S1 + 2 * R], xy[S1 + 2 * R];
 #pragma unroll
                 for (int t = 0; t < S1 + 2 * R; t++) {
                     const int col = c0 + t;
                     xs[t] = col < D::RW ? X[r * D::RW + col] : 0.f;
                     ys[t] = col < D::RW ? Y[r * D::RW + col] : 0.f;
+                    xx[t] = xs[t] * xs[t];
+                    yy[t] = ys[t] * ys[t];
+                    xy[t] = xs[t] * ys[t];
                 }
 #pragma unroll
                 for (int k = 0; k < S1; k++) {
@@ -123,12 +133,12 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
                     float mx = 0.f, my = 0.f, sxx = 0.f, syy = 0.f, sxy = 0.f;
 #pragma unroll
                     for (int t = 0; t < K; t++) {
-                        const float xv = xs[k + t], yv = ys[k + t], wt = w[t];
-                        mx += wt * xv;
-                        my += wt * yv;
-                        sxx += wt * xv * xv;
-                        syy += wt * yv * yv;
-                        sxy += wt * xv * yv;
+                        const float wt = w[t];
+                        mx = fmaf(wt, xs[k + t], mx);
+                        my = fmaf(wt, ys[k + t], my);
+                        sxx = fmaf(wt, xx[k + t], sxx);
+                        syy = fmaf(wt, yy[k + t], syy);
+                        sxy = fmaf(wt, xy[k + t], sxy);
                     }
                     const int o = r * D::HW + c0 + k;
                     HM[0 * D::RH * D::HW + o] = mx;
@@ -170,8 +180,11 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
                         const float a2 = 2.0f * (sxy - mx * my) + C2;
                         const float b1 = mx * mx + my * my + C1;
                         const float b2 = (sxx - mx * mx) + (syy - my * my) + C2;
-                        const float ia1 = __frcp_rn(a1), ia2 = __frcp_rn(a2);
-                        const float ib1 = __frcp_rn(b1), ib2 = __frcp_rn(b2);
+                        // The approximate reciprocal instruction (about 1 ulp) without flushing
+                        // subnormals; a1, b1 >= C1 and b2 >= C2 (variances are >= 0 up to
+                        // rounding), a2 = 2 cov + C2 may take either sign.
+                        const float ia1 = rcp_approx(a1), ia2 = rcp_approx(a2);
+                        const float ib1 = rcp_approx(b1), ib2 = rcp_approx(b2);
                         const float ssim = a1 * a2 * ib1 * ib2;
                         ca = 2.0f * ssim * (my * ia1 - my * ia2 - mx * ib1 + mx * ib2);
                         cb = -ssim * ib2;

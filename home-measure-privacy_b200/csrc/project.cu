@@ -130,10 +130,15 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
         a.geo1[pair] = make_float4(p.ok ? p.c : 0.f, p.ok ? opacity : 0.f, p.ok ? p.radius : 0.f,
                                    p.ok ? p.depth : 0.f);
         a.rgb[pair] = make_float4(r, g, b, p.ok ? 1.0f : 0.0f);
-        a.rect[pair] = make_uint2((unsigned)x0 | ((unsigned)x1 << 16), (unsigned)y0 | ((unsigned)y1 << 16));
         a.keys[pair] = covers ? __float_as_uint(p.depth) : GS_KEY_SENTINEL;
         a.pcount[pair] = covers ? count : 0u;
-        a.spans[pair] = make_uint4(sp[0], sp[1], sp[2], sp[3]);
+        if (covers) {
+            uint4* er = reinterpret_cast<uint4*>(a.erec + pair);
+            er[0] = make_uint4((uint32_t)(vw.tile_offset + y0 * vw.tiles_x + x0),
+                               (uint32_t)vw.tiles_x | ((uint32_t)(x1 - x0) << 16) | (count & GS_PCOUNT_RECT),
+                               count & ~GS_PCOUNT_RECT, 0u);
+            er[1] = make_uint4(sp[0], sp[1], sp[2], sp[3]);
+        }
         my_visible += covers ? 1u : 0u;
     }
     if (a.visible) {

@@ -431,15 +431,12 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
         for (uint32_t j = threadIdx.x; j < EM_OUT; j += EM_THREADS) s_head[j] = 0u;
         for (uint32_t j = threadIdx.x; j < np; j += EM_THREADS) {
             const uint32_t pair = __ldg(a.sorted_pairs + base + p_lo + j);
-            const uint2 r = a.rect[pair];
-            const ViewDesc& vw = a.views[a.view_first + pair / (uint32_t)a.n_pad];
-            const uint32_t x0 = r.x & 0xffffu, x1 = r.x >> 16, y0 = r.y & 0xffffu;
-            const uint32_t whole = (a.pcount[pair] & GS_PCOUNT_RECT) ? 1u : 0u;
+            const uint4* er = reinterpret_cast<const uint4*>(a.erec + pair);
+            const uint4 h = __ldg(er);
             s_off[j] = a.pair_offsets[p_lo + j];
             s_pair[j] = pair;
-            s_geom[j] = make_uint2((uint32_t)vw.tile_offset + y0 * (uint32_t)vw.tiles_x + x0,
-                                   (uint32_t)vw.tiles_x | ((x1 - x0) << 16) | (whole << 31));
-            s_span[j] = a.spans[pair];
+            s_geom[j] = make_uint2(h.x, h.y);
+            s_span[j] = __ldg(er + 1);
         }
         __syncthreads();
         // Head flags: the instance where each pair starts gets the pair's local index;
