@@ -172,7 +172,7 @@ __device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1,
 }
 
 template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT) raster_fwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(256 / PPT, 16 / PPT) raster_fwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -304,7 +304,7 @@ __device__ __forceinline__ float warp_sum8_transposed(float v[8]) {
 }
 
 template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT) raster_bwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(256 / PPT, 16 / PPT) raster_bwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
