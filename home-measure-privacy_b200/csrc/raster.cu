@@ -139,28 +139,28 @@ __device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g
 
 // alpha of splat (g0, g1, q) at offset (dx, dy), or 0 when the pixel skips it:
 // alphaAt (trainer/gpu.js:91-103).  2^q by the fast exp2; within ALPHA_Q_BAND of the
-// alpha_min threshold the reference expression min(0.99, op exp(power)) decides, so
-// skip decisions match the reference's.  Explicit rounding intrinsics keep forward and
-// backward bit-identical.
+// alpha_min threshold the reference expression min(0.99, op exp(power)) decides (a rare
+// branch), so skip decisions match the reference's.  Otherwise branch-free.  Explicit
+// rounding intrinsics keep forward and backward bit-identical.
+__device__ __forceinline__ float alpha_band(const float4& g0, const float4& g1, float dx, float dy, float amax,
+                                         float amin) {
+    const float power = __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(__fmul_rn(__fmul_rn(g0.z, dx), dx),
+                                                             __fmul_rn(__fmul_rn(g1.x, dy), dy))),
+                                  __fmul_rn(__fmul_rn(g0.w, dx), dy));
+    if (power > 0.f) return 0.f;
+    const float alpha = __fmul_rn(g1.y, expf(power));
+    return alpha < amin ? 0.f : fminf(amax, alpha);
+}
+
 __device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, float dx, float dy,
                                           float amax, float amin, float qlo, float qhi) {
-    if (fabsf(dx) > g1.z || fabsf(dy) > g1.z) return 0.f;
     const float t = __fmaf_rn(q.y, dy, __fmul_rn(q.x, dx));
     float e = __fmaf_rn(dx, t, q.w);
     e = __fmaf_rn(__fmul_rn(q.z, dy), dy, e);
-    if (e < qlo) return 0.f;
-    float alpha;
-    if (e < qhi) {
-        const float power = __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(__fmul_rn(__fmul_rn(g0.z, dx), dx),
-                                                                 __fmul_rn(__fmul_rn(g1.x, dy), dy))),
-                                      __fmul_rn(__fmul_rn(g0.w, dx), dy));
-        if (power > 0.f) return 0.f;
-        alpha = __fmul_rn(g1.y, expf(power));
-        if (alpha < amin) return 0.f;
-    } else {
-        alpha = ex2_approx(e);
-    }
-    return fminf(amax, alpha);
+    const bool inb = fabsf(dx) <= g1.z && fabsf(dy) <= g1.z;
+    float alpha = (inb && e >= qhi) ? fminf(amax, ex2_approx(e)) : 0.f;
+    if (inb && e >= qlo && e < qhi) alpha = alpha_band(g0, g1, dx, dy, amax, amin);
+    return alpha;
 }
 
 // Can splat (g0, g1) give any pixel centre of the warp's rectangle alpha >= alpha_min?
@@ -172,7 +172,7 @@ __device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1,
 }
 
 template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT, 16 / PPT) raster_fwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(256 / PPT, 4 * PPT) raster_fwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -234,17 +234,19 @@ __global__ void __launch_bounds__(256 / PPT, 16 / PPT) raster_fwd_kernel(RasterA
                     const float dx = pxf - g0.x;
 #pragma unroll
                     for (int p = 0; p < PPT; p++) {
-                        if (done[p]) continue;
-                        const float alpha = alpha_at(g0, g1, q, dx, pyf[p] - g0.y, a.alpha_max, a.alpha_min, qlo, qhi);
-                        if (alpha == 0.f) continue;
+                        // Branch-free per lane (alpha = 0 leaves colour, T and last as
+                        // they are); the warp skips the pixel row when no lane blends.
+                        float alpha = alpha_at(g0, g1, q, dx, pyf[p] - g0.y, a.alpha_max, a.alpha_min, qlo, qhi);
+                        alpha = done[p] ? 0.f : alpha;
+                        if (!__any_sync(FULL_MASK, alpha != 0.f)) continue;
                         const float4 c = cs[j];
                         const float w = alpha * T[p];
                         cr[p] += c.x * w;
                         cg[p] += c.y * w;
                         cb[p] += c.z * w;
                         T[p] *= 1.0f - alpha;
-                        last[p] = b0 + (uint32_t)j + 1u;
-                        if (T[p] <= a.t_min) done[p] = true;
+                        last[p] = alpha != 0.f ? b0 + (uint32_t)j + 1u : last[p];
+                        done[p] = done[p] || T[p] <= a.t_min;
                     }
                 }
                 all_done = true;
@@ -304,7 +306,7 @@ __device__ __forceinline__ float warp_sum8_transposed(float v[8]) {
 }
 
 template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT, 16 / PPT) raster_bwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(256 / PPT, 4 * PPT) raster_bwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -404,13 +406,15 @@ __global__ void __launch_bounds__(256 / PPT, 16 / PPT) raster_bwd_kernel(RasterA
                         // (opacity logit, u, v, A, B, C) after the reduction.
                         float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                         float v8 = 0.f;
-                        bool contrib = false;
+                        bool contrib = false;  // warp-uniform
 #pragma unroll
                         for (int p = 0; p < PPT; p++) {
-                            if (!(k < mylast[p])) continue;
+                            // Branch-free per lane: alpha = 0 adds zeros and leaves T
+                            // (T / 1) and dL.behind as they are.
                             const float dy = pyf[p] - g0.y;
-                            const float alpha = alpha_at(g0, g1, q, dx, dy, a.alpha_max, a.alpha_min, qlo, qhi);
-                            if (alpha == 0.f) continue;
+                            float alpha = alpha_at(g0, g1, q, dx, dy, a.alpha_max, a.alpha_min, qlo, qhi);
+                            alpha = k < mylast[p] ? alpha : 0.f;
+                            if (!__any_sync(FULL_MASK, alpha != 0.f)) continue;
                             contrib = true;
                             const float4 c = cs[j];
                             const float ioma = rcp_approx(1.0f - alpha);
@@ -425,18 +429,17 @@ __global__ void __launch_bounds__(256 / PPT, 16 / PPT) raster_bwd_kernel(RasterA
                             const float dA = Tk * dlc - ioma * bd[p];
                             bd[p] += dlc * at;
                             T[p] = Tk;
-                            if (alpha < a.alpha_max) {
-                                const float dP = dA * alpha;
-                                const float dPx = dP * dx, dPy = dP * dy;
-                                v[3] += dP;
-                                v[4] += dPx;
-                                v[5] += dPy;
-                                v[6] += dPx * dx;
-                                v[7] += dPx * dy;
-                                v8 += dPy * dy;
-                            }
+                            // alpha clamped at alpha_max has no gradient through the power.
+                            const float dP = alpha < a.alpha_max ? dA * alpha : 0.f;
+                            const float dPx = dP * dx, dPy = dP * dy;
+                            v[3] += dP;
+                            v[4] += dPx;
+                            v[5] += dPy;
+                            v[6] += dPx * dx;
+                            v[7] += dPx * dy;
+                            v8 += dPy * dy;
                         }
-                        if (__any_sync(FULL_MASK, contrib)) {
+                        if (contrib) {
                             float s = warp_sum8_transposed(v);
                             float s8 = v8;
 #pragma unroll
