@@ -13,52 +13,71 @@
 
 namespace gs {
 
+// One thread per (plane, 4 Gaussians) float4 of every plane except the rotation's, and
+// one per 4 Gaussians for the four rotation planes together (updated, then
+// renormalised): 14M independent float4 updates at the benchmark size, so the loads of
+// many planes are in flight at once.
+__device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, float4& v, float lr, float b1, float b2,
+                                      float omb1, float omb2, float ibc1, float ibc2, float eps) {
+    float* pp = &p.x;
+    const float* gg = &g.x;
+    float* mm = &m.x;
+    float* vv = &v.x;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        mm[e] = b1 * mm[e] + omb1 * gg[e];
+        vv[e] = b2 * vv[e] + omb2 * gg[e] * gg[e];
+        pp[e] -= lr * (mm[e] * ibc1) / (sqrtf(vv[e] * ibc2) + eps);
+    }
+}
+
 __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
     // Skip the update when this step's instances overflowed -- on every replica at once
     // when the gradients were reduced across replicas (the tail's overflow count).
     if (a.skip ? (*a.skip > 0.f) : (a.status->overflow != 0u)) return;
-    const int i4 = blockIdx.x * blockDim.x + threadIdx.x;  // group of 4 Gaussians
-    const int i = i4 * 4;
-    if (i >= a.n_pad) return;
+    const int groups = a.n_pad / 4;
+    const int units_per_group = a.planes - 3;  // planes other than 6..9, plus one rotation unit
+    const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= (long long)groups * units_per_group) return;
+    const int unit = (int)(u / groups), grp = (int)(u % groups);
     const int t = a.status->step_t + 1;
-    const float bc1 = 1.0f - powf(a.beta1, (float)t);
-    const float bc2 = 1.0f - powf(a.beta2, (float)t);
+    const float ibc1 = 1.0f / (1.0f - powf(a.beta1, (float)t));
+    const float ibc2 = 1.0f / (1.0f - powf(a.beta2, (float)t));
     const float omb1 = 1.0f - a.beta1, omb2 = 1.0f - a.beta2;
     const size_t np = (size_t)a.n_pad;
-    float4 q[4];
-#pragma unroll 1
-    for (int j = 0; j < a.planes; j++) {
-        const size_t off = (size_t)j * np + i;
+    const size_t col = (size_t)grp * 4;
+    if (unit != 6) {
+        const int j = unit < 6 ? unit : unit + 3;  // skip planes 7..9 (unit 6 = rotation)
+        const size_t off = (size_t)j * np + col;
         float4 p = *reinterpret_cast<const float4*>(a.params + off);
         const float4 g = *reinterpret_cast<const float4*>(a.grads + off);
         float4 m = *reinterpret_cast<const float4*>(a.m + off);
         float4 v = *reinterpret_cast<const float4*>(a.v + off);
-        const float lr = a.lr[j];
-        float* pp = &p.x;
-        const float* gg = &g.x;
-        float* mm = &m.x;
-        float* vv = &v.x;
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            mm[e] = a.beta1 * mm[e] + omb1 * gg[e];
-            vv[e] = a.beta2 * vv[e] + omb2 * gg[e] * gg[e];
-            pp[e] -= lr * (mm[e] / bc1) / (sqrtf(vv[e] / bc2) + a.eps);
-        }
-        if (j >= 11 && j <= 13) {
+        adam4(p, g, m, v, a.lr[j], a.beta1, a.beta2, omb1, omb2, ibc1, ibc2, a.eps);
+        if (j >= 11 && j <= 13) {  // colour (SH DC) clamped to [0, 1]
             p.x = fminf(fmaxf(p.x, 0.f), 1.f);
             p.y = fminf(fmaxf(p.y, 0.f), 1.f);
             p.z = fminf(fmaxf(p.z, 0.f), 1.f);
             p.w = fminf(fmaxf(p.w, 0.f), 1.f);
         }
-        if (j >= 6 && j <= 9) {
-            q[j - 6] = p;
-        } else {
-            *reinterpret_cast<float4*>(a.params + off) = p;
-        }
+        *reinterpret_cast<float4*>(a.params + off) = p;
+        *reinterpret_cast<float4*>(a.m + off) = m;
+        *reinterpret_cast<float4*>(a.v + off) = v;
+        return;
+    }
+    // Rotation planes 6..9: update, then renormalise the quaternions.
+    float4 q[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const size_t off = (size_t)(6 + k) * np + col;
+        q[k] = *reinterpret_cast<const float4*>(a.params + off);
+        const float4 g = *reinterpret_cast<const float4*>(a.grads + off);
+        float4 m = *reinterpret_cast<const float4*>(a.m + off);
+        float4 v = *reinterpret_cast<const float4*>(a.v + off);
+        adam4(q[k], g, m, v, a.lr[6 + k], a.beta1, a.beta2, omb1, omb2, ibc1, ibc2, a.eps);
         *reinterpret_cast<float4*>(a.m + off) = m;
         *reinterpret_cast<float4*>(a.v + off) = v;
     }
-    // Renormalise the rotations (planes 6..9).
     float* qw = &q[0].x;
     float* qx = &q[1].x;
     float* qy = &q[2].x;
@@ -72,14 +91,14 @@ __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
         qz[e] /= nrm;
     }
 #pragma unroll
-    for (int k = 0; k < 4; k++) *reinterpret_cast<float4*>(a.params + (size_t)(6 + k) * np + i) = q[k];
+    for (int k = 0; k < 4; k++) *reinterpret_cast<float4*>(a.params + (size_t)(6 + k) * np + col) = q[k];
 }
 
 void launch_adam(const AdamArgs& a, cudaStream_t s) {
-    const int groups = a.n_pad / 4;
+    const long long units = (long long)(a.n_pad / 4) * (a.planes - 3);
     const int threads = 256;
-    const int blocks = (groups + threads - 1) / threads;
-    if (blocks > 0) adam_kernel<<<blocks, threads, 0, s>>>(a);
+    const long long blocks = (units + threads - 1) / threads;
+    if (blocks > 0) adam_kernel<<<(unsigned)blocks, threads, 0, s>>>(a);
 }
 
 // Loss of a step from the per-view sums: mean over views of

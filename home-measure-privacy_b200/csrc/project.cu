@@ -13,6 +13,19 @@
 
 namespace gs {
 
+// Approximate PTX instructions for the conservative tile spans (their slack covers the
+// ~1e-6 relative error); the records themselves use exact rounding.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <int DEG>
 __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
     constexpr int NK = (DEG + 1) * (DEG + 1) - 1;
@@ -47,6 +60,10 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
 #pragma unroll
         for (int k = 0; k < 9; k++) finite = finite && isfinite(Sig[k]);
     }
+    // Culling bound of the tile spans: alpha >= alpha_min needs the conic's quadratic
+    // form <= 2 ln(opacity / alpha_min); the slack keeps the spans conservative against
+    // the approximate arithmetic below and the raster's own rounding.
+    const float thr_g = opacity > 0.f ? 2.0f * (__logf(opacity) - __logf(a.alpha_min)) + 1e-3f : -1.0f;
     unsigned int my_visible = 0;
     for (int s = 0; s < a.num_views; s++) {
         const ViewDesc& vw = a.views[a.view_first + s];
@@ -68,25 +85,30 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
                 // image): the band's x-extent of the ellipse is contiguous, its right edge
                 // concave and its left edge convex in dy, so each extreme sits at its
                 // stationary point dy* = -/+ B sqrt(thr / (det C)) clamped to the band.
-                const float thr = 2.0f * (logf(opacity) - logf(a.alpha_min)) + 1e-3f;
+                const float thr = thr_g;
                 const float A = p.a, B = p.b, C = p.c;
                 const float det = fmaxf(A * C - B * B, 1e-30f);
-                const float ymax = sqrtf(fmaxf(thr, 0.f) * A / det);
-                const float ystat = B * sqrtf(fmaxf(thr, 0.f) / (det * C));
-                const float iA = 1.0f / A;
+                const float idet = rcp_approx(det);
+                const float tp = fmaxf(thr, 0.f);
+                const float ymax = sqrt_approx(tp * A * idet);
+                const float ystat = B * sqrt_approx(tp * idet * rcp_approx(C));
+                const float iA = rcp_approx(A);
                 const float H1 = (float)vw.height - 0.5f, W1 = (float)vw.width - 0.5f;
                 const float xlo_lim = fmaxf(p.u - p.radius, 0.5f), xhi_lim = fminf(p.u + p.radius, W1);
+                const float slack = 1e-3f * (1.0f + p.radius);
                 count = 0;
-                for (int ty = y0; ty < y1; ty++) {
+#pragma unroll
+                for (int r = 0; r < GS_SPAN_ROWS; r++) {
+                    const int ty = y0 + r;
+                    if (ty >= y1) break;
                     float yl = fmaxf(fmaxf((float)(ty * GS_TILE) + 0.5f, p.v - p.radius), p.v - ymax) - p.v;
                     float yh = fminf(fminf(fminf((float)(ty * GS_TILE) + 15.5f, H1), p.v + p.radius), p.v + ymax) - p.v;
                     int xs = 0, xe = 0;
                     if (thr > 0.f && yl <= yh) {
                         const float dr = fminf(fmaxf(-ystat, yl), yh);   // right edge maximiser
                         const float dl = fminf(fmaxf(ystat, yl), yh);    // left edge minimiser
-                        const float sr = sqrtf(fmaxf(A * thr - det * dr * dr, 0.f));
-                        const float sl = sqrtf(fmaxf(A * thr - det * dl * dl, 0.f));
-                        const float slack = 1e-3f * (1.0f + p.radius);
+                        const float sr = sqrt_approx(fmaxf(A * thr - det * dr * dr, 0.f));
+                        const float sl = sqrt_approx(fmaxf(A * thr - det * dl * dl, 0.f));
                         const float xhi = fminf(p.u + (-B * dr + sr) * iA + slack, xhi_lim);
                         const float xlo = fmaxf(p.u + (-B * dl - sl) * iA - slack, xlo_lim);
                         if (xlo <= xhi) {
@@ -96,7 +118,6 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
                             if (xe < xs) xe = xs;
                         }
                     }
-                    const int r = ty - y0;
                     if (xe > xs) {
                         sp[r >> 1] |= ((uint32_t)(xs - x0) | ((uint32_t)(xe - x0) << 8)) << (16 * (r & 1));
                         count += (uint32_t)(xe - xs);
