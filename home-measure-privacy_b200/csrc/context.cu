@@ -342,7 +342,7 @@ static int set_scratch_camera(GsContext* c, const GsCamera& cam) {
 // Pair buffers for `views` view slots and the segment table.
 static int size_pairs(GsContext* c, int views) {
     const int64_t pairs = (int64_t)std::max(views, 1) * c->n_pad;
-    if (pairs > 0x7fffffffLL) return fail(GS_ERR_INVALID_ARG, "too many (view, Gaussian) pairs");
+    if (pairs > 0x3fffffffLL) return fail(GS_ERR_INVALID_ARG, "too many (view, Gaussian) pairs");
     if (pairs > c->pair_cap) {
         CKI(ensure(c->geo0, (size_t)pairs * 16, c));
         CKI(ensure(c->geo1, (size_t)pairs * 16, c));
@@ -379,7 +379,7 @@ static int write_segments(GsContext* c) {
 }
 
 static int size_instances(GsContext* c, int64_t cap) {
-    if (cap > 0xfffff000LL) cap = 0xfffff000LL;
+    if (cap > 0x3ffff000LL) cap = 0x3ffff000LL;  // the sort's look-back counts hold 30 bits
     if (cap <= c->inst_cap) return GS_OK;
     CKI(ensure(c->ikeys, (size_t)cap * 4, c));
     CKI(ensure(c->ivals, (size_t)cap * 4, c));
@@ -492,9 +492,10 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ra.end_bit = 31;
     ra.hist = c->hist.as<uint32_t>();
     ra.totals = c->totals.as<uint32_t>();
+    ra.timeout = &c->status.as<DevStatus>()->sort_timeout;
     ra.max_parts = (int)(((int64_t)vcount * c->n_pad + radix_tile_items() - 1) / radix_tile_items());
     launch_radix_sort(ra, c->stream, c->num_sms);
-    count_launches(c, ST_SORT_PAIRS, 3 * radix_sort_passes(0, 31));
+    count_launches(c, ST_SORT_PAIRS, 1 + radix_sort_passes(0, 31));
     // Key instances in depth order.
     CKI(mark(c, ST_EMIT));
     EmitArgs ea;
@@ -533,7 +534,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     rb.max_parts = (int)((c->inst_cap + radix_tile_items() - 1) / radix_tile_items());
     launch_radix_sort(rb, c->stream, c->num_sms);
     launch_ranges(c->ikeys.as<uint32_t>(), inst_seg, c->ranges.as<uint2>(), c->stream, c->num_sms);
-    count_launches(c, ST_SORT_INST, 3 * radix_sort_passes(0, c->tile_bits) + 1);
+    count_launches(c, ST_SORT_INST, 1 + radix_sort_passes(0, c->tile_bits) + 1);
     // Blend.
     RasterArgs r = raster_args(c, vfirst, vcount);
     if (batched) {
@@ -781,6 +782,7 @@ static int launch_graph(GsContext* c, StepGraph& g) {
 static int read_status(GsContext* c) {
     CK(cudaMemcpyAsync(c->status_host, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->status_host->sort_timeout) return fail(GS_ERR_CUDA, "radix sort look-back wait timed out");
     return GS_OK;
 }
 
@@ -926,7 +928,7 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if ((rc = ensure(c->status, sizeof(DevStatus), c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->visible, sizeof(unsigned) * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->acc, sizeof(double) * 2 * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
-    if ((rc = ensure(c->totals, 256 * 4, c)) != GS_OK) return bail(rc);
+    if ((rc = ensure(c->totals, 8192, c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->views_d, sizeof(ViewDesc) * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
     if (cudaMemset(c->status.p, 0, sizeof(DevStatus)) != cudaSuccess) return bail(fail(GS_ERR_CUDA, "memset"));
     if (cudaMallocHost((void**)&c->status_host, sizeof(DevStatus)) != cudaSuccess)
@@ -1423,6 +1425,7 @@ static int poll_status(GsContext* c, bool wait) {
         return GS_OK;
     }
     c->status_pending = false;
+    if (c->status_host->sort_timeout) return fail(GS_ERR_CUDA, "radix sort look-back wait timed out");
     if (c->status_host->overflow) {
         c->skipped_steps++;
         CKI(grow_instances(c, c->status_host->instances_needed));

@@ -50,7 +50,8 @@ struct DevStatus {
     int skipped;                          // the last step skipped its update
     float loss;                           // mean loss of the last step over its views
     int nonfinite;                        // last loss was not finite
-    unsigned int pad[6];
+    unsigned int sort_timeout;            // a radix look-back wait gave up (never expected)
+    unsigned int pad[5];
 };
 #define GS_STATUS_FORWARD_BYTES 24
 

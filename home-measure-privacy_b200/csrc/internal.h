@@ -65,9 +65,10 @@ struct RadixSortArgs {
     int iota;                // 1: values start as the absolute element index
     const SegInfo* seg;
     int begin_bit, end_bit;  // bits to sort
-    uint32_t* hist;          // 256 * max_parts
-    uint32_t* totals;        // 256
+    uint32_t* hist;          // look-back words, 256 * max_parts
+    uint32_t* totals;        // digit counts of every pass and partition counters (>= 1028 words)
     int max_parts;
+    unsigned int* timeout;   // set when a look-back wait gave up
 };
 int radix_sort_passes(int begin_bit, int end_bit);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms);

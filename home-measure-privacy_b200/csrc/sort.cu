@@ -81,187 +81,228 @@ __device__ __forceinline__ uint32_t warp_peers(uint32_t d, bool valid) {
     return peers;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) radix_upsweep(const uint32_t* __restrict__ keys,
-                                                            const SegInfo* seg, int shift, int bits,
-                                                            uint32_t* __restrict__ hist) {
-    __shared__ uint32_t wh[RS_WARPS][256];
+// ---------------------------------------------------------------------------------
+// Radix sort, one sweep per digit (the Onesweep scheme of Adinets and Merrill): one
+// kernel counts the digits of every pass over the whole segment; each pass is then a
+// single kernel in which a block takes the next partition of RS_TILE keys (in launch
+// order, from a counter), ranks them in shared memory, publishes its digit counts,
+// looks back over the earlier partitions' published counts for its global offsets
+// (decoupled look-back) and scatters keys and values.  Keys and values are read once
+// and written once per pass.
+//
+// Look-back words: bits 31..30 = 0 (not yet published), 1 (this partition's count),
+// 2 (inclusive prefix over partitions 0..p); bits 29..0 = the count.  A block waits only
+// on earlier partitions, which took their index earlier and wait only on theirs, so the
+// waits end; each wait is still bounded (OS_SPIN_LIMIT polls), after which the block
+// sets the timeout flag and goes on with a wrong offset instead of hanging.
+// ---------------------------------------------------------------------------------
+constexpr uint32_t OS_AGG = 1u << 30;
+constexpr uint32_t OS_INC = 2u << 30;
+constexpr uint32_t OS_VALUE = OS_AGG - 1u;
+constexpr int OS_SPIN_LIMIT = 1 << 22;
+constexpr int OS_LOOK = 8;  // look-back words read per round trip
+constexpr int OS_MAX_PASSES = 4;
+constexpr int OS_HIST_BLOCKS = 1184;  // 148 SMs x 8
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Digit counts of all passes over the segment: ghist[pass * 256 + digit].  Shared-memory
+// atomics into per-warp rows (equal digits within a warp serialise in hardware, which
+// costs little even when a byte is constant), four keys per thread per round.
+__global__ void __launch_bounds__(RS_THREADS) radix_hist_all(const uint32_t* __restrict__ keys, const SegInfo* seg,
+                                                             int begin_bit, int passes, uint32_t* __restrict__ ghist) {
+    __shared__ uint32_t wh[OS_MAX_PASSES][RS_WARPS][256];
     const uint32_t base = seg->base, n = seg->count;
-    const uint32_t P = (n + RS_TILE - 1) / RS_TILE;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t mask = (1u << bits) - 1u;
-    const uint32_t lt_mask = (1u << lane) - 1u;
-    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
-        for (int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS) (&wh[0][0])[d] = 0u;
-        __syncthreads();
-        const uint32_t start = p * RS_TILE + warp * (RS_ITEMS * 32);
-        uint32_t kk[RS_ITEMS];
+    const int warp = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < OS_MAX_PASSES * RS_WARPS * 256; d += RS_THREADS) (&wh[0][0][0])[d] = 0u;
+    __syncthreads();
+    const uint32_t stride = gridDim.x * RS_THREADS * 4;
+    for (uint32_t i0 = blockIdx.x * RS_THREADS * 4 + threadIdx.x; i0 < n; i0 += stride) {
+        uint32_t k[4];
 #pragma unroll
-        for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = start + j * 32 + lane;
-            kk[j] = idx < n ? __ldg(keys + base + idx) : 0u;  // all loads in flight together
+        for (int t = 0; t < 4; t++) {
+            const uint32_t idx = i0 + t * RS_THREADS;
+            k[t] = idx < n ? __ldg(keys + base + idx) : 0u;
         }
 #pragma unroll
-        for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = start + j * 32 + lane;
-            const bool valid = idx < n;
-            const uint32_t d = valid ? (kk[j] >> shift) & mask : 0u;
-            // The lowest lane of each group of equal digits adds the group's size to the
-            // warp's histogram: one plain shared-memory update per distinct digit.
-            const uint32_t peers = warp_peers(d, valid);
-            if (valid && (peers & lt_mask) == 0u) wh[warp][d] += __popc(peers);
+        for (int t = 0; t < 4; t++) {
+            if (i0 + t * RS_THREADS >= n) continue;
+            for (int p = 0; p < passes; p++) atomicAdd(&wh[p][warp][(k[t] >> (begin_bit + 8 * p)) & 0xffu], 1u);
         }
-        __syncthreads();
-        for (int d = threadIdx.x; d < 256; d += RS_THREADS) {
-            uint32_t s = 0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += RS_THREADS) {
+        const int p = i >> 8, d = i & 255;
+        uint32_t s = 0;
 #pragma unroll
-            for (int w = 0; w < RS_WARPS; w++) s += wh[w][d];
-            hist[(size_t)d * P + p] = s;
-        }
-        __syncthreads();
+        for (int w = 0; w < RS_WARPS; w++) s += wh[p][w][d];
+        if (s) atomicAdd(ghist + i, s);
     }
 }
 
-// One block per digit: exclusive scan of that digit's counts over the partitions.
-__global__ void __launch_bounds__(1024) radix_scan(const SegInfo* seg, uint32_t* __restrict__ hist,
-                                                   uint32_t* __restrict__ totals) {
-    __shared__ uint32_t s_tmp[32];
-    const uint32_t n = seg->count;
-    const uint32_t P = (n + RS_TILE - 1) / RS_TILE;
-    uint32_t* h = hist + (size_t)blockIdx.x * P;
-    uint32_t carry = 0;
-    for (uint32_t b = 0; b < P; b += 1024) {
-        const uint32_t idx = b + threadIdx.x;
-        const uint32_t v = idx < P ? h[idx] : 0u;
-        uint32_t tot;
-        const uint32_t ex = block_excl_scan<1024>(v, s_tmp, tot);
-        if (idx < P) h[idx] = carry + ex;
-        carry += tot;
-    }
-    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
-}
-
-__global__ void __launch_bounds__(RS_THREADS, 3) radix_downsweep(
-    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift,
-    int bits, const uint32_t* __restrict__ hist, const uint32_t* __restrict__ totals) {
+__global__ void __launch_bounds__(RS_THREADS, 3) radix_onesweep(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ ghist,
+    uint32_t* look, uint32_t* counter, unsigned int* timeout) {
     __shared__ uint32_t s_keys[RS_TILE];
     __shared__ uint32_t s_vals[RS_TILE];
     __shared__ uint32_t s_warp[RS_WARPS][256];
     __shared__ uint32_t s_digit_start[256];
     __shared__ uint32_t s_global[256];
-    __shared__ uint32_t s_total_excl[256];
     __shared__ uint32_t s_tmp[32];
+    __shared__ uint32_t s_part;
     const uint32_t base = seg->base, n = seg->count;
     const uint32_t P = (n + RS_TILE - 1) / RS_TILE;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t mask = (1u << bits) - 1u;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    if (blockIdx.x >= P) return;
+    if (threadIdx.x == 0) s_part = atomicAdd(counter, 1u);
+    for (int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS) (&s_warp[0][0])[d] = 0u;
+    __syncthreads();
+    const uint32_t p = s_part;
+    if (p >= P) return;
+    const uint32_t part_start = p * RS_TILE;
+    const uint32_t warp_start = part_start + warp * (RS_ITEMS * 32);
+    uint32_t k[RS_ITEMS], pos[RS_ITEMS];
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t idx = warp_start + j * 32 + lane;
+        k[j] = idx < n ? __ldg(keys_in + base + idx) : 0xffffffffu;
+    }
+    // Rank within the warp: equal digits by ballot, counts in the warp's row.
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t idx = warp_start + j * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = (k[j] >> shift) & 0xffu;
+        const uint32_t peers = warp_peers(d, valid);
+        uint32_t prev = 0;
+        if (valid) {
+            prev = s_warp[warp][d];
+            pos[j] = prev + __popc(peers & lt_mask);
+        }
+        __syncwarp();
+        if (valid && (peers & lt_mask) == 0u) s_warp[warp][d] = prev + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    const int d = threadIdx.x;  // RS_THREADS == 256 digits
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; w++) {
+        const uint32_t c = s_warp[w][d];
+        s_warp[w][d] = cnt;
+        cnt += c;
+    }
+    // Publish this partition's count as early as possible.
+    uint32_t* my = look + (size_t)p * 256 + d;
+    st_relaxed(my, (p == 0 ? OS_INC : OS_AGG) | cnt);
     {
         uint32_t tot;
-        const uint32_t ex = block_excl_scan<RS_THREADS>(totals[threadIdx.x], s_tmp, tot);
-        s_total_excl[threadIdx.x] = ex;
+        const uint32_t gex = block_excl_scan<RS_THREADS>(ghist[d], s_tmp, tot);
+        s_global[d] = gex;
+        const uint32_t lex = block_excl_scan<RS_THREADS>(cnt, s_tmp, tot);
+        s_digit_start[d] = lex;
     }
-    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
-        for (int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS) (&s_warp[0][0])[d] = 0u;
-        __syncthreads();
-        const uint32_t part_start = p * RS_TILE;
-        const uint32_t warp_start = part_start + warp * (RS_ITEMS * 32);
-        const uint32_t my_hist = hist[(size_t)threadIdx.x * P + p];  // digit threadIdx.x
-        uint32_t k[RS_ITEMS], rank[RS_ITEMS];
+    __syncthreads();
+    // Keys to their block-sorted slots.
 #pragma unroll
-        for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = warp_start + j * 32 + lane;
-            k[j] = idx < n ? __ldg(keys_in + base + idx) : 0xffffffffu;
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t idx = warp_start + j * 32 + lane;
+        if (idx < n) {
+            const uint32_t dj = (k[j] >> shift) & 0xffu;
+            pos[j] += s_digit_start[dj] + s_warp[warp][dj];
+            s_keys[pos[j]] = k[j];
         }
+    }
+    // Values in flight while this thread looks back for digit d.
+    uint32_t v[RS_ITEMS];
 #pragma unroll
-        for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = warp_start + j * 32 + lane;
-            const bool valid = idx < n;
-            const uint32_t d = (k[j] >> shift) & mask;
-            const uint32_t peers = warp_peers(d, valid);
-            uint32_t prev = 0;
-            if (valid) {
-                prev = s_warp[warp][d];
-                rank[j] = prev + __popc(peers & lt_mask);
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t idx = warp_start + j * 32 + lane;
+        v[j] = (idx < n) ? (vals_in ? __ldg(vals_in + base + idx) : base + idx) : 0u;
+    }
+    if (p > 0) {
+        // Walk back OS_LOOK partitions per round trip: sum published counts until an
+        // inclusive prefix; re-poll from the first partition that has published nothing.
+        uint32_t excl = 0;
+        int q = (int)p - 1;
+        int spins = 0;
+        bool done = false;
+        while (!done) {
+            uint32_t w[OS_LOOK];
+#pragma unroll
+            for (int t = 0; t < OS_LOOK; t++) w[t] = q - t >= 0 ? ld_relaxed(look + (size_t)(q - t) * 256 + d) : OS_INC;
+            int used = 0;
+            bool stop = false;
+#pragma unroll
+            for (int t = 0; t < OS_LOOK; t++) {
+                if (stop) continue;
+                const uint32_t flag = w[t] & ~OS_VALUE;
+                if (flag == 0u) {
+                    stop = true;
+                    continue;
+                }
+                excl += w[t] & OS_VALUE;
+                used++;
+                if (flag == OS_INC) {
+                    stop = true;
+                    done = true;
+                }
             }
-            __syncwarp();
-            if (valid && (peers & lt_mask) == 0u) s_warp[warp][d] = prev + __popc(peers);
-            __syncwarp();
-        }
-        __syncthreads();
-        {
-            const int d = threadIdx.x;  // RS_THREADS == 256 digits
-            uint32_t s = 0;
-#pragma unroll
-            for (int w = 0; w < RS_WARPS; w++) {
-                const uint32_t c = s_warp[w][d];
-                s_warp[w][d] = s;
-                s += c;
-            }
-            uint32_t tot;
-            const uint32_t ex = block_excl_scan<RS_THREADS>(s, s_tmp, tot);
-            s_digit_start[d] = ex;
-            s_global[d] = s_total_excl[d] + my_hist;
-        }
-        __syncthreads();
-        // Keys to their block-sorted slots; then all values are loaded at once (no load
-        // waits behind a shared-memory store) and follow the keys.
-#pragma unroll
-        for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = warp_start + j * 32 + lane;
-            if (idx < n) {
-                const uint32_t d = (k[j] >> shift) & mask;
-                rank[j] += s_digit_start[d] + s_warp[warp][d];
-                s_keys[rank[j]] = k[j];
+            q -= used;
+            if (!done && used == 0) {
+                if (++spins > OS_SPIN_LIMIT) {
+                    atomicOr(timeout, 1u);
+                    break;
+                }
+                __nanosleep(32);
             }
         }
-        uint32_t v[RS_ITEMS];
+        st_relaxed(my, OS_INC | (excl + cnt));
+        s_global[d] += excl;
+    }
 #pragma unroll
-        for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = warp_start + j * 32 + lane;
-            v[j] = (idx < n) ? (vals_in ? __ldg(vals_in + base + idx) : base + idx) : 0u;
-        }
-#pragma unroll
-        for (int j = 0; j < RS_ITEMS; j++) {
-            const uint32_t idx = warp_start + j * 32 + lane;
-            if (idx < n) s_vals[rank[j]] = v[j];
-        }
-        __syncthreads();
-        const uint32_t cnt = min((uint32_t)RS_TILE, n - part_start);
-        for (uint32_t i = threadIdx.x; i < cnt; i += RS_THREADS) {
-            const uint32_t key = s_keys[i];
-            const uint32_t d = (key >> shift) & mask;
-            const uint32_t out = base + s_global[d] + (i - s_digit_start[d]);
-            keys_out[out] = key;
-            vals_out[out] = s_vals[i];
-        }
-        __syncthreads();
+    for (int j = 0; j < RS_ITEMS; j++) {
+        const uint32_t idx = warp_start + j * 32 + lane;
+        if (idx < n) s_vals[pos[j]] = v[j];
+    }
+    __syncthreads();
+    const uint32_t total = min((uint32_t)RS_TILE, n - part_start);
+    for (uint32_t i = threadIdx.x; i < total; i += RS_THREADS) {
+        const uint32_t key = s_keys[i];
+        const uint32_t dk = (key >> shift) & 0xffu;
+        const uint32_t out = base + s_global[dk] + (i - s_digit_start[dk]);
+        keys_out[out] = key;
+        vals_out[out] = s_vals[i];
     }
 }
 
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
+    (void)num_sms;
     int passes, step;
     pass_plan(a.begin_bit, a.end_bit, passes, step);
-    // One block per partition of the largest segment this buffer can hold; blocks past
-    // the segment's live partitions exit at once.  (Persistent blocks walking many
-    // partitions left the loads' latency exposed.)
-    const int grid_up = a.max_parts > 0 ? a.max_parts : num_sms;
-    const int grid_down = grid_up;
+    const int grid = a.max_parts > 0 ? a.max_parts : 1;
+    uint32_t* ghist = a.totals;                           // [passes][256]
+    uint32_t* counters = a.totals + OS_MAX_PASSES * 256;  // one partition counter per pass
+    cudaMemsetAsync(a.totals, 0, (OS_MAX_PASSES * 256 + OS_MAX_PASSES) * sizeof(uint32_t), s);
+    radix_hist_all<<<min(grid, OS_HIST_BLOCKS), RS_THREADS, 0, s>>>(a.keys, a.seg, a.begin_bit, passes, ghist);
     uint32_t* kb[2] = {a.keys, a.keys_alt};
     uint32_t* vb[2] = {a.vals, a.vals_alt};
     for (int p = 0; p < passes; p++) {
         const int in = p & 1, out = in ^ 1;
-        const int shift = a.begin_bit + p * step;
-        const int bits = 8;
-        radix_upsweep<<<grid_up, RS_THREADS, 0, s>>>(kb[in], a.seg, shift, bits, a.hist);
-        radix_scan<<<256, 1024, 0, s>>>(a.seg, a.hist, a.totals);
-        radix_downsweep<<<grid_down, RS_THREADS, 0, s>>>(kb[in], (p == 0 && a.iota) ? nullptr : vb[in],
-                                                          kb[out], vb[out], a.seg, shift, bits, a.hist,
-                                                          a.totals);
+        cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
+        radix_onesweep<<<grid, RS_THREADS, 0, s>>>(kb[in], (p == 0 && a.iota) ? nullptr : vb[in], kb[out], vb[out],
+                                                    a.seg, a.begin_bit + p * step, ghist + p * 256, a.hist,
+                                                    counters + p, a.timeout);
     }
 }
-
 
 // ---------------------------------------------------------------------------------
 // Key-instance emission.  Depth-sorted pairs are taken in chunks of EM_CHUNK:
