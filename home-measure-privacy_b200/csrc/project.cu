@@ -113,8 +113,8 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
                         const float xlo = fmaxf(p.u + (-B * dl - sl) * iA - slack, xlo_lim);
                         if (xlo <= xhi) {
                             // Tile tx holds pixel centres [16 tx + 0.5, 16 tx + 15.5].
-                            xs = max(x0, (int)ceilf((xlo - 15.5f) * 0.0625f));
-                            xe = min(x1, (int)floorf((xhi - 0.5f) * 0.0625f) + 1);
+                            xs = max(x0, __float2int_ru((xlo - 15.5f) * 0.0625f));
+                            xe = min(x1, __float2int_rd((xhi - 0.5f) * 0.0625f) + 1);
                             if (xe < xs) xe = xs;
                         }
                     }
