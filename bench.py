@@ -251,6 +251,9 @@ def run_b200(args, rank, local, world, dist):
             N.check(r.lib.gs_host_free(host))
         e2e = dict(value=world * 1000.0 / (t_e / args.steps), unit="steps/s", h2d_bytes_per_step=int(targets.nbytes),
                    d2h_bytes_per_step=int(ctypes.sizeof(ctypes.c_float) * 0 + 64))
+    # ---- densification on the device (trainScene's settings), after the timed region
+    if not args.no_densify and not dp:
+        res["densify"] = densify_measure(hmp, r, c, cams, ad, lam, window, args)
     r.close()
     # ---- plain: one view per launch per stage, same step
     plain = None
@@ -290,6 +293,42 @@ def profile_case(args):
         print(json.dumps(dict(case="profile", views=len(cams), pixels=int(st["pixels"]),
                               instances=int(st["instances"]), loss=float(loss),
                               stages_ms=r.stage_times()["ms"])), flush=True)
+
+
+def densify_measure(hmp, r, c, cams, ad, lam, window, args):
+    """gs_densify on the benchmark scene after 5 steps of statistics, with trainScene's
+    thresholds (gradient 2e-4 / (0.5 x first view width), split above 1 % of the scene
+    extent, room for 10 % more); beside it the reference's host densify() restated in C
+    on the same records and statistics (one thread)."""
+    r.set_densify_stats(True)
+    for _ in range(5):
+        r.train_step(ad, lam, window, loss=False)
+    r.synchronize()
+    n0 = r.lib.gs_num_gaussians(r.ctx)
+    extent = hmp.sceneExtent([dict(cam=cm) for cm in cams])
+    cfg = dict(grad_threshold=2e-4 / (0.5 * cams[0]["width"]), size_threshold=0.01 * extent,
+               max_count=int(n0 * 1.1), seed=11)
+    host = None
+    if not args.no_cpu:
+        before = r.get_gaussians()
+        sums, counts = r.densify_stats()
+        host = (before, sums, counts)
+    t0 = time.perf_counter()
+    n1 = r.densify(**cfg)
+    gpu_ms = (time.perf_counter() - t0) * 1e3
+    out = dict(gaussians_before=int(n0), gaussians_after=int(n1), gpu_ms=round(gpu_ms, 3),
+               note="host-timed C-ABI call: classification, scan, one wait for the count, scatter, "
+                    "buffer re-sizing and zeroing of moments and statistics")
+    if host is not None:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle as O
+        t0 = time.perf_counter()
+        ref = O.densify(*host, **cfg)
+        out["cpu_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+        out["cpu_kind"] = "port (reference densify() restated in C, 1 thread)"
+        out["matches_cpu"] = bool(ref.shape[0] == n1)
+    r.set_densify_stats(False)
+    return out
 
 
 def cpu_baseline(hmp, steps=1, warmup=0, budget_s=150.0):
@@ -368,6 +407,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-densify", action="store_true")
     ap.add_argument("--dp", action="store_true",
                     help="use the data-parallel step (gradients, NCCL all-reduce, update) even on one GPU")
     ap.add_argument("--autotune-cache", default=None,
@@ -436,6 +476,8 @@ def main():
             stage_rooflines=per_stage,
             e2e=res["e2e"],
         )
+        if res.get("densify"):
+            line["densify"] = res["densify"]
         if res.get("plain_stages"):
             ps = res["plain_stages"]
             line["plain_stages_ms_per_step"] = {k: round(v / max(1, ps["steps"]), 4) for k, v in ps["ms"].items()}

@@ -66,6 +66,12 @@ CTX = ctypes.c_void_p
 # name -> (restype, argtypes)
 GRAD_TAIL_FLOATS = 64  # GS_GRAD_TAIL_FLOATS
 
+
+class GsDensifyConfig(ctypes.Structure):
+    _fields_ = [("grad_threshold", ctypes.c_double), ("size_threshold", ctypes.c_double),
+                ("min_opacity", ctypes.c_double), ("max_size", ctypes.c_double), ("max_count", c_int32),
+                ("reserved", c_int32), ("seed", ctypes.c_uint64)]
+
 SIGNATURES = {
     "gs_config_default": (None, [ctypes.POINTER(GsConfig)]),
     "gs_adam_default": (None, [ctypes.POINTER(GsAdamConfig)]),
@@ -103,6 +109,13 @@ SIGNATURES = {
                                      ctypes.POINTER(c_int32)]),
     "gs_get_stream": (ctypes.c_int, [CTX, ctypes.POINTER(VP)]),
     "gs_get_blend_count": (ctypes.c_int, [CTX, ctypes.POINTER(ctypes.c_uint64)]),
+    "gs_set_densify_stats": (ctypes.c_int, [CTX, c_int32]),
+    "gs_reset_densify_stats": (ctypes.c_int, [CTX]),
+    "gs_get_densify_stats": (ctypes.c_int, [CTX, VP, VP]),
+    "gs_densify_config_default": (None, [ctypes.POINTER(GsDensifyConfig)]),
+    "gs_densify": (ctypes.c_int, [CTX, ctypes.POINTER(GsDensifyConfig), ctypes.POINTER(c_int32)]),
+    "gs_reset_opacity": (ctypes.c_int, [CTX, ctypes.c_double]),
+    "gs_scene_extent": (ctypes.c_int, [ctypes.POINTER(GsCamera), c_int32, ctypes.POINTER(c_float)]),
     "gs_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(VP)]),
     "gs_host_free": (ctypes.c_int, [VP]),
     "gs_synchronize": (ctypes.c_int, [CTX]),

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <string>
 #include <vector>
@@ -107,8 +108,14 @@ struct GsContext {
     std::string device_name;
     // scene
     int n = 0, n_pad = 0, degree = 0, planes = 14;
-    DevBuf params, grads, mom1, mom2;   // grads: planes x n_pad, then GS_GRAD_TAIL_FLOATS
+    // grads: planes x n_pad gradients, 2 x n_pad step-local densification statistics,
+    // then GS_GRAD_TAIL_FLOATS (loss sum, overflow, views)
+    DevBuf params, grads, mom1, mom2;
     bool grads_pending = false;         // gs_step_gradients queued, gs_step_apply not yet
+    DevBuf stats;                       // densification statistics [2][n_pad]: norm sums, view counts
+    bool stats_on = false;              // training steps accumulate them
+    bool stats_active = false;          // set while a training step's kernels are enqueued
+    DevBuf dn_scratch;                  // densify block sums and result
     // views: training views [0, V) plus one scratch view at index V for render /
     // gradients / loss-gradient calls on arbitrary cameras or images
     std::vector<GsCamera> cams;
@@ -162,6 +169,11 @@ struct GsContext {
 };
 
 static const int SEG_ALL = 0, SEG_PAIR = 65, SEG_INST_ALL = 129, SEG_INST = 130, SEG_COUNT = 194;
+
+// Gradient buffer layout: parameter gradients, step-local statistics, tail.
+static float* step_stats(GsContext* c) { return c->grads.as<float>() + (size_t)c->planes * c->n_pad; }
+static float* grad_tail(GsContext* c) { return c->grads.as<float>() + (size_t)(c->planes + 2) * c->n_pad; }
+static size_t grad_buffer_floats(GsContext* c) { return (size_t)(c->planes + 2) * c->n_pad + GS_GRAD_TAIL_FLOATS; }
 
 static int ensure(DevBuf& b, size_t bytes, GsContext* c) {
     if (bytes == 0) bytes = 16;
@@ -477,6 +489,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     pa.alpha_min = c->cfg.alpha_min;
     pa.pcount = c->pcount.as<uint32_t>();
     pa.erec = c->erec.as<EmitRec>();
+    pa.stats_cnt = c->stats_active ? step_stats(c) + c->n_pad : nullptr;
     launch_project_fwd(pa, c->stream);
     count_launches(c, ST_PROJECT, 1);
     // Depth sort of the pairs (31 bits: depths are positive, the sentinel is 0x7fffffff).
@@ -612,6 +625,7 @@ static int enqueue_backward_view(GsContext* c, int first, int step_first, int co
     pb.sg1 = c->sg1.as<float>();
     pb.grads = c->grads.as<float>();
     pb.accumulate = accumulate ? 1 : 0;
+    pb.stats_sum = c->stats_active ? step_stats(c) : nullptr;
     launch_project_bwd(pb, c->stream);
     count_launches(c, ST_PROJECT_BWD, 1);
     CK(cudaGetLastError());
@@ -629,7 +643,6 @@ static void fill_lrs(GsContext* c, const GsAdamConfig& ad, float* lr) {
 }
 
 // The whole training step (no host synchronisation inside).
-static float* grad_tail(GsContext* c) { return c->grads.as<float>() + (size_t)c->planes * c->n_pad; }
 
 static void fill_adam_args(GsContext* c, const GsAdamConfig& ad, AdamArgs& aa) {
     memset(&aa, 0, sizeof aa);
@@ -652,6 +665,12 @@ static void fill_adam_args(GsContext* c, const GsAdamConfig& ad, AdamArgs& aa) {
 static int enqueue_step(GsContext* c, const GsAdamConfig& ad, const GsLossConfig& lc, int first, int count,
                         bool batched, int kind, int phase = 0) {
     CK(cudaMemsetAsync(c->acc.p, 0, sizeof(double) * 2 * (GS_MAX_VIEWS + 1), c->stream));
+    if (c->stats_on) CK(cudaMemsetAsync(step_stats(c), 0, (size_t)2 * c->n_pad * 4, c->stream));
+    struct StatsScope {
+        GsContext* c;
+        ~StatsScope() { c->stats_active = false; }
+    } stats_scope{c};
+    c->stats_active = c->stats_on;
     if (batched) {
         CKI(enqueue_forward(c, first, count, true));
         CKI(enqueue_loss_view(c, first, count, lc, kind));
@@ -665,6 +684,7 @@ static int enqueue_step(GsContext* c, const GsAdamConfig& ad, const GsLossConfig
             CKI(enqueue_backward_view(c, v, first, 1, false, v > first));
         }
     }
+    c->stats_active = false;
     if (phase == 1) {
         launch_grad_tail(c->status.as<DevStatus>(), c->acc.as<double>(), c->views_d.as<ViewDesc>(), first, count,
                          lc.ssim_lambda, lc.window, grad_tail(c), c->stream);
@@ -676,6 +696,11 @@ static int enqueue_step(GsContext* c, const GsAdamConfig& ad, const GsLossConfig
     AdamArgs aa;
     fill_adam_args(c, ad, aa);
     launch_adam(aa, c->stream);
+    if (c->stats_on) {
+        launch_stats_commit(c->stats.as<float>(), step_stats(c), c->n_pad, c->status.as<DevStatus>(), nullptr,
+                            c->stream);
+        count_launches(c, ST_ADAM, 1);
+    }
     launch_step_end(c->status.as<DevStatus>(), c->acc.as<double>(), c->views_d.as<ViewDesc>(), first, count,
                     lc.ssim_lambda, lc.window, 1, c->stream);
     count_launches(c, ST_ADAM, 2);
@@ -969,27 +994,40 @@ int gs_destroy(GsContext* c) {
 }
 
 // ---- scene ------------------------------------------------------------------------
-static int upload_planes(GsContext* c, int n, const std::vector<float>& planes_host) {
+// Sizes every per-Gaussian buffer for n Gaussians and clears gradients, moments and the
+// densification statistics; pair buffers, capacities and graphs start over.  The Adam
+// step counter is kept when keep_step (densification keeps training's t).
+static int resize_scene(GsContext* c, int n, bool keep_step) {
     c->n = n;
     c->n_pad = ((n + 127) / 128) * 128;
     if (c->n_pad == 0) c->n_pad = 128;
     const size_t bytes = (size_t)c->planes * c->n_pad * 4;
     CKI(ensure(c->params, bytes, c));
-    CKI(ensure(c->grads, bytes + GS_GRAD_TAIL_FLOATS * 4, c));
+    CKI(ensure(c->grads, grad_buffer_floats(c) * 4, c));
     CKI(ensure(c->mom1, bytes, c));
     CKI(ensure(c->mom2, bytes, c));
-    CK(cudaMemcpyAsync(c->params.p, planes_host.data(), bytes, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(c->grads.p, 0, bytes + GS_GRAD_TAIL_FLOATS * 4, c->stream));
+    CKI(ensure(c->stats, (size_t)2 * c->n_pad * 4, c));
+    CK(cudaMemsetAsync(c->grads.p, 0, grad_buffer_floats(c) * 4, c->stream));
     CK(cudaMemsetAsync(c->mom1.p, 0, bytes, c->stream));
     CK(cudaMemsetAsync(c->mom2.p, 0, bytes, c->stream));
-    CK(cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream));
+    CK(cudaMemsetAsync(c->stats.p, 0, (size_t)2 * c->n_pad * 4, c->stream));
+    if (keep_step) CK(cudaMemsetAsync(c->status.p, 0, GS_STATUS_FORWARD_BYTES, c->stream));
+    else CK(cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream));
     CKI(write_segments(c));
     c->pair_cap = 0;  // re-size pair buffers for the new n_pad
     CKI(size_pairs(c, std::max(c->V, 1)));
     c->inst_cap_valid = false;
     c->last_first = -1;
     c->have_loss = false;
+    c->grads_pending = false;
     drop_graphs(c);
+    return GS_OK;
+}
+
+static int upload_planes(GsContext* c, int n, const std::vector<float>& planes_host) {
+    CKI(resize_scene(c, n, false));
+    CK(cudaMemcpyAsync(c->params.p, planes_host.data(), (size_t)c->planes * c->n_pad * 4, cudaMemcpyHostToDevice,
+                       c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return GS_OK;
 }
@@ -1541,7 +1579,7 @@ int gs_step_gradients(GsContext* c, const GsLossConfig* lc, int32_t first, int32
     c->have_loss = true;
     c->grads_pending = true;
     *grads_device = c->grads.as<float>();
-    *num_floats = (int64_t)c->planes * c->n_pad + GS_GRAD_TAIL_FLOATS;
+    *num_floats = (int64_t)grad_buffer_floats(c);
     return GS_OK;
 }
 
@@ -1554,6 +1592,9 @@ int gs_step_apply(GsContext* c, const GsAdamConfig* ad, float* loss_out, int32_t
     fill_adam_args(c, *ad, aa);
     aa.skip = grad_tail(c) + 1;
     launch_adam(aa, c->stream);
+    if (c->stats_on)
+        launch_stats_commit(c->stats.as<float>(), step_stats(c), c->n_pad, c->status.as<DevStatus>(),
+                            grad_tail(c) + 1, c->stream);
     launch_reduced_step_end(c->status.as<DevStatus>(), grad_tail(c), c->stream);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->status_host, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
@@ -1714,6 +1755,126 @@ int gs_get_blend_count(GsContext* c, uint64_t* blends_out) {
     CK(cudaMemcpyAsync(&n, c->scratch16.p, 8, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     *blends_out = (uint64_t)n;
+    return GS_OK;
+}
+
+// ---- densification ------------------------------------------------------------------
+int gs_set_densify_stats(GsContext* c, int32_t enable) {
+    CTX_CHECK(c);
+    const bool on = enable != 0;
+    if (on != c->stats_on) {
+        c->stats_on = on;
+        drop_graphs(c);  // the step graphs hold (or lack) the statistics kernels
+    }
+    return GS_OK;
+}
+
+int gs_reset_densify_stats(GsContext* c) {
+    CTX_CHECK(c);
+    if (c->stats.p) CK(cudaMemsetAsync(c->stats.p, 0, (size_t)2 * c->n_pad * 4, c->stream));
+    return GS_OK;
+}
+
+int gs_get_densify_stats(GsContext* c, float* sums, float* counts) {
+    CTX_CHECK(c);
+    if ((!sums || !counts) && c->n > 0) return fail(GS_ERR_INVALID_ARG, "null output");
+    if (c->n == 0) return GS_OK;
+    CK(cudaMemcpyAsync(sums, c->stats.p, (size_t)c->n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(counts, c->stats.as<float>() + c->n_pad, (size_t)c->n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return GS_OK;
+}
+
+void gs_densify_config_default(GsDensifyConfig* d) {
+    if (!d) return;
+    memset(d, 0, sizeof *d);
+    d->grad_threshold = 2e-4;
+    d->size_threshold = 0.1;
+    d->min_opacity = 0.005;
+    d->max_count = 400000;
+    d->max_size = INFINITY;
+    d->seed = 0;
+}
+
+int gs_densify(GsContext* c, const GsDensifyConfig* d, int32_t* new_count) {
+    CTX_CHECK(c);
+    if (!d) return fail(GS_ERR_INVALID_ARG, "config is null");
+    if (std::isnan(d->grad_threshold) || std::isnan(d->size_threshold) || std::isnan(d->min_opacity) ||
+        std::isnan(d->max_size) || d->max_count < 0)
+        return fail(GS_ERR_INVALID_ARG, "bad densify config");
+    if (c->n == 0) {
+        if (new_count) *new_count = 0;
+        return GS_OK;
+    }
+    const int blocks = densify_blocks(c->n);
+    CKI(ensure(c->dn_scratch, (size_t)blocks * 8 + 64, c));
+    DensifyArgs a;
+    memset(&a, 0, sizeof a);
+    a.params = c->params.as<float>();
+    a.stats = c->stats.as<float>();
+    a.n = c->n;
+    a.n_pad = c->n_pad;
+    a.planes = c->planes;
+    a.grad_threshold = d->grad_threshold;
+    a.size_threshold = d->size_threshold;
+    a.min_opacity = d->min_opacity;
+    a.max_size = d->max_size;
+    a.log_split = std::log(1.6);
+    a.room = (long long)d->max_count - c->n;
+    a.seed = d->seed;
+    a.block_sums = reinterpret_cast<uint2*>(c->dn_scratch.p);
+    a.result = reinterpret_cast<unsigned*>(c->dn_scratch.as<char>() + (size_t)blocks * 8);
+    launch_densify_count(a, c->stream);
+    CK(cudaGetLastError());
+    unsigned res[3] = {0, 0, 0};
+    CK(cudaMemcpyAsync(res, a.result, sizeof res, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int new_n = (int)res[2];
+    if (res[2] > (1u << 28)) return fail(GS_ERR_CAPACITY, "densified set too large (%u)", res[2]);
+    // The new planes go into the first moment's buffer, which becomes the parameters;
+    // the old parameter buffer becomes the first moment (zeroed below).
+    const int new_np = new_n > 0 ? ((new_n + 127) / 128) * 128 : 128;
+    CKI(ensure(c->mom1, (size_t)c->planes * new_np * 4, c));
+    a.out = c->mom1.as<float>();
+    a.out_n_pad = new_np;
+    launch_densify_scatter(a, new_n, c->stream);
+    CK(cudaGetLastError());
+    std::swap(c->params, c->mom1);
+    c->generation = ++g_generation_counter;
+    CKI(resize_scene(c, new_n, true));
+    CK(cudaStreamSynchronize(c->stream));
+    if (new_count) *new_count = new_n;
+    return GS_OK;
+}
+
+int gs_reset_opacity(GsContext* c, double max_logit) {
+    CTX_CHECK(c);
+    if (std::isnan(max_logit)) return fail(GS_ERR_INVALID_ARG, "max_logit is NaN");
+    launch_opacity_cap(c->params.as<float>() + (size_t)10 * c->n_pad, c->n, max_logit, c->stream);
+    CK(cudaGetLastError());
+    return GS_OK;
+}
+
+int gs_scene_extent(const GsCamera* cams, int32_t count, float* extent_out) {
+    if (!cams || count < 1 || !extent_out) return fail(GS_ERR_INVALID_ARG, "bad cameras");
+    // Camera centres -R^T t in double, as the reference's JavaScript does.
+    std::vector<double> cx(count), cy(count), cz(count);
+    double mx = 0, my = 0, mz = 0;
+    for (int k = 0; k < count; k++) {
+        const float* m = cams[k].view;
+        cx[k] = -((double)m[0] * m[3] + (double)m[4] * m[7] + (double)m[8] * m[11]);
+        cy[k] = -((double)m[1] * m[3] + (double)m[5] * m[7] + (double)m[9] * m[11]);
+        cz[k] = -((double)m[2] * m[3] + (double)m[6] * m[7] + (double)m[10] * m[11]);
+        mx += cx[k];
+        my += cy[k];
+        mz += cz[k];
+    }
+    mx /= count;
+    my /= count;
+    mz /= count;
+    double far = 1e-3;
+    for (int k = 0; k < count; k++) far = std::max(far, std::hypot(cx[k] - mx, cy[k] - my, cz[k] - mz));
+    *extent_out = (float)(1.1 * far);
     return GS_OK;
 }
 

@@ -35,6 +35,7 @@ struct ProjectArgs {
     float alpha_min;
     uint32_t* pcount;        // instances of the pair (0 when it covers no tile)
     EmitRec* erec;           // written for pairs that cover >= 1 tile
+    float* stats_cnt;        // training steps: += views the Gaussian projects into (or nullptr)
 };
 void launch_project_fwd(const ProjectArgs& a, cudaStream_t s);
 
@@ -50,8 +51,30 @@ struct ProjectBwdArgs {
     const float* sg1;        // [pairs]
     float* grads;            // [planes][n_pad]
     int accumulate;          // add to grads instead of overwriting them
+    float* stats_sum;        // training steps: += |(dL/du, dL/dv)| over the views (or nullptr)
 };
 void launch_project_bwd(const ProjectBwdArgs& a, cudaStream_t s);
+
+// ---- densification -----------------------------------------------------------------
+struct DensifyArgs {
+    const float* params;     // [planes][n_pad]
+    const float* stats;      // [2][n_pad]: sums of gradient norms, view counts
+    int n, n_pad, planes;
+    float* out;              // [planes][out_n_pad]
+    int out_n_pad;
+    double grad_threshold, size_threshold, min_opacity, max_size, log_split;
+    long long room;          // max_count - n
+    unsigned long long seed;
+    uint2* block_sums;       // scratch, densify_blocks(n) entries
+    unsigned* result;        // [0] kept or densified, [1] candidates, [2] new count
+};
+int densify_blocks(int n);
+void launch_densify_count(const DensifyArgs& a, cudaStream_t s);
+void launch_densify_scatter(const DensifyArgs& a, int new_n, cudaStream_t s);
+void launch_opacity_cap(float* plane, int n, double max_logit, cudaStream_t s);
+// stats += step unless the step's update was skipped (skip: reduced flag, or status).
+void launch_stats_commit(float* stats, const float* step, int n_pad, const DevStatus* status, const float* skip,
+                         cudaStream_t s);
 
 // ---- sorting ----------------------------------------------------------------------
 // LSD radix sort of u32 keys with u32 values over a segment [seg->base, +seg->count)

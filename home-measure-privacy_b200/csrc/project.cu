@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
     // form <= 2 ln(opacity / alpha_min); the slack keeps the spans conservative against
     // the approximate arithmetic below and the raster's own rounding.
     const float thr_g = opacity > 0.f ? 2.0f * (__logf(opacity) - __logf(a.alpha_min)) + 1e-3f : -1.0f;
-    unsigned int my_visible = 0;
+    unsigned int my_visible = 0, ok_views = 0;
     for (int s = 0; s < a.num_views; s++) {
         const ViewDesc& vw = a.views[a.view_first + s];
         const size_t pair = (size_t)(a.pair_slot_first + s) * np + i;
@@ -161,7 +161,9 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
             er[1] = make_uint4(sp[0], sp[1], sp[2], sp[3]);
         }
         my_visible += covers ? 1u : 0u;
+        ok_views += p.ok ? 1u : 0u;
     }
+    if (a.stats_cnt && ok_views) a.stats_cnt[i] += (float)ok_views;  // STATS count (trainer/gpu.js:494-496)
     if (a.visible) {
         // One atomic per warp.
         unsigned int sum = my_visible;
@@ -228,6 +230,7 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(ProjectBwdArgs a) {
 #pragma unroll
         for (int k = 0; k < 9; k++) gSig[k] = 0.f;
         float gmean[3] = {0.f, 0.f, 0.f};
+        float gnorm = 0.f;
         for (int sidx = 0; sidx < a.num_views; sidx++) {
             const size_t pair = (size_t)(a.pair_slot_first + sidx) * np + i;
             const float4 s0 = a.sg8[pair * 2 + 0];
@@ -236,6 +239,7 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(ProjectBwdArgs a) {
             if (s0.x == 0.f && s0.y == 0.f && s0.z == 0.f && s0.w == 0.f && s1.x == 0.f && s1.y == 0.f &&
                 s1.z == 0.f && s1.w == 0.f && gC == 0.f)
                 continue;
+            gnorm += sqrtf(s1.x * s1.x + s1.y * s1.y);  // STATS: length of (dL/du, dL/dv)
             const ViewDesc& vw = a.views[a.view_first + sidx];
             const float* W = vw.R;
             const float grgb[3] = {s0.x, s0.y, s0.z};
@@ -369,6 +373,7 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(ProjectBwdArgs a) {
         G[0] = gmean[0];
         G[1] = gmean[1];
         G[2] = gmean[2];
+        if (a.stats_sum && gnorm != 0.f) a.stats_sum[i] += gnorm;
     }
 #pragma unroll
     for (int k = 0; k < P; k++) {

@@ -178,11 +178,15 @@ class Renderer:
         N.check(self.lib.gs_train(self.ctx, int(steps), ctypes.byref(ad), N.ptr(losses)))
         return dict(gaussians=self.get_gaussians(), losses=[float(x) for x in losses])
 
-    def trainScene(self, start, views, steps=3000, ssim=0.0, onProgress=None, shouldStop=None, lr=None,
-                   seed=0, **unused):
-        """trainScene() (trainer/gpu.js:890-959) without densification: every photo once per
-        round in a shuffled order, one view per step, mean L1 sampled every 25 steps and
-        reported every 50.  views: [{cam, image: uint8 RGB}]."""
+    def trainScene(self, start, views, steps=3000, densifyEvery=100, densifyFrom=300, densifyUntil=2000,
+                   maxSplats=400000, ssim=0.0, prune=False, opacityReset=False, onProgress=None, shouldStop=None,
+                   lr=None, seed=0, **unused):
+        """trainScene() (trainer/gpu.js:890-959): every photo once per round in a shuffled
+        order, one view per step; gradient statistics every step and densification on the
+        device every `densifyEvery` steps in [densifyFrom, densifyUntil] (split above 1 %
+        of the scene extent, with `prune` drop above 10 %), the opacity reset halfway
+        when `opacityReset`; mean L1 sampled every 25 steps and reported every 50.
+        views: [{cam, image: uint8 RGB}]."""
         self.set_gaussians(start)
         self.set_views([v["cam"] for v in views])
         for k, v in enumerate(views):
@@ -190,6 +194,11 @@ class Renderer:
         ad = adam_config(lr)
         lc = N.GsLossConfig(float(ssim), 0)
         rng = np.random.default_rng(seed)
+        extent = sceneExtent(views)
+        reset_at = (math.floor((densifyFrom + densifyUntil) / 2 / densifyEvery + 0.5) * densifyEvery
+                    if opacityReset else -1)
+        low_opacity = math.log(0.01 / 0.99)
+        self.set_densify_stats(True)
         order = []
         loss_sum, loss_count = 0.0, 0
         for t in range(1, steps + 1):
@@ -205,13 +214,57 @@ class Renderer:
             if sample:
                 loss_sum += loss.value
                 loss_count += 1
+            if densifyFrom <= t <= densifyUntil and t % densifyEvery == 0:
+                # The reference's threshold is per pixel of its first view (trainer/gpu.js:939-940).
+                self.densify(grad_threshold=2e-4 / (0.5 * views[0]["cam"]["width"]), max_count=maxSplats,
+                             size_threshold=0.01 * extent, max_size=0.1 * extent if prune else math.inf,
+                             seed=seed * 1000003 + t)
+                if t == reset_at:
+                    self.reset_opacity(low_opacity)
             if t % 50 == 0:
                 if onProgress:
                     onProgress(dict(step=t, loss=loss_sum / loss_count if loss_count else float("nan"),
                                     count=self.lib.gs_num_gaussians(self.ctx)))
                 loss_sum, loss_count = 0.0, 0
         N.check(self.lib.gs_synchronize(self.ctx))
+        self.set_densify_stats(False)
         return self.get_gaussians()
+
+    # ---- densification on the device --------------------------------------------------
+    def set_densify_stats(self, enable=True):
+        N.check(self.lib.gs_set_densify_stats(self.ctx, 1 if enable else 0))
+
+    def reset_densify_stats(self):
+        N.check(self.lib.gs_reset_densify_stats(self.ctx))
+
+    def densify_stats(self):
+        """(sums, counts) of |(dL/du, dL/dv)| per Gaussian since the last reset."""
+        n = self.lib.gs_num_gaussians(self.ctx)
+        sums = np.zeros(max(n, 1), np.float32)
+        counts = np.zeros(max(n, 1), np.float32)
+        N.check(self.lib.gs_get_densify_stats(self.ctx, N.ptr(sums), N.ptr(counts)))
+        return sums[:n], counts[:n]
+
+    def densify(self, grad_threshold=2e-4, size_threshold=0.1, min_opacity=0.005, max_count=400000,
+                max_size=math.inf, seed=0):
+        """densify() (trainer/gpu.js:575-599) on the device; returns the new count."""
+        d = N.GsDensifyConfig()
+        self.lib.gs_densify_config_default(ctypes.byref(d))
+        d.grad_threshold, d.size_threshold, d.min_opacity = grad_threshold, size_threshold, min_opacity
+        d.max_size, d.max_count, d.seed = max_size, int(max_count), int(seed) & 0xFFFFFFFFFFFFFFFF
+        n = ctypes.c_int32(0)
+        N.check(self.lib.gs_densify(self.ctx, ctypes.byref(d), ctypes.byref(n)))
+        return n.value
+
+    def reset_opacity(self, max_logit=math.log(0.01 / 0.99)):
+        N.check(self.lib.gs_reset_opacity(self.ctx, float(max_logit)))
+
+    def scene_extent(self, cams):
+        """sceneExtent (trainer/gpu.js:564-568) of cameras, through the C ABI."""
+        arr = (N.GsCamera * len(cams))(*[_camera(c) for c in cams])
+        out = ctypes.c_float(0.0)
+        N.check(self.lib.gs_scene_extent(arr, len(cams), ctypes.byref(out)))
+        return out.value
 
     # ---- the Function pair and the batched step ----------------------------------------
     def forward(self, first=0, count=None, images=True):

@@ -233,8 +233,9 @@ GS_API int gs_train(GsContext* ctx, int32_t steps, const GsAdamConfig* adam, flo
  *
  * gs_step_gradients queues forward, loss and backward of views [first, first+count) on
  * the context's stream and leaves the parameter gradients in the context's gradient
- * buffer: num_params x n_pad floats (plane-major, n_pad = n rounded up to 128) followed
- * by GS_GRAD_TAIL_FLOATS floats: [0] the sum over these views of their mean losses,
+ * buffer: num_params x n_pad floats (plane-major, n_pad = n rounded up to 128), then
+ * 2 x n_pad floats of this step's densification statistics (zero unless enabled), then
+ * GS_GRAD_TAIL_FLOATS floats: [0] the sum over these views of their mean losses,
  * [1] 1 if the step's key instances overflowed their buffer, [2] the view count, rest 0.
  * *grads_device gets the buffer's device address and *num_floats its length.  Sum the
  * whole buffer across replicas (e.g. an NCCL all-reduce on gs_get_stream's stream),
@@ -253,6 +254,49 @@ GS_API int gs_step_apply(GsContext* ctx, const GsAdamConfig* adam, float* loss_o
 /* The context's CUDA stream (a cudaStream_t), for work the caller orders with the
  * library's: a collective over gs_step_gradients' buffer, a copy, an event. */
 GS_API int gs_get_stream(GsContext* ctx, void** stream_out);
+
+/* ---- Densification (trainer/gpu.js:484-497 STATS, :564-599 sceneExtent / densify,
+ * :902-903 and :944 the opacity reset) --------------------------------------------------
+ * The reference reads every Gaussian back to the host each densification, densifies in
+ * JavaScript and uploads the result with fresh moments and statistics.  Here all of it
+ * stays on the device. */
+
+/* STATS: while enabled, every training step (gs_train_step, gs_train_step_host,
+ * gs_step_gradients + gs_step_apply) adds, for each Gaussian and each of the step's
+ * views it projects into, |(dL/du, dL/dv)| to its sum and 1 to its count.  A step whose
+ * update was skipped (instance overflow) adds nothing.  Off by default. */
+GS_API int gs_set_densify_stats(GsContext* ctx, int32_t enable);
+GS_API int gs_reset_densify_stats(GsContext* ctx);
+/* sums[n], counts[n]: the statistics since the last reset / densify / gs_set_gaussians. */
+GS_API int gs_get_densify_stats(GsContext* ctx, float* sums, float* counts);
+
+typedef struct GsDensifyConfig {
+    double grad_threshold;   /* average gradient norm that densifies (reference default 2e-4;
+                                trainScene passes 2e-4 / (0.5 * width of its first view)) */
+    double size_threshold;   /* largest scale up to which a Gaussian is cloned, else split */
+    double min_opacity;      /* sigmoid(opacity logit) below this: dropped */
+    double max_size;         /* largest scale above this: dropped (INFINITY: never) */
+    int32_t max_count;       /* clones and splits stop once the count would pass this */
+    int32_t reserved;
+    uint64_t seed;           /* split offsets: SplitMix64(seed, index, copy, axis) instead of
+                                the reference's Math.random() */
+} GsDensifyConfig;
+GS_API void gs_densify_config_default(GsDensifyConfig* cfg);
+
+/* densify() on the device: the new set replaces the context's Gaussians in the
+ * reference's order (each kept Gaussian in place; a clone is the Gaussian then its copy;
+ * a split is its two moved, shrunk copies).  Moments and statistics restart at zero,
+ * the Adam step counter continues (as trainScene's t does).  *new_count gets the new
+ * number of Gaussians.  Waits for the stream once (to size the new buffers). */
+GS_API int gs_densify(GsContext* ctx, const GsDensifyConfig* cfg, int32_t* new_count);
+
+/* Opacity reset: logit = min(logit, max_logit) for every Gaussian (trainScene passes
+ * log(0.01 / 0.99)). */
+GS_API int gs_reset_opacity(GsContext* ctx, double max_logit);
+
+/* sceneExtent(views): 1.1 x the largest distance of a camera centre from their mean
+ * (at least 1e-3).  Host only. */
+GS_API int gs_scene_extent(const GsCamera* cams, int32_t count, float* extent_out);
 
 /* Step counter t (number of Adam updates applied since gs_set_gaussians). */
 GS_API int gs_get_step(GsContext* ctx, int32_t* t_out);

@@ -1112,3 +1112,67 @@ EXPORT void d64_grad(const OrcCamera* cam, const double* params, int n, int degr
     free(sg);
     scene64_free(&sc);
 }
+
+/* ---------------------------------------------------------------------------------
+ * densify() (trainer/gpu.js:575-599), sequential as written there: in index order drop
+ * transparent (sigmoid(logit) < min_opacity) and oversized (largest exp(logScale) >
+ * max_size) Gaussians, keep those whose average gradient norm is below the threshold
+ * or when no room is left, otherwise spend one unit of room on a clone (largest scale
+ * <= size_threshold) or a split (two copies moved by (u - 0.5) exp(logScale), log-scales
+ * minus ln 1.6).  JavaScript numbers are doubles; the records are float.  The
+ * reference's Math.random() is replaced by the same counter-based SplitMix64 draw as the
+ * library's (seed, index, copy, axis).  params/out: host records of `stride` floats;
+ * sums/counts: the statistics.  Returns the new count (out must hold 2 n records).
+ * --------------------------------------------------------------------------------- */
+static uint64_t orc_splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static double orc_uniform(uint64_t seed, uint64_t i, int k, int j) {
+    const uint64_t z = orc_splitmix64(orc_splitmix64(seed) ^ ((i * 8ull + (uint64_t)(k * 4 + j)) * 0xD1B54A32D192ED03ull));
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+static double js_max3(double a, double b, double c) {
+    if (isnan(a) || isnan(b) || isnan(c)) return NAN;
+    double m = a > b ? a : b;
+    return m > c ? m : c;
+}
+
+int orc_densify(const float* params, int n, int stride, const float* sums, const float* counts, double grad_threshold,
+                double size_threshold, double min_opacity, double max_size, int max_count, uint64_t seed, float* out) {
+    const double log_split = log(1.6);
+    long long room = (long long)max_count - n;
+    int o = 0;
+    for (int i = 0; i < n; i++) {
+        const float* g = params + (size_t)i * stride;
+        const double op = 1.0 / (1.0 + exp(-(double)g[10]));
+        if (op < min_opacity) continue;
+        const double size = js_max3(exp((double)g[3]), exp((double)g[4]), exp((double)g[5]));
+        if (size > max_size) continue;
+        const double avg = (counts[i] != 0.f && !isnan(counts[i])) ? (double)sums[i] / (double)counts[i] : 0.0;
+        if (avg < grad_threshold || room <= 0) {
+            memcpy(out + (size_t)o++ * stride, g, sizeof(float) * stride);
+            continue;
+        }
+        room--;
+        if (size <= size_threshold) {
+            memcpy(out + (size_t)o++ * stride, g, sizeof(float) * stride);
+            memcpy(out + (size_t)o++ * stride, g, sizeof(float) * stride);
+        } else {
+            for (int k = 0; k < 2; k++) {
+                float* c = out + (size_t)o++ * stride;
+                memcpy(c, g, sizeof(float) * stride);
+                for (int j = 0; j < 3; j++) {
+                    c[j] = (float)((double)g[j] + (orc_uniform(seed, (uint64_t)i, k, j) - 0.5) * exp((double)g[3 + j]));
+                    c[3 + j] = (float)((double)g[3 + j] - log_split);
+                }
+            }
+        }
+    }
+    return o;
+}

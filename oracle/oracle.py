@@ -45,6 +45,8 @@ def lib():
         CP = ctypes.POINTER(OrcCamera)
         i, f, d = ctypes.c_int, ctypes.c_float, ctypes.c_double
         i64 = ctypes.c_int64
+        L.orc_densify.argtypes = [F32P, i, i, F32P, F32P, d, d, d, d, i, ctypes.c_uint64, F32P]
+        L.orc_densify.restype = i
         L.orc_stride.argtypes = [i]
         L.orc_stride.restype = i
         L.orc32_preprocess.argtypes = [CP, F32P, i, i, f, f, F32P]
@@ -150,6 +152,18 @@ def adam(params, grads, m, v, degree, t, lr6, beta1=0.9, beta2=0.999, eps=1e-8):
     n = params.shape[0]
     lib().orc32_adam(params.reshape(-1), np.ascontiguousarray(grads, np.float32).reshape(-1), m.reshape(-1),
                      v.reshape(-1), n, degree, t, np.asarray(lr6, np.float32), beta1, beta2, eps)
+
+
+def densify(params, sums, counts, grad_threshold=2e-4, size_threshold=0.1, min_opacity=0.005, max_count=400000,
+            max_size=float("inf"), seed=0):
+    """densify() (trainer/gpu.js:575-599) on host records; returns the new records."""
+    n, stride_ = params.shape
+    out = np.zeros((max(2 * n, 1), stride_), np.float32)
+    m = lib().orc_densify(np.ascontiguousarray(params, np.float32).reshape(-1), n, stride_,
+                          np.ascontiguousarray(sums, np.float32), np.ascontiguousarray(counts, np.float32),
+                          grad_threshold, size_threshold, min_opacity, max_size, int(max_count),
+                          int(seed) & 0xFFFFFFFFFFFFFFFF, out.reshape(-1))
+    return out[:m]
 
 
 def step(cam, params, m, v, degree, target, lam, window, t, lr6, near=0.2, cap=1024):

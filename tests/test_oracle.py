@@ -224,3 +224,37 @@ def test_adam_matches_reference_formula(oracle):
     q = expect[:, 6:10]
     expect[:, 6:10] = q / np.linalg.norm(q, axis=1, keepdims=True)
     assert np.allclose(p, expect, atol=1e-5)
+
+
+def test_densify_rules(oracle):
+    """densify() (trainer/gpu.js:575-599) on hand-made records: drop, keep, clone, split,
+    the room limit and the output order."""
+    stride = 14
+    recs = np.zeros((6, stride), np.float32)
+    recs[:, 6] = 1.0  # unit rotations
+    recs[:, 10] = 2.0  # opaque
+    recs[:, 3:6] = math.log(0.05)  # small
+    recs[0, 10] = -8.0  # transparent: dropped
+    recs[2, 3:6] = math.log(0.5)  # large: split
+    recs[:, 0] = np.arange(6)  # means tell them apart
+    sums = np.array([1, 0, 1, 1, 1, 1], np.float32)
+    counts = np.array([1, 1, 1, 1, 0, 1], np.float32)  # index 1: zero gradient; index 4: no views
+    out = oracle.densify(recs, sums, counts, grad_threshold=0.5, size_threshold=0.1, max_count=8, seed=3)
+    # 0 dropped; 1 kept; 2 split (2 copies); 3 cloned (2); 4 kept (count 0 -> average 0);
+    # 5 candidate but room = 8 - 6 = 2 is used up by 2 and 3: kept.
+    assert out.shape[0] == 1 + 2 + 2 + 1 + 1
+    np.testing.assert_array_equal(out[0], recs[1])
+    for c in out[1:3]:
+        assert np.all(np.abs(c[0:3] - recs[2, 0:3]) <= 0.5 * 0.5 + 1e-6)
+        np.testing.assert_allclose(c[3:6], np.float32(math.log(0.5) - math.log(1.6)), rtol=1e-6)
+        np.testing.assert_array_equal(c[6:], recs[2, 6:])
+    assert not np.array_equal(out[1], out[2])
+    np.testing.assert_array_equal(out[3], recs[3])
+    np.testing.assert_array_equal(out[4], recs[3])
+    np.testing.assert_array_equal(out[5], recs[4])
+    np.testing.assert_array_equal(out[6], recs[5])
+    # the same seed gives the same splits; max_size drops the large one
+    np.testing.assert_array_equal(oracle.densify(recs, sums, counts, 0.5, 0.1, max_count=8, seed=3), out)
+    # max_size drops the large one; the room it leaves lets index 5 clone too
+    out2 = oracle.densify(recs, sums, counts, 0.5, 0.1, max_count=8, max_size=0.3, seed=3)
+    assert out2.shape[0] == 1 + 2 + 1 + 2
