@@ -251,6 +251,9 @@ def run_b200(args, rank, local, world, dist):
             N.check(r.lib.gs_host_free(host))
         e2e = dict(value=world * 1000.0 / (t_e / args.steps), unit="steps/s", h2d_bytes_per_step=int(targets.nbytes),
                    d2h_bytes_per_step=int(ctypes.sizeof(ctypes.c_float) * 0 + 64))
+    # ---- scene file load / save at the benchmark size, after the timed region
+    if not args.no_densify and not dp:
+        res["scene_io"] = scene_io_measure(r, args)
     # ---- densification on the device (trainScene's settings), after the timed region
     if not args.no_densify and not dp:
         res["densify"] = densify_measure(hmp, r, c, cams, ad, lam, window, args)
@@ -293,6 +296,26 @@ def profile_case(args):
         print(json.dumps(dict(case="profile", views=len(cams), pixels=int(st["pixels"]),
                               instances=int(st["instances"]), loss=float(loss),
                               stages_ms=r.stage_times()["ms"])), flush=True)
+
+
+def scene_io_measure(r, args):
+    """toPly with the SH bands and fromPly of the result through the C ABI (host bytes in
+    and out; the load sends the body to the device unchanged and transposes it there),
+    beside the restated fromPly on the host (numpy, SH0 part only)."""
+    t0 = time.perf_counter()
+    data = r.save_ply(with_sh=True)
+    save_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    n = r.load_ply(data)
+    load_ms = (time.perf_counter() - t0) * 1e3
+    out = dict(gaussians=int(n), ply_bytes=len(data), save_ms=round(save_ms, 2), load_ms=round(load_ms, 2))
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle as O
+        t0 = time.perf_counter()
+        O.from_ply(data)
+        out["cpu_from_ply_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    return out
 
 
 def densify_measure(hmp, r, c, cams, ad, lam, window, args):
@@ -478,6 +501,8 @@ def main():
         )
         if res.get("densify"):
             line["densify"] = res["densify"]
+        if res.get("scene_io"):
+            line["scene_io"] = res["scene_io"]
         if res.get("plain_stages"):
             ps = res["plain_stages"]
             line["plain_stages_ms_per_step"] = {k: round(v / max(1, ps["steps"]), 4) for k, v in ps["ms"].items()}

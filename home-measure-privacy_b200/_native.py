@@ -109,6 +109,9 @@ SIGNATURES = {
                                      ctypes.POINTER(c_int32)]),
     "gs_get_stream": (ctypes.c_int, [CTX, ctypes.POINTER(VP)]),
     "gs_get_blend_count": (ctypes.c_int, [CTX, ctypes.POINTER(ctypes.c_uint64)]),
+    "gs_load_ply": (ctypes.c_int, [CTX, VP, ctypes.c_int64, ctypes.POINTER(c_int32)]),
+    "gs_save_ply": (ctypes.c_int, [CTX, c_int32, VP, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+    "gs_save_splat": (ctypes.c_int, [CTX, VP, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "gs_set_densify_stats": (ctypes.c_int, [CTX, c_int32]),
     "gs_reset_densify_stats": (ctypes.c_int, [CTX]),
     "gs_get_densify_stats": (ctypes.c_int, [CTX, VP, VP]),

@@ -1758,6 +1758,85 @@ int gs_get_blend_count(GsContext* c, uint64_t* blends_out) {
     return GS_OK;
 }
 
+// ---- scene I/O ------------------------------------------------------------------------
+int gs_load_ply(GsContext* c, const void* data, int64_t bytes, int32_t* count_out) {
+    CTX_CHECK(c);
+    if (!data || bytes <= 0) return fail(GS_ERR_INVALID_ARG, "no data");
+    PlyHeaderInfo h;
+    std::string err;
+    if (ply_parse(data, bytes, c->planes, &h, &err) != 0) return fail(GS_ERR_INVALID_ARG, ".ply: %s", err.c_str());
+    if (h.count > (1 << 28)) return fail(GS_ERR_INVALID_ARG, ".ply: too many vertices");
+    const int n = (int)h.count;
+    CKI(resize_scene(c, n, false));
+    const size_t body = (size_t)h.count * h.nprops * 4;
+    if (body > 0) {
+        // The file's body as it is; the kernel transposes it into the parameter planes.
+        CKI(ensure(c->dn_scratch, body, c));
+        CK(cudaMemcpyAsync(c->dn_scratch.p, static_cast<const char*>(data) + h.header_bytes, body,
+                           cudaMemcpyHostToDevice, c->stream));
+    }
+    launch_ply_to_planes(c->dn_scratch.as<float>(), h, c->n_pad, c->planes, c->params.as<float>(), c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    if (count_out) *count_out = n;
+    return GS_OK;
+}
+
+int gs_save_ply(GsContext* c, int32_t with_sh, void* out, int64_t capacity, int64_t* bytes_out) {
+    CTX_CHECK(c);
+    if (!bytes_out) return fail(GS_ERR_INVALID_ARG, "bytes_out is null");
+    const int nk_out = with_sh ? (c->planes - 14) / 3 : 0;
+    const std::string header = ply_header(c->n, nk_out);
+    const int nprops = 17 + 3 * nk_out;
+    const size_t body = (size_t)c->n * nprops * 4;
+    const int64_t total = (int64_t)(header.size() + body);
+    *bytes_out = total;
+    if (!out) return GS_OK;
+    if (capacity < total) return fail(GS_ERR_CAPACITY, "buffer holds %lld of %lld bytes", (long long)capacity,
+                                      (long long)total);
+    memcpy(out, header.data(), header.size());
+    if (body > 0) {
+        CKI(ensure(c->dn_scratch, body, c));
+        launch_planes_to_ply(c->params.as<float>(), c->n, c->n_pad, c->planes, nk_out, c->dn_scratch.as<float>(),
+                             c->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(static_cast<char*>(out) + header.size(), c->dn_scratch.p, body, cudaMemcpyDeviceToHost,
+                           c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return GS_OK;
+}
+
+int gs_save_splat(GsContext* c, void* out, int64_t capacity, int64_t* bytes_out) {
+    CTX_CHECK(c);
+    if (!bytes_out) return fail(GS_ERR_INVALID_ARG, "bytes_out is null");
+    const int n = c->n;
+    std::vector<unsigned char> rec((size_t)n * 32), finite((size_t)n);
+    std::vector<double> weight((size_t)n);
+    if (n > 0) {
+        const size_t need = (size_t)n * (32 + 8 + 1) + 64;
+        CKI(ensure(c->dn_scratch, need, c));
+        unsigned char* d_rec = c->dn_scratch.as<unsigned char>();
+        double* d_w = reinterpret_cast<double*>(d_rec + (size_t)n * 32);
+        unsigned char* d_f = reinterpret_cast<unsigned char*>(d_w + n);
+        launch_splat_records(c->params.as<float>(), n, c->n_pad, d_rec, d_w, d_f, c->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(rec.data(), d_rec, (size_t)n * 32, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(weight.data(), d_w, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(finite.data(), d_f, (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    const std::vector<int> order = splat_order(weight, finite);
+    const int64_t total = (int64_t)order.size() * 32;
+    *bytes_out = total;
+    if (!out) return GS_OK;
+    if (capacity < total) return fail(GS_ERR_CAPACITY, "buffer holds %lld of %lld bytes", (long long)capacity,
+                                      (long long)total);
+    unsigned char* o = static_cast<unsigned char*>(out);
+    for (size_t k = 0; k < order.size(); k++) memcpy(o + k * 32, rec.data() + (size_t)order[k] * 32, 32);
+    return GS_OK;
+}
+
 // ---- densification ------------------------------------------------------------------
 int gs_set_densify_stats(GsContext* c, int32_t enable) {
     CTX_CHECK(c);

@@ -213,4 +213,25 @@ void launch_screen_grads16(const float4* sg8, const float* sg1, int n, float* ou
 void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb,
                      const uint32_t* keys, int n, float* out12, cudaStream_t s);
 
+// ---- scene I/O -------------------------------------------------------------------------
+struct PlyHeaderInfo {
+    int64_t header_bytes, count;
+    int nprops;
+    int col[GS_MAX_PLANES];   // file column of each parameter plane (-1: absent)
+    int dc[3];
+    int file_sh_coeffs;       // f_rest coefficients per channel in the file
+};
+}  // namespace gs
+#include <string>
+#include <vector>
+namespace gs {
+int ply_parse(const void* data, int64_t bytes, int planes, PlyHeaderInfo* out, std::string* err);
+void launch_ply_to_planes(const float* body, const PlyHeaderInfo& h, int n_pad, int planes, float* params,
+                          cudaStream_t s);
+std::string ply_header(int64_t n, int nk_out);
+void launch_planes_to_ply(const float* params, int n, int n_pad, int planes, int nk_out, float* body, cudaStream_t s);
+void launch_splat_records(const float* params, int n, int n_pad, unsigned char* rec, double* weight,
+                          unsigned char* finite, cudaStream_t s);
+std::vector<int> splat_order(const std::vector<double>& weight, const std::vector<unsigned char>& finite);
+
 }  // namespace gs

@@ -230,6 +230,31 @@ class Renderer:
         self.set_densify_stats(False)
         return self.get_gaussians()
 
+    # ---- scene files ---------------------------------------------------------------------
+    def load_ply(self, data):
+        """fromPly (trainer/gpu.js:983-999) into this context (f_rest bands up to its SH
+        degree); returns the count."""
+        buf = bytes(data)
+        n = ctypes.c_int32(0)
+        N.check(self.lib.gs_load_ply(self.ctx, buf, len(buf), ctypes.byref(n)))
+        return n.value
+
+    def save_ply(self, with_sh=False):
+        """toPly (trainer/gpu.js:524-531) -> bytes; with_sh adds the f_rest bands."""
+        size = ctypes.c_int64(0)
+        N.check(self.lib.gs_save_ply(self.ctx, 1 if with_sh else 0, None, 0, ctypes.byref(size)))
+        out = ctypes.create_string_buffer(size.value)
+        N.check(self.lib.gs_save_ply(self.ctx, 1 if with_sh else 0, out, size.value, ctypes.byref(size)))
+        return out.raw[:size.value]
+
+    def save_splat(self):
+        """toSplat (trainer/gpu.js:538-556) -> bytes."""
+        size = ctypes.c_int64(0)
+        N.check(self.lib.gs_save_splat(self.ctx, None, 0, ctypes.byref(size)))
+        out = ctypes.create_string_buffer(max(size.value, 1))
+        N.check(self.lib.gs_save_splat(self.ctx, out, size.value, ctypes.byref(size)))
+        return out.raw[:size.value]
+
     # ---- densification on the device --------------------------------------------------
     def set_densify_stats(self, enable=True):
         N.check(self.lib.gs_set_densify_stats(self.ctx, 1 if enable else 0))

@@ -255,6 +255,26 @@ GS_API int gs_step_apply(GsContext* ctx, const GsAdamConfig* adam, float* loss_o
  * library's: a collective over gs_step_gradients' buffer, a copy, an event. */
 GS_API int gs_get_stream(GsContext* ctx, void** stream_out);
 
+/* ---- Scene files ---------------------------------------------------------------------
+ * fromPly (trainer/gpu.js:983-999): replaces the context's Gaussians with a binary
+ * little-endian .ply of float vertex properties (x y z, scale_0..2, rot_0..3 w x y z,
+ * opacity, f_dc_0..2 required; colour = clamp(f_dc SH0 + 0.5, 0, 1)), and, beyond the
+ * reference, the f_rest_* bands up to the context's SH degree (channel-major; missing
+ * bands are zero).  The header is looked for in the first 4096 bytes, as the reference
+ * does.  The file's body goes to the device unchanged and is transposed there. */
+GS_API int gs_load_ply(GsContext* ctx, const void* data, int64_t bytes, int32_t* count_out);
+
+/* toPly (trainer/gpu.js:524-531): with_sh = 0 gives the reference's 17 properties
+ * (x y z nx ny nz f_dc_0..2 opacity scale_0..2 rot_0..3, f_dc = (colour - 0.5) / SH0);
+ * with_sh = 1 adds f_rest_* after f_dc (the 3DGS order).  out = NULL: *bytes_out gets
+ * the size only. */
+GS_API int gs_save_ply(GsContext* ctx, int32_t with_sh, void* out, int64_t capacity, int64_t* bytes_out);
+
+/* toSplat (trainer/gpu.js:538-556): 32 bytes per finite Gaussian (position, scales,
+ * colour / opacity / rotation bytes), largest exp(sum log-scales) x opacity first, ties
+ * in index order.  out = NULL: *bytes_out gets the size only. */
+GS_API int gs_save_splat(GsContext* ctx, void* out, int64_t capacity, int64_t* bytes_out);
+
 /* ---- Densification (trainer/gpu.js:484-497 STATS, :564-599 sceneExtent / densify,
  * :902-903 and :944 the opacity reset) --------------------------------------------------
  * The reference reads every Gaussian back to the host each densification, densifies in

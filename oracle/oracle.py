@@ -5,6 +5,7 @@ the product never imports it.  See gs_oracle.c for what each function restates
 (trainer/gpu.js of barakatiass-alt/home-measure-privacy) and how parity is pinned.
 """
 import ctypes
+import math
 import os
 import subprocess
 
@@ -217,3 +218,62 @@ def sh_constants64():
     out = np.zeros(15, np.float64)
     lib().d64_sh_constants(out)
     return out
+
+
+# ---- scene files (fromPly / toPly / toSplat, trainer/gpu.js:983-999, :524-556) -----------
+SH0 = 0.28209479177387814
+
+
+def from_ply(data):
+    """fromPly: bytes of a binary .ply -> host records (float32, n x 14), SH0 only."""
+    head_end = data.index(b"end_header\n", 0, 4096 + 11) + len(b"end_header\n")
+    header = data[:head_end].decode()
+    count = int(header.split("element vertex ")[1].split()[0])
+    props = [ln.split()[2] for ln in header.splitlines() if ln.startswith("property float")]
+    body = np.frombuffer(data[head_end:head_end + count * len(props) * 4], np.float32).reshape(count, len(props))
+    at = {p: body[:, k] for k, p in enumerate(props)}
+    rec = np.zeros((count, 14), np.float32)
+    rec[:, 0], rec[:, 1], rec[:, 2] = at["x"], at["y"], at["z"]
+    rec[:, 3], rec[:, 4], rec[:, 5] = at["scale_0"], at["scale_1"], at["scale_2"]
+    rec[:, 6], rec[:, 7], rec[:, 8], rec[:, 9] = at["rot_0"], at["rot_1"], at["rot_2"], at["rot_3"]
+    rec[:, 10] = at["opacity"]
+    for k in range(3):
+        rec[:, 11 + k] = np.clip(at[f"f_dc_{k}"].astype(np.float64) * SH0 + 0.5, 0.0, 1.0)
+    return rec
+
+
+def to_ply(rec):
+    """toPly: host records (n x >= 14) -> bytes (the reference's 17 properties)."""
+    props = ["x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2", "opacity", "scale_0", "scale_1",
+             "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"]
+    n = rec.shape[0]
+    header = "\n".join(["ply", "format binary_little_endian 1.0", f"element vertex {n}"]
+                       + [f"property float {p}" for p in props] + ["end_header", ""])
+    body = np.zeros((n, 17), np.float32)
+    body[:, 0:3] = rec[:, 0:3]
+    body[:, 6:9] = (rec[:, 11:14].astype(np.float64) - 0.5) / SH0
+    body[:, 9] = rec[:, 10]
+    body[:, 10:13] = rec[:, 3:6]
+    body[:, 13:17] = rec[:, 6:10]
+    return header.encode() + body.tobytes()
+
+
+def to_splat(rec):
+    """toSplat: host records -> bytes, 32 per finite splat, largest weight first."""
+    def js_byte(v):
+        return max(0, min(255, math.floor(v + 0.5)))
+
+    keep = [i for i in range(rec.shape[0]) if np.all(np.isfinite(rec[i, :14]))]
+    weight = [math.exp(float(rec[i, 3]) + float(rec[i, 4]) + float(rec[i, 5])) / (1 + math.exp(-float(rec[i, 10])))
+              for i in keep]
+    order = sorted(range(len(keep)), key=lambda k: -weight[k])  # stable, as Array.sort
+    out = bytearray()
+    for k in order:
+        g = rec[keep[k]]
+        f = np.array([g[0], g[1], g[2]] + [math.exp(float(g[3 + j])) for j in range(3)], np.float32)
+        q = [float(v) for v in g[6:10]]
+        ln = math.hypot(*q) or 1.0
+        u = [js_byte(float(c) * 255) for c in g[11:14]] + [js_byte(255 / (1 + math.exp(-float(g[10]))))]
+        u += [js_byte(v / ln * 128 + 128) for v in q]
+        out += f.tobytes() + bytes(u)
+    return bytes(out)

@@ -11,6 +11,12 @@ ssim_test.npz -- the reference's loss-gradient check, trainer/ssim-test.html, re
     of the GPU gradient against these values and checks the L1-only gradient against
     sign(x - y) / len to 1e-9 (ssim-test.html:41-54).
 
+sample_head256.ply / sample_head256.npz -- the first 256 splats of tour/sample.ply as a
+    .ply of their own (the reference's header with the vertex count set to 256, then the
+    first 256 rows of its body), with what the CPU restatements of fromPly, toPly and
+    toSplat (oracle/oracle.py) make of it: the records, the .ply bytes of those records
+    and the .splat bytes.
+
 sample_ply_quarter.npz -- every 4th splat of the reference's tour/sample.ply (the start
     set of trainer/scene-test.html:77), decoded as fromPly does (trainer/gpu.js:983-999:
     colour = clamp(f_dc * SH0 + 0.5, 0, 1), opacity logit, log-scales, rotation w,x,y,z),
@@ -99,8 +105,26 @@ def from_ply(path):
     return rec
 
 
+def make_ply_head(n=256):
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+    import oracle as O
+    data = open(os.path.join(REF, "tour", "sample.ply"), "rb").read()
+    head_end = data.index(b"end_header\n") + len(b"end_header\n")
+    header = data[:head_end].decode()
+    count = int(header.split("element vertex ")[1].split()[0])
+    props = [ln for ln in header.splitlines() if ln.startswith("property float")]
+    head = header.replace(f"element vertex {count}\n", f"element vertex {n}\n").encode()
+    small = head + data[head_end:head_end + n * len(props) * 4]
+    open(os.path.join(HERE, "sample_head256.ply"), "wb").write(small)
+    rec = O.from_ply(small)
+    np.savez_compressed(os.path.join(HERE, "sample_head256.npz"), records=rec,
+                        ply=np.frombuffer(O.to_ply(rec), np.uint8), splat=np.frombuffer(O.to_splat(rec), np.uint8))
+    return rec.shape[0]
+
+
 if __name__ == "__main__":
     print("ssim case indices:", make_ssim_case())
+    print("sample.ply head splats:", make_ply_head())
     rec = from_ply(os.path.join(REF, "tour", "sample.ply"))
     quarter = rec[::4].copy()
     np.savez_compressed(os.path.join(HERE, "sample_ply_quarter.npz"), records=quarter)
