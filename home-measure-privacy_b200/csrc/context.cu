@@ -115,7 +115,8 @@ struct GsContext {
     DevBuf stats;                       // densification statistics [2][n_pad]: norm sums, view counts
     bool stats_on = false;              // training steps accumulate them
     bool stats_active = false;          // set while a training step's kernels are enqueued
-    DevBuf dn_scratch;                  // densify block sums and result
+    DevBuf dn_scratch;                  // densify block sums and result; scene-file bodies
+    DevBuf nb_scratch;                  // neighbour search: table, cubes, points
     // views: training views [0, V) plus one scratch view at index V for render /
     // gradients / loss-gradient calls on arbitrary cameras or images
     std::vector<GsCamera> cams;
@@ -1755,6 +1756,97 @@ int gs_get_blend_count(GsContext* c, uint64_t* blends_out) {
     CK(cudaMemcpyAsync(&n, c->scratch16.p, 8, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     *blends_out = (uint64_t)n;
+    return GS_OK;
+}
+
+// ---- initialisation from points ---------------------------------------------------------
+// Device copies of xyz (and rgb), the neighbour table and the sizes in nb_scratch;
+// returns the device sizes.
+static int neighbour_sizes_device(GsContext* c, const float* xyz, int count, double mn, double mx, double fb,
+                                  const float* rgb, float** d_xyz_out, float** d_rgb_out, float** d_sizes_out) {
+    unsigned T = 1024;
+    while (T < 2u * (unsigned)count) T <<= 1;
+    const size_t n = (size_t)count;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off += (bytes + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_keys = take((size_t)T * 8), o_ids = take((size_t)T * 4), o_cnt = take(64);
+    const size_t o_slot = take(n * 4), o_cc = take(n * 4), o_cs = take(n * 4), o_cur = take(n * 4),
+                 o_pts = take(n * 4), o_xyz = take(n * 12), o_rgb = take(n * 12), o_sz = take(n * 4);
+    CKI(ensure(c->nb_scratch, off, c));
+    char* base = c->nb_scratch.as<char>();
+    NeighbourArgs a;
+    memset(&a, 0, sizeof a);
+    a.xyz = reinterpret_cast<float*>(base + o_xyz);
+    a.count = count;
+    a.keys = reinterpret_cast<unsigned long long*>(base + o_keys);
+    a.ids = reinterpret_cast<unsigned*>(base + o_ids);
+    a.mask = T - 1;
+    a.counters = reinterpret_cast<unsigned*>(base + o_cnt);
+    a.point_slot = reinterpret_cast<unsigned*>(base + o_slot);
+    a.cell_count = reinterpret_cast<unsigned*>(base + o_cc);
+    a.cell_start = reinterpret_cast<unsigned*>(base + o_cs);
+    a.cell_cursor = reinterpret_cast<unsigned*>(base + o_cur);
+    a.cell_points = reinterpret_cast<unsigned*>(base + o_pts);
+    a.sizes = reinterpret_cast<float*>(base + o_sz);
+    a.min_size = mn;
+    a.max_size = mx;
+    a.fallback = fb;
+    CK(cudaMemcpyAsync(base + o_xyz, xyz, n * 12, cudaMemcpyHostToDevice, c->stream));
+    if (rgb) CK(cudaMemcpyAsync(base + o_rgb, rgb, n * 12, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(a.keys, 0xff, (size_t)T * 8, c->stream));
+    CK(cudaMemsetAsync(a.counters, 0, 64, c->stream));
+    CK(cudaMemsetAsync(a.cell_count, 0, n * 4, c->stream));
+    launch_neighbour_sizes(a, c->stream);
+    CK(cudaGetLastError());
+    *d_xyz_out = reinterpret_cast<float*>(base + o_xyz);
+    if (d_rgb_out) *d_rgb_out = reinterpret_cast<float*>(base + o_rgb);
+    *d_sizes_out = a.sizes;
+    return GS_OK;
+}
+
+int gs_neighbour_sizes(GsContext* c, const float* xyz, int32_t count, double min_size, double max_size,
+                       double fallback, float* sizes_out) {
+    CTX_CHECK(c);
+    if (count < 0 || count > (1 << 28) || (count > 0 && (!xyz || !sizes_out)))
+        return fail(GS_ERR_INVALID_ARG, "bad point count or pointer");
+    if (count == 0) return GS_OK;
+    float *dx = nullptr, *ds = nullptr;
+    CKI(neighbour_sizes_device(c, xyz, count, min_size, max_size, fallback, nullptr, &dx, nullptr, &ds));
+    CK(cudaMemcpyAsync(sizes_out, ds, (size_t)count * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return GS_OK;
+}
+
+int gs_init_from_points(GsContext* c, const float* xyz, const float* rgb, int32_t count, float size) {
+    CTX_CHECK(c);
+    if (count < 0 || count > (1 << 28) || (count > 0 && (!xyz || !rgb)))
+        return fail(GS_ERR_INVALID_ARG, "bad point count or pointer");
+    if (count == 0) {
+        std::vector<float> none((size_t)c->planes * 128, 0.f);
+        for (int i = 0; i < 128; i++) none[(size_t)6 * 128 + i] = 1.f;
+        return upload_planes(c, 0, none);
+    }
+    float *dx = nullptr, *drgb = nullptr, *ds = nullptr;
+    if (size > 0.f) {
+        CKI(ensure(c->nb_scratch, (size_t)count * 24 + 256, c));
+        dx = c->nb_scratch.as<float>();
+        drgb = dx + (size_t)count * 3 + 64;
+        CK(cudaMemcpyAsync(dx, xyz, (size_t)count * 12, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(drgb, rgb, (size_t)count * 12, cudaMemcpyHostToDevice, c->stream));
+    } else {
+        // neighbourSizes with the reference's defaults (min 0.005, max 0.1, fallback 0.06).
+        CKI(neighbour_sizes_device(c, xyz, count, 0.005, 0.1, 0.06, rgb, &dx, &drgb, &ds));
+    }
+    // resize_scene allocates only the per-Gaussian buffers; the scratch stays valid.
+    CKI(resize_scene(c, count, false));
+    launch_init_planes(dx, drgb, size > 0.f ? nullptr : ds, size, count, c->n_pad, c->planes, c->params.as<float>(),
+                       c->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
     return GS_OK;
 }
 

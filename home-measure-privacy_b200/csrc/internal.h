@@ -213,6 +213,26 @@ void launch_screen_grads16(const float4* sg8, const float* sg1, int n, float* ou
 void launch_splats12(const float4* geo0, const float4* geo1, const float4* rgb,
                      const uint32_t* keys, int n, float* out12, cudaStream_t s);
 
+// ---- initialisation from points -----------------------------------------------------------
+struct NeighbourArgs {
+    const float* xyz;
+    int count;
+    unsigned long long* keys;   // hash table of cube keys (mask + 1 entries, empty = all ones)
+    unsigned* ids;              // dense cube id per table entry
+    unsigned mask;
+    unsigned* counters;         // [0] cubes
+    unsigned* point_slot;       // table entry of each point's cube
+    unsigned* cell_count;       // points per cube
+    unsigned* cell_start;
+    unsigned* cell_cursor;
+    unsigned* cell_points;      // point indices grouped by cube
+    float* sizes;
+    double min_size, max_size, fallback;
+};
+void launch_neighbour_sizes(const NeighbourArgs& a, cudaStream_t s);
+void launch_init_planes(const float* xyz, const float* rgb, const float* sizes, float fixed_size, int count, int n_pad,
+                        int planes, float* params, cudaStream_t s);
+
 // ---- scene I/O -------------------------------------------------------------------------
 struct PlyHeaderInfo {
     int64_t header_bytes, count;

@@ -9,6 +9,7 @@ reference throws Error, trainer/gpu.js:705).  There is no CPU path.
 """
 import ctypes
 import math
+from builtins import max as max_
 
 import numpy as np
 
@@ -228,6 +229,24 @@ class Renderer:
                 loss_sum, loss_count = 0.0, 0
         N.check(self.lib.gs_synchronize(self.ctx))
         self.set_densify_stats(False)
+        return self.get_gaussians()
+
+    # ---- initialisation from a point cloud ------------------------------------------------
+    def neighbour_sizes(self, xyz, min=0.005, max=0.1, fallback=0.06):
+        """neighbourSizes (trainer/neighbours.js:13-53) on the device."""
+        xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+        out = np.zeros(max_(len(xyz), 1), np.float32)
+        N.check(self.lib.gs_neighbour_sizes(self.ctx, N.ptr(xyz), len(xyz), float(min), float(max), float(fallback),
+                                            N.ptr(out)))
+        return out[:len(xyz)]
+
+    def initFromPoints(self, points, size=None):
+        """initFromPoints({xyz, rgb, count}, size) (trainer/gpu.js:507-521) into this
+        context; returns the Gaussians as host records."""
+        xyz = np.ascontiguousarray(points["xyz"], np.float32).reshape(-1, 3)
+        rgb = np.ascontiguousarray(points["rgb"], np.float32).reshape(-1, 3)
+        n = int(points.get("count", len(xyz)))
+        N.check(self.lib.gs_init_from_points(self.ctx, N.ptr(xyz), N.ptr(rgb), n, float(size or 0.0)))
         return self.get_gaussians()
 
     # ---- scene files ---------------------------------------------------------------------

@@ -255,6 +255,20 @@ GS_API int gs_step_apply(GsContext* ctx, const GsAdamConfig* adam, float* loss_o
  * library's: a collective over gs_step_gradients' buffer, a copy, an event. */
 GS_API int gs_get_stream(GsContext* ctx, void** stream_out);
 
+/* ---- Initialisation from a point cloud ----------------------------------------------
+ * neighbourSizes (trainer/neighbours.js:13-53): per point, the root mean square distance
+ * to its 3 nearest other points within the 27 cubes of 0.1 m around its own, clamped to
+ * [min_size, max_size], or `fallback` when there is none.  xyz: count x 3 floats.
+ * sizes_out: count floats. */
+GS_API int gs_neighbour_sizes(GsContext* ctx, const float* xyz, int32_t count, double min_size, double max_size,
+                              double fallback, float* sizes_out);
+
+/* initFromPoints (trainer/gpu.js:507-521): replaces the context's Gaussians with one per
+ * point: log-size on all axes (`size` > 0 for all, else neighbourSizes with the
+ * reference's defaults 0.005 / 0.1 / 0.06), identity rotation, opacity 0.1, the point's
+ * colour (rgb: count x 3 floats in [0, 1]); SH bands zero. */
+GS_API int gs_init_from_points(GsContext* ctx, const float* xyz, const float* rgb, int32_t count, float size);
+
 /* ---- Scene files ---------------------------------------------------------------------
  * fromPly (trainer/gpu.js:983-999): replaces the context's Gaussians with a binary
  * little-endian .ply of float vertex properties (x y z, scale_0..2, rot_0..3 w x y z,

@@ -1176,3 +1176,80 @@ int orc_densify(const float* params, int n, int stride, const float* sums, const
     }
     return o;
 }
+
+/* ---------------------------------------------------------------------------------
+ * neighbourSizes (trainer/neighbours.js:13-53): cubes of 0.1 m keyed as the reference
+ * keys its Map; per point the three smallest squared distances (double) to other points
+ * of the 27 surrounding cubes, their root mean, clamped; `fallback` with none.  Cubes are
+ * found here by sorting (key, point) pairs and binary search (the result does not depend
+ * on the order inside a cube).
+ * --------------------------------------------------------------------------------- */
+typedef struct {
+    long long key;
+    int idx;
+} OrcCellPt;
+
+static int cmp_cellpt(const void* a, const void* b) {
+    const long long ka = ((const OrcCellPt*)a)->key, kb = ((const OrcCellPt*)b)->key;
+    if (ka != kb) return ka < kb ? -1 : 1;
+    return ((const OrcCellPt*)a)->idx - ((const OrcCellPt*)b)->idx;
+}
+
+static long long orc_cell(float v) { return (long long)floor((double)v / 0.1); }
+static long long orc_key(long long i, long long j, long long k) {
+    return ((i + 32768) * 65536 + (j + 32768)) * 65536 + (k + 32768);
+}
+
+void orc_neighbour_sizes(const float* xyz, int count, double mn, double mx, double fallback, float* sizes) {
+    OrcCellPt* pts = (OrcCellPt*)malloc(sizeof(OrcCellPt) * (size_t)(count > 0 ? count : 1));
+    for (int p = 0; p < count; p++) {
+        pts[p].key = orc_key(orc_cell(xyz[p * 3]), orc_cell(xyz[p * 3 + 1]), orc_cell(xyz[p * 3 + 2]));
+        pts[p].idx = p;
+    }
+    qsort(pts, (size_t)count, sizeof(OrcCellPt), cmp_cellpt);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int p = 0; p < count; p++) {
+        double best[3] = {INFINITY, INFINITY, INFINITY};
+        const long long ci = orc_cell(xyz[p * 3]), cj = orc_cell(xyz[p * 3 + 1]), ck = orc_cell(xyz[p * 3 + 2]);
+        const double x = xyz[p * 3], y = xyz[p * 3 + 1], z = xyz[p * 3 + 2];
+        for (int di = -1; di <= 1; di++)
+            for (int dj = -1; dj <= 1; dj++)
+                for (int dk = -1; dk <= 1; dk++) {
+                    const long long key = orc_key(ci + di, cj + dj, ck + dk);
+                    int lo = 0, hi = count;  /* first entry with key >= wanted */
+                    while (lo < hi) {
+                        const int mid = (lo + hi) / 2;
+                        if (pts[mid].key < key) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    for (int t = lo; t < count && pts[t].key == key; t++) {
+                        const int q = pts[t].idx;
+                        if (q == p) continue;
+                        const double dx = (double)xyz[q * 3] - x, dy = (double)xyz[q * 3 + 1] - y,
+                                     dz = (double)xyz[q * 3 + 2] - z;
+                        const double d2 = dx * dx + dy * dy + dz * dz;
+                        if (d2 >= best[2]) continue;
+                        if (d2 < best[0]) {
+                            best[2] = best[1];
+                            best[1] = best[0];
+                            best[0] = d2;
+                        } else if (d2 < best[1]) {
+                            best[2] = best[1];
+                            best[1] = d2;
+                        } else {
+                            best[2] = d2;
+                        }
+                    }
+                }
+        int found = 0;
+        double sum = 0.0;
+        for (int k = 0; k < 3; k++)
+            if (isfinite(best[k])) {
+                sum += best[k];
+                found++;
+            }
+        const double size = found ? sqrt(sum / found) : fallback;
+        sizes[p] = (float)fmin(mx, fmax(mn, size));
+    }
+    free(pts);
+}

@@ -46,6 +46,8 @@ def lib():
         CP = ctypes.POINTER(OrcCamera)
         i, f, d = ctypes.c_int, ctypes.c_float, ctypes.c_double
         i64 = ctypes.c_int64
+        L.orc_neighbour_sizes.argtypes = [F32P, i, d, d, d, F32P]
+        L.orc_neighbour_sizes.restype = None
         L.orc_densify.argtypes = [F32P, i, i, F32P, F32P, d, d, d, d, i, ctypes.c_uint64, F32P]
         L.orc_densify.restype = i
         L.orc_stride.argtypes = [i]
@@ -153,6 +155,28 @@ def adam(params, grads, m, v, degree, t, lr6, beta1=0.9, beta2=0.999, eps=1e-8):
     n = params.shape[0]
     lib().orc32_adam(params.reshape(-1), np.ascontiguousarray(grads, np.float32).reshape(-1), m.reshape(-1),
                      v.reshape(-1), n, degree, t, np.asarray(lr6, np.float32), beta1, beta2, eps)
+
+
+def neighbour_sizes(xyz, min_size=0.005, max_size=0.1, fallback=0.06):
+    """neighbourSizes (trainer/neighbours.js:13-53): xyz (n x 3) -> sizes (n)."""
+    xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1)
+    n = xyz.size // 3
+    out = np.zeros(max(n, 1), np.float32)
+    lib().orc_neighbour_sizes(xyz if n else np.zeros(3, np.float32), n, min_size, max_size, fallback, out)
+    return out[:n]
+
+
+def init_from_points(xyz, rgb, sizes, degree=0):
+    """initFromPoints (trainer/gpu.js:507-521) -> host records."""
+    n = xyz.shape[0]
+    rec = np.zeros((n, stride(degree)), np.float32)
+    rec[:, 0:3] = xyz
+    ls = np.log(sizes.astype(np.float64)).astype(np.float32)
+    rec[:, 3:6] = ls[:, None]
+    rec[:, 6] = 1.0
+    rec[:, 10] = np.float32(math.log(0.1 / (1 - 0.1)))
+    rec[:, 11:14] = rgb
+    return rec
 
 
 def densify(params, sums, counts, grad_threshold=2e-4, size_threshold=0.1, min_opacity=0.005, max_count=400000,

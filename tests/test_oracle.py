@@ -275,3 +275,44 @@ def test_scene_file_fixture_consistent(oracle):
     back = oracle.from_ply(oracle.to_ply(rec))
     np.testing.assert_array_equal(back[:, :11], rec[:, :11])
     np.testing.assert_allclose(back[:, 11:], rec[:, 11:], atol=1e-7)
+
+
+def _neighbour_sizes_literal(xyz, mn=0.005, mx=0.1, fallback=0.06):
+    """trainer/neighbours.js:13-53 line by line (a dict of cube lists, Python floats)."""
+    cell = 0.1
+    key = lambda i, j, k: ((i + 32768) * 65536 + (j + 32768)) * 65536 + (k + 32768)
+    pts = [[float(v) for v in p] for p in xyz]
+    cell_of = lambda p: [math.floor(p[a] / cell) for a in range(3)]
+    cells = {}
+    for idx, p in enumerate(pts):
+        cells.setdefault(key(*cell_of(p)), []).append(idx)
+    out = np.zeros(len(pts), np.float32)
+    for idx, p in enumerate(pts):
+        best = [math.inf] * 3
+        ci, cj, ck = cell_of(p)
+        for di in (-1, 0, 1):
+            for dj in (-1, 0, 1):
+                for dk in (-1, 0, 1):
+                    for q in cells.get(key(ci + di, cj + dj, ck + dk), []):
+                        if q == idx:
+                            continue
+                        dx, dy, dz = pts[q][0] - p[0], pts[q][1] - p[1], pts[q][2] - p[2]
+                        d2 = dx * dx + dy * dy + dz * dz
+                        if d2 >= best[2]:
+                            continue
+                        if d2 < best[0]:
+                            best = [d2, best[0], best[1]]
+                        elif d2 < best[1]:
+                            best = [best[0], d2, best[1]]
+                        else:
+                            best[2] = d2
+        found = [b for b in best if math.isfinite(b)]
+        size = math.sqrt(sum(found) / len(found)) if found else fallback
+        out[idx] = min(mx, max(mn, size))
+    return out
+
+
+def test_neighbour_sizes_literal(oracle):
+    rng = np.random.default_rng(5)
+    xyz = np.concatenate([rng.normal(0, 0.15, (300, 3)), rng.uniform(-3, 3, (40, 3))]).astype(np.float32)
+    np.testing.assert_array_equal(oracle.neighbour_sizes(xyz), _neighbour_sizes_literal(xyz))
