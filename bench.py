@@ -254,6 +254,7 @@ def run_b200(args, rank, local, world, dist):
     # ---- scene file load / save at the benchmark size, after the timed region
     if not args.no_densify and not dp:
         res["scene_io"] = scene_io_measure(r, args)
+        res["init"] = init_measure(r, args)
     # ---- densification on the device (trainScene's settings), after the timed region
     if not args.no_densify and not dp:
         res["densify"] = densify_measure(hmp, r, c, cams, ad, lam, window, args)
@@ -296,6 +297,28 @@ def profile_case(args):
         print(json.dumps(dict(case="profile", views=len(cams), pixels=int(st["pixels"]),
                               instances=int(st["instances"]), loss=float(loss),
                               stages_ms=r.stage_times()["ms"])), flush=True)
+
+
+def init_measure(r, args):
+    """neighbourSizes for 1M points 3 cm apart on a sphere (a LiDAR-like scan) through the
+    C ABI, beside the restated reference on all host threads."""
+    rng = np.random.default_rng(21)
+    v = rng.normal(size=(1_000_000, 3))
+    xyz = (8.5 * v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+    r.neighbour_sizes(xyz[:1000])  # first call sizes the scratch
+    t0 = time.perf_counter()
+    sizes = r.neighbour_sizes(xyz)
+    gpu_ms = (time.perf_counter() - t0) * 1e3
+    out = dict(points=len(xyz), gpu_ms=round(gpu_ms, 2), note="host-timed C-ABI call incl. 12 MB up, 4 MB down")
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle as O
+        t0 = time.perf_counter()
+        ref = O.neighbour_sizes(xyz)
+        out["cpu_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+        out["cpu_threads"] = O.num_threads()
+        out["matches_cpu"] = bool(np.array_equal(ref, sizes))
+    return out
 
 
 def scene_io_measure(r, args):
@@ -503,6 +526,8 @@ def main():
             line["densify"] = res["densify"]
         if res.get("scene_io"):
             line["scene_io"] = res["scene_io"]
+        if res.get("init"):
+            line["init"] = res["init"]
         if res.get("plain_stages"):
             ps = res["plain_stages"]
             line["plain_stages_ms_per_step"] = {k: round(v / max(1, ps["steps"]), 4) for k, v in ps["ms"].items()}

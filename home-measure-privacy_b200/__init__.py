@@ -12,4 +12,4 @@ helpers.  Import it by path:
 from ._native import GsError, load  # noqa: F401
 from .scene import (camera_centre, config, look_at, packGaussians, records_from_packed,  # noqa: F401
                     ring_cameras, stride, synthetic_scene, unpackGaussians)
-from .trainer import Renderer, adam_config, createRenderer, sceneExtent, shuffled  # noqa: F401
+from .trainer import Renderer, adam_config, chooseSharp, createRenderer, sceneExtent, shuffled  # noqa: F401

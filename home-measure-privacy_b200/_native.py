@@ -111,6 +111,8 @@ SIGNATURES = {
     "gs_get_blend_count": (ctypes.c_int, [CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "gs_neighbour_sizes": (ctypes.c_int, [CTX, VP, c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, VP]),
     "gs_init_from_points": (ctypes.c_int, [CTX, VP, VP, c_int32, c_float]),
+    "gs_sharpness": (ctypes.c_int, [CTX, VP, c_int32, c_int32, c_int32, c_int32, VP]),
+    "gs_choose_sharp": (ctypes.c_int, [VP, c_int32, c_int32, VP, ctypes.POINTER(c_int32)]),
     "gs_load_ply": (ctypes.c_int, [CTX, VP, ctypes.c_int64, ctypes.POINTER(c_int32)]),
     "gs_save_ply": (ctypes.c_int, [CTX, c_int32, VP, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "gs_save_splat": (ctypes.c_int, [CTX, VP, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),

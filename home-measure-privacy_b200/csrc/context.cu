@@ -1850,6 +1850,74 @@ int gs_init_from_points(GsContext* c, const float* xyz, const float* rgb, int32_
     return GS_OK;
 }
 
+// ---- photo selection -------------------------------------------------------------------
+int gs_sharpness(GsContext* c, const uint8_t* images, int32_t count, int32_t width, int32_t height,
+                 int32_t channels, double* scores) {
+    CTX_CHECK(c);
+    if (count < 0 || width < 1 || height < 1 || (channels != 1 && channels != 3) || (count > 0 && (!images || !scores)))
+        return fail(GS_ERR_INVALID_ARG, "bad images");
+    if (count == 0) return GS_OK;
+    const size_t px = (size_t)width * height * count;
+    const size_t off_grey = ((px * channels + 255) & ~(size_t)255);
+    const size_t off_sums = off_grey + ((px + 255) & ~(size_t)255);
+    CKI(ensure(c->nb_scratch, off_sums + (size_t)count * 16, c));
+    uint8_t* base = c->nb_scratch.as<uint8_t>();
+    CK(cudaMemcpyAsync(base, images, px * channels, cudaMemcpyHostToDevice, c->stream));
+    const uint8_t* grey = base;
+    if (channels == 3) {
+        launch_grey(base, px, base + off_grey, c->stream);
+        grey = base + off_grey;
+    }
+    long long* sums = reinterpret_cast<long long*>(base + off_sums);
+    CK(cudaMemsetAsync(sums, 0, (size_t)count * 16, c->stream));
+    launch_laplacian_sums(grey, count, width, height, sums, c->stream);
+    CK(cudaGetLastError());
+    std::vector<long long> h((size_t)count * 2);
+    CK(cudaMemcpyAsync(h.data(), sums, (size_t)count * 16, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const long long n = (long long)std::max(0, width - 2) * std::max(0, height - 2);
+    for (int k = 0; k < count; k++) {
+        if (!n) {
+            scores[k] = 0.0;
+            continue;
+        }
+        const double mean = (double)h[2 * k] / (double)n;
+        scores[k] = (double)h[2 * k + 1] / (double)n - mean * mean;
+    }
+    return GS_OK;
+}
+
+int gs_choose_sharp(const double* scores, int32_t count, int32_t max_views, int32_t* chosen, int32_t* chosen_count) {
+    if (count < 0 || max_views < 1 || (count > 0 && (!scores || !chosen)) || !chosen_count)
+        return fail(GS_ERR_INVALID_ARG, "bad arguments");
+    // chooseSharp (trainer/sharpness.js:39-55) in the reference's double arithmetic.
+    const double step = std::max(1.0, (double)count / (double)max_views);
+    std::vector<int> pick;
+    for (double start = 0; start < count; start += step) {
+        const int from = (int)std::floor(start);
+        const int to = (int)std::min((double)count, std::floor(start + step));
+        int best = from;
+        for (int i = from + 1; i < to; i++)
+            if (scores[i] > scores[best]) best = i;
+        pick.push_back(best);
+    }
+    std::vector<double> sorted(scores, scores + count);
+    std::stable_sort(sorted.begin(), sorted.end(), [](double a, double b) { return a - b < 0; });
+    const double median = count ? sorted[(size_t)((count - 1) / 2)] : 0.0;
+    std::vector<int> blurry;
+    for (int i : pick)
+        if (scores[i] < median * 0.35) blurry.push_back(i);
+    std::stable_sort(blurry.begin(), blurry.end(), [&](int a, int b) { return scores[a] - scores[b] < 0; });
+    const size_t ndrop = std::min(blurry.size(), (size_t)std::floor(pick.size() * 0.25));
+    std::vector<char> drop((size_t)std::max(count, 1), 0);
+    for (size_t k = 0; k < ndrop; k++) drop[(size_t)blurry[k]] = 1;
+    int m = 0;
+    for (int i : pick)
+        if (!drop[(size_t)i]) chosen[m++] = i;
+    *chosen_count = m;
+    return GS_OK;
+}
+
 // ---- scene I/O ------------------------------------------------------------------------
 int gs_load_ply(GsContext* c, const void* data, int64_t bytes, int32_t* count_out) {
     CTX_CHECK(c);

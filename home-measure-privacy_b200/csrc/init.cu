@@ -10,6 +10,8 @@
 // walks its 27 cubes.  The three smallest squared distances and their mean are order-
 // independent, so the bucket order does not matter; distances use double arithmetic
 // with explicit rounding (no fused multiply-add), as JavaScript evaluates them.
+#include <algorithm>
+
 #include "internal.h"
 
 namespace gs {
@@ -200,6 +202,54 @@ void launch_init_planes(const float* xyz, const float* rgb, const float* sizes, 
                         int planes, float* params, cudaStream_t s) {
     const int blocks = (n_pad + 255) / 256;
     if (blocks > 0) init_planes_kernel<<<blocks, 256, 0, s>>>(xyz, rgb, sizes, fixed_size, count, n_pad, planes, params);
+}
+
+}  // namespace gs
+
+// ---- photo selection (trainer/sharpness.js:15-31, trainer/dataset.js:45) ---------------------
+namespace gs {
+
+// Grey bytes of RGB bytes: (77 R + 150 G + 29 B) >> 8, as dataset.js:45 does.
+__global__ void grey_kernel(const uint8_t* __restrict__ rgb, size_t pixels, uint8_t* __restrict__ grey) {
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= pixels) return;
+    grey[p] = (uint8_t)((rgb[p * 3] * 77 + rgb[p * 3 + 1] * 150 + rgb[p * 3 + 2] * 29) >> 8);
+}
+
+// Per image (blockIdx.y): sums of the 4-neighbour Laplacian and of its square over the
+// interior pixels, in exact integers.
+__global__ void laplacian_sums_kernel(const uint8_t* __restrict__ grey, int width, int height,
+                                      long long* __restrict__ sums) {
+    const uint8_t* g = grey + (size_t)blockIdx.y * width * height;
+    long long s = 0, s2 = 0;
+    const int inner_w = width - 2, inner = inner_w > 0 && height > 2 ? inner_w * (height - 2) : 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < inner; t += gridDim.x * blockDim.x) {
+        const int x = 1 + t % inner_w, y = 1 + t / inner_w;
+        const int i = y * width + x;
+        const int lap = (int)g[i - 1] + g[i + 1] + g[i - width] + g[i + width] - 4 * (int)g[i];
+        s += lap;
+        s2 += (long long)lap * lap;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(sums + 2 * blockIdx.y), (unsigned long long)s);
+        atomicAdd(reinterpret_cast<unsigned long long*>(sums + 2 * blockIdx.y + 1), (unsigned long long)s2);
+    }
+}
+
+void launch_grey(const uint8_t* rgb, size_t pixels, uint8_t* grey, cudaStream_t s) {
+    if (pixels) grey_kernel<<<(unsigned)((pixels + 255) / 256), 256, 0, s>>>(rgb, pixels, grey);
+}
+
+void launch_laplacian_sums(const uint8_t* grey, int count, int width, int height, long long* sums, cudaStream_t s) {
+    if (count <= 0) return;
+    const int inner = (width - 2) * (height - 2);
+    const int blocks = inner > 0 ? std::min(64, (inner + 255) / 256) : 1;
+    laplacian_sums_kernel<<<dim3(blocks, count), 256, 0, s>>>(grey, width, height, sums);
 }
 
 }  // namespace gs

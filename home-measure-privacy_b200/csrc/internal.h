@@ -233,6 +233,9 @@ void launch_neighbour_sizes(const NeighbourArgs& a, cudaStream_t s);
 void launch_init_planes(const float* xyz, const float* rgb, const float* sizes, float fixed_size, int count, int n_pad,
                         int planes, float* params, cudaStream_t s);
 
+void launch_grey(const uint8_t* rgb, size_t pixels, uint8_t* grey, cudaStream_t s);
+void launch_laplacian_sums(const uint8_t* grey, int count, int width, int height, long long* sums, cudaStream_t s);
+
 // ---- scene I/O -------------------------------------------------------------------------
 struct PlyHeaderInfo {
     int64_t header_bytes, count;

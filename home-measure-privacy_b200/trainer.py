@@ -249,6 +249,17 @@ class Renderer:
         N.check(self.lib.gs_init_from_points(self.ctx, N.ptr(xyz), N.ptr(rgb), n, float(size or 0.0)))
         return self.get_gaussians()
 
+    # ---- photo selection -----------------------------------------------------------------
+    def sharpness(self, images, width, height):
+        """sharpness (trainer/sharpness.js:15-31) of a batch of grey (n, h, w) or RGB
+        (n, h, w, 3) byte images of one size; returns float64 scores."""
+        imgs = np.ascontiguousarray(images, np.uint8)
+        channels = 3 if imgs.ndim == 4 else 1
+        count = imgs.shape[0]
+        out = np.zeros(max_(count, 1), np.float64)
+        N.check(self.lib.gs_sharpness(self.ctx, N.ptr(imgs), count, int(width), int(height), channels, N.ptr(out)))
+        return out[:count]
+
     # ---- scene files ---------------------------------------------------------------------
     def load_ply(self, data):
         """fromPly (trainer/gpu.js:983-999) into this context (f_rest bands up to its SH
@@ -462,10 +473,20 @@ class Renderer:
         N.check(self.lib.gs_stage_times_reset(self.ctx))
 
 
+def chooseSharp(scores, maxViews):
+    """chooseSharp (trainer/sharpness.js:39-55) through the C ABI."""
+    lib = N.load()
+    sc = np.ascontiguousarray(scores, np.float64)
+    out = np.zeros(max(len(sc), 1), np.int32)
+    m = ctypes.c_int32(0)
+    N.check(lib.gs_choose_sharp(N.ptr(sc), len(sc), int(maxViews), N.ptr(out), ctypes.byref(m)))
+    return [int(i) for i in out[:m.value]]
+
+
 def createRenderer(gpuTiles=True, **opts):
     """createRenderer({gpuTiles}) (trainer/gpu.js:704-712)."""
     return Renderer(gpuTiles=gpuTiles, **opts)
 
 
-__all__ = ["createRenderer", "Renderer", "adam_config", "sceneExtent", "shuffled", "unpackGaussians",
+__all__ = ["createRenderer", "Renderer", "adam_config", "chooseSharp", "sceneExtent", "shuffled", "unpackGaussians",
            "packed_from_records"]

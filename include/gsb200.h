@@ -269,6 +269,20 @@ GS_API int gs_neighbour_sizes(GsContext* ctx, const float* xyz, int32_t count, d
  * colour (rgb: count x 3 floats in [0, 1]); SH bands zero. */
 GS_API int gs_init_from_points(GsContext* ctx, const float* xyz, const float* rgb, int32_t count, float size);
 
+/* ---- Photo selection (trainer/sharpness.js, trainer/dataset.js:35-47) -------------------
+ * sharpness(grey, width, height): variance of the 4-neighbour Laplacian over the interior
+ * pixels, for `count` images of one size at once (channels = 1: grey bytes; 3: RGB bytes,
+ * turned grey as (77 R + 150 G + 29 B) >> 8).  The reference measures it on a 160-pixel-
+ * wide copy the browser scales; the caller passes the images at the size to score. */
+GS_API int gs_sharpness(GsContext* ctx, const uint8_t* images, int32_t count, int32_t width, int32_t height,
+                        int32_t channels, double* scores);
+
+/* chooseSharp(scores, maxViews) (trainer/sharpness.js:39-55): the sharpest photo of
+ * each of max_views stretches of the walk, without the blurriest (below 0.35 x the
+ * median, at most a quarter).  chosen: room for min(count, max_views) indices.  Host only. */
+GS_API int gs_choose_sharp(const double* scores, int32_t count, int32_t max_views, int32_t* chosen,
+                           int32_t* chosen_count);
+
 /* ---- Scene files ---------------------------------------------------------------------
  * fromPly (trainer/gpu.js:983-999): replaces the context's Gaussians with a binary
  * little-endian .ply of float vertex properties (x y z, scale_0..2, rot_0..3 w x y z,

@@ -301,3 +301,43 @@ def to_splat(rec):
         u += [js_byte(v / ln * 128 + 128) for v in q]
         out += f.tobytes() + bytes(u)
     return bytes(out)
+
+
+# ---- photo selection (trainer/sharpness.js) --------------------------------------------------
+def sharpness(grey, width, height):
+    """Variance of the 4-neighbour Laplacian over the interior (sharpness.js:15-31)."""
+    g = np.asarray(grey, np.int64).reshape(height, width)
+    if width < 3 or height < 3:
+        return 0.0
+    lap = g[1:-1, :-2] + g[1:-1, 2:] + g[:-2, 1:-1] + g[2:, 1:-1] - 4 * g[1:-1, 1:-1]
+    n = lap.size
+    s, s2 = int(lap.sum()), int((lap * lap).sum())
+    mean = s / n
+    return s2 / n - mean * mean
+
+
+def grey(rgb):
+    """(77 R + 150 G + 29 B) >> 8 (dataset.js:45)."""
+    c = np.asarray(rgb, np.int64)
+    return ((c[..., 0] * 77 + c[..., 1] * 150 + c[..., 2] * 29) >> 8).astype(np.uint8)
+
+
+def choose_sharp(scores, max_views):
+    """chooseSharp (sharpness.js:39-55), as written there."""
+    step = max(1.0, len(scores) / max_views)
+    chosen = []
+    start = 0.0
+    while start < len(scores):
+        frm = math.floor(start)
+        to = min(len(scores), math.floor(start + step))
+        best = frm
+        for i in range(frm + 1, to):
+            if scores[i] > scores[best]:
+                best = i
+        chosen.append(best)
+        start += step
+    srt = sorted(scores)
+    median = srt[(len(srt) - 1) // 2] if srt else 0
+    blurry = sorted([i for i in chosen if scores[i] < median * 0.35], key=lambda i: scores[i])
+    drop = set(blurry[:math.floor(len(chosen) * 0.25)])
+    return [i for i in chosen if i not in drop]

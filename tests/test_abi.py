@@ -93,3 +93,12 @@ def test_missing_library_raises(tmp_path, hmp):
             N.load(str(tmp_path / "libgsb200.so"))
     finally:
         N._lib = saved
+
+
+def test_choose_sharp_matches_restatement(hmp, oracle):
+    """chooseSharp through the C ABI (host only) against the restatement."""
+    rng = np.random.default_rng(4)
+    for count, views in [(1, 5), (7, 3), (50, 12), (301, 300), (1000, 77)]:
+        scores = rng.gamma(2.0, 50.0, count)
+        scores[rng.random(count) < 0.2] *= 0.1  # blurry ones
+        assert hmp.chooseSharp(scores, views) == oracle.choose_sharp(list(scores), views)

@@ -38,3 +38,26 @@ def test_init_from_points_matches_oracle(hmp, oracle, size):
     sizes = oracle.neighbour_sizes(xyz) if size is None else np.full(len(xyz), np.float32(size))
     np.testing.assert_array_equal(got, oracle.init_from_points(xyz, rgb, sizes, degree=1))
     assert np.isfinite(loss).all()
+
+
+def test_sharpness_matches_restatement(hmp, oracle):
+    """sharpness (trainer/sharpness.js:15-31) for a batch of photos, grey and RGB."""
+    rng = np.random.default_rng(12)
+    w, h = 160, 120
+    base = rng.integers(0, 256, (1, h, w, 3)).astype(np.uint8)
+    # progressively blurred copies: box-filtered, so their sharpness drops
+    imgs = [base[0]]
+    for k in range(1, 6):
+        im = imgs[-1].astype(np.float64)
+        im = (im + np.roll(im, 1, 0) + np.roll(im, 1, 1) + np.roll(im, (1, 1), (0, 1))) / 4
+        imgs.append(np.round(im).astype(np.uint8))
+    rgb = np.stack(imgs)
+    grey = oracle.grey(rgb)
+    with hmp.createRenderer(sh_degree=0) as r:
+        s_rgb = r.sharpness(rgb, w, h)
+        s_grey = r.sharpness(grey, w, h)
+    want = np.array([oracle.sharpness(g, w, h) for g in grey])
+    np.testing.assert_array_equal(s_grey, want)
+    np.testing.assert_array_equal(s_rgb, want)
+    assert np.all(np.diff(want) < 0)
+    assert hmp.chooseSharp(list(want), 2) == oracle.choose_sharp(list(want), 2)
