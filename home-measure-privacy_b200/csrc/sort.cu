@@ -147,13 +147,21 @@ __global__ void __launch_bounds__(RS_THREADS) radix_hist_all(const uint32_t* __r
     }
 }
 
-__global__ void __launch_bounds__(RS_THREADS, 3) radix_onesweep(
+// One partition of OS_THREADS x OS_ITEMS = RS_TILE keys per block: more, shorter
+// ranking chains (one per warp) than 256 threads x 16 items.
+constexpr int OS_THREADS = 512;
+constexpr int OS_ITEMS = RS_TILE / OS_THREADS;
+constexpr int OS_WARPS = OS_THREADS / 32;
+
+__global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ ghist,
     uint32_t* look, uint32_t* counter, unsigned int* timeout) {
     __shared__ uint32_t s_keys[RS_TILE];
     __shared__ uint32_t s_vals[RS_TILE];
-    __shared__ uint32_t s_warp[RS_WARPS][256];
+    // The warps' digit counts live in s_vals until the keys are placed.
+    static_assert(OS_WARPS * 256 <= RS_TILE, "warp rows must fit in s_vals");
+    uint32_t(*s_warp)[256] = reinterpret_cast<uint32_t(*)[256]>(s_vals);
     __shared__ uint32_t s_digit_start[256];
     __shared__ uint32_t s_global[256];
     __shared__ uint32_t s_tmp[32];
@@ -163,57 +171,62 @@ __global__ void __launch_bounds__(RS_THREADS, 3) radix_onesweep(
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     if (threadIdx.x == 0) s_part = atomicAdd(counter, 1u);
-    for (int d = threadIdx.x; d < RS_WARPS * 256; d += RS_THREADS) (&s_warp[0][0])[d] = 0u;
+    for (int d = threadIdx.x; d < OS_WARPS * 256; d += OS_THREADS) (&s_warp[0][0])[d] = 0u;
     __syncthreads();
     const uint32_t p = s_part;
     if (p >= P) return;
     const uint32_t part_start = p * RS_TILE;
-    const uint32_t warp_start = part_start + warp * (RS_ITEMS * 32);
-    uint32_t k[RS_ITEMS], pos[RS_ITEMS];
+    const uint32_t warp_start = part_start + warp * (OS_ITEMS * 32);
+    uint32_t k[OS_ITEMS], pos[OS_ITEMS], peers[OS_ITEMS];
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < OS_ITEMS; j++) {
         const uint32_t idx = warp_start + j * 32 + lane;
         k[j] = idx < n ? __ldg(keys_in + base + idx) : 0xffffffffu;
     }
-    // Rank within the warp: equal digits by ballot, counts in the warp's row.
+    // Equal digits by ballot for every item first (independent), then the running
+    // counts in the warp's row, item by item.
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
-        const uint32_t idx = warp_start + j * 32 + lane;
-        const bool valid = idx < n;
+    for (int j = 0; j < OS_ITEMS; j++) peers[j] = warp_peers((k[j] >> shift) & 0xffu, warp_start + j * 32 + lane < n);
+#pragma unroll
+    for (int j = 0; j < OS_ITEMS; j++) {
+        const bool valid = warp_start + j * 32 + lane < n;
         const uint32_t d = (k[j] >> shift) & 0xffu;
-        const uint32_t peers = warp_peers(d, valid);
         uint32_t prev = 0;
         if (valid) {
             prev = s_warp[warp][d];
-            pos[j] = prev + __popc(peers & lt_mask);
+            pos[j] = prev + __popc(peers[j] & lt_mask);
         }
         __syncwarp();
-        if (valid && (peers & lt_mask) == 0u) s_warp[warp][d] = prev + __popc(peers);
+        if (valid && (peers[j] & lt_mask) == 0u) s_warp[warp][d] = prev + __popc(peers[j]);
         __syncwarp();
     }
     __syncthreads();
-    const int d = threadIdx.x;  // RS_THREADS == 256 digits
+    // Threads 0..255 own one digit each.
+    const int d = threadIdx.x;
+    const bool owner = d < 256;
     uint32_t cnt = 0;
+    if (owner) {
 #pragma unroll
-    for (int w = 0; w < RS_WARPS; w++) {
-        const uint32_t c = s_warp[w][d];
-        s_warp[w][d] = cnt;
-        cnt += c;
+        for (int w = 0; w < OS_WARPS; w++) {
+            const uint32_t c = s_warp[w][d];
+            s_warp[w][d] = cnt;
+            cnt += c;
+        }
     }
     // Publish this partition's count as early as possible.
-    uint32_t* my = look + (size_t)p * 256 + d;
-    st_relaxed(my, (p == 0 ? OS_INC : OS_AGG) | cnt);
+    uint32_t* my = look + (size_t)p * 256 + (owner ? d : 0);
+    if (owner) st_relaxed(my, (p == 0 ? OS_INC : OS_AGG) | cnt);
     {
         uint32_t tot;
-        const uint32_t gex = block_excl_scan<RS_THREADS>(ghist[d], s_tmp, tot);
-        s_global[d] = gex;
-        const uint32_t lex = block_excl_scan<RS_THREADS>(cnt, s_tmp, tot);
-        s_digit_start[d] = lex;
+        const uint32_t gex = block_excl_scan<OS_THREADS>(owner ? ghist[d] : 0u, s_tmp, tot);
+        if (owner) s_global[d] = gex;
+        const uint32_t lex = block_excl_scan<OS_THREADS>(cnt, s_tmp, tot);
+        if (owner) s_digit_start[d] = lex;
     }
     __syncthreads();
     // Keys to their block-sorted slots.
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < OS_ITEMS; j++) {
         const uint32_t idx = warp_start + j * 32 + lane;
         if (idx < n) {
             const uint32_t dj = (k[j] >> shift) & 0xffu;
@@ -222,13 +235,13 @@ __global__ void __launch_bounds__(RS_THREADS, 3) radix_onesweep(
         }
     }
     // Values in flight while this thread looks back for digit d.
-    uint32_t v[RS_ITEMS];
+    uint32_t v[OS_ITEMS];
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < OS_ITEMS; j++) {
         const uint32_t idx = warp_start + j * 32 + lane;
         v[j] = (idx < n) ? (vals_in ? __ldg(vals_in + base + idx) : base + idx) : 0u;
     }
-    if (p > 0) {
+    if (p > 0 && owner) {
         // Walk back OS_LOOK partitions per round trip: sum published counts until an
         // inclusive prefix; re-poll from the first partition that has published nothing.
         uint32_t excl = 0;
@@ -268,14 +281,15 @@ __global__ void __launch_bounds__(RS_THREADS, 3) radix_onesweep(
         st_relaxed(my, OS_INC | (excl + cnt));
         s_global[d] += excl;
     }
+    __syncthreads();  // every warp has read its row of s_warp
 #pragma unroll
-    for (int j = 0; j < RS_ITEMS; j++) {
+    for (int j = 0; j < OS_ITEMS; j++) {
         const uint32_t idx = warp_start + j * 32 + lane;
         if (idx < n) s_vals[pos[j]] = v[j];
     }
     __syncthreads();
     const uint32_t total = min((uint32_t)RS_TILE, n - part_start);
-    for (uint32_t i = threadIdx.x; i < total; i += RS_THREADS) {
+    for (uint32_t i = threadIdx.x; i < total; i += OS_THREADS) {
         const uint32_t key = s_keys[i];
         const uint32_t dk = (key >> shift) & 0xffu;
         const uint32_t out = base + s_global[dk] + (i - s_digit_start[dk]);
@@ -298,7 +312,7 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
     for (int p = 0; p < passes; p++) {
         const int in = p & 1, out = in ^ 1;
         cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
-        radix_onesweep<<<grid, RS_THREADS, 0, s>>>(kb[in], (p == 0 && a.iota) ? nullptr : vb[in], kb[out], vb[out],
+        radix_onesweep<<<grid, OS_THREADS, 0, s>>>(kb[in], (p == 0 && a.iota) ? nullptr : vb[in], kb[out], vb[out],
                                                     a.seg, a.begin_bit + p * step, ghist + p * 256, a.hist,
                                                     counters + p, a.timeout);
     }
