@@ -355,7 +355,7 @@ static int set_scratch_camera(GsContext* c, const GsCamera& cam) {
 // Pair buffers for `views` view slots and the segment table.
 static int size_pairs(GsContext* c, int views) {
     const int64_t pairs = (int64_t)std::max(views, 1) * c->n_pad;
-    if (pairs > 0x3fffffffLL) return fail(GS_ERR_INVALID_ARG, "too many (view, Gaussian) pairs");
+    if (pairs > 0x7fffffffLL) return fail(GS_ERR_INVALID_ARG, "too many (view, Gaussian) pairs");
     if (pairs > c->pair_cap) {
         CKI(ensure(c->geo0, (size_t)pairs * 16, c));
         CKI(ensure(c->geo1, (size_t)pairs * 16, c));
@@ -372,7 +372,7 @@ static int size_pairs(GsContext* c, int views) {
         CKI(ensure(c->pair_offsets, (size_t)pairs * 4, c));
         c->pair_cap = pairs;
         const int64_t parts = (std::max(pairs, c->inst_cap) + radix_tile_items() - 1) / radix_tile_items() + 1;
-        CKI(ensure(c->hist, (size_t)parts * 256 * 4, c));
+        CKI(ensure(c->hist, (size_t)parts * 256 * 8, c));
         // Zeroed once; every backward re-zeroes the slots it uses.
         CK(cudaMemsetAsync(c->sg8.p, 0, c->sg8.bytes, c->stream));
         CK(cudaMemsetAsync(c->sg1.p, 0, c->sg1.bytes, c->stream));
@@ -392,7 +392,7 @@ static int write_segments(GsContext* c) {
 }
 
 static int size_instances(GsContext* c, int64_t cap) {
-    if (cap > 0x3ffff000LL) cap = 0x3ffff000LL;  // the sort's look-back counts hold 30 bits
+    if (cap > 0xfffff000LL) cap = 0xfffff000LL;  // instance positions are 32-bit
     if (cap <= c->inst_cap) return GS_OK;
     CKI(ensure(c->ikeys, (size_t)cap * 4, c));
     CKI(ensure(c->ivals, (size_t)cap * 4, c));
@@ -401,7 +401,7 @@ static int size_instances(GsContext* c, int64_t cap) {
     CKI(ensure(c->block_first_pair, (size_t)(cap / emit_out_items() + 2) * 4, c));
     c->inst_cap = cap;
     const int64_t parts = (std::max(c->pair_cap, c->inst_cap) + radix_tile_items() - 1) / radix_tile_items() + 1;
-    CKI(ensure(c->hist, (size_t)parts * 256 * 4, c));
+    CKI(ensure(c->hist, (size_t)parts * 256 * 8, c));
     return GS_OK;
 }
 
@@ -504,7 +504,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ra.seg = pair_seg;
     ra.begin_bit = 0;
     ra.end_bit = 31;
-    ra.hist = c->hist.as<uint32_t>();
+    ra.hist = c->hist.as<unsigned long long>();
     ra.totals = c->totals.as<uint32_t>();
     ra.timeout = &c->status.as<DevStatus>()->sort_timeout;
     ra.max_parts = (int)(((int64_t)vcount * c->n_pad + radix_tile_items() - 1) / radix_tile_items());

@@ -88,7 +88,7 @@ struct RadixSortArgs {
     int iota;                // 1: values start as the absolute element index
     const SegInfo* seg;
     int begin_bit, end_bit;  // bits to sort
-    uint32_t* hist;          // look-back words, 256 * max_parts
+    unsigned long long* hist;  // look-back words, 256 * max_parts
     uint32_t* totals;        // digit counts of every pass and partition counters (>= 1028 words)
     int max_parts;
     unsigned int* timeout;   // set when a look-back wait gave up

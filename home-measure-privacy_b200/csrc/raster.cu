@@ -148,7 +148,9 @@ __device__ __forceinline__ float alpha_band(const float4& g0, const float4& g1, 
                                                              __fmul_rn(__fmul_rn(g1.x, dy), dy))),
                                   __fmul_rn(__fmul_rn(g0.w, dx), dy));
     if (power > 0.f) return 0.f;
-    const float alpha = __fmul_rn(g1.y, expf(power));
+    // The specified exp (gs_common.cuh), as the CPU restatement uses: the two agree
+    // bit for bit even when alpha lies within an ulp of alpha_min.
+    const float alpha = __fmul_rn(g1.y, spec_expf(power));
     return alpha < amin ? 0.f : fminf(amax, alpha);
 }
 

@@ -90,20 +90,34 @@ __device__ __forceinline__ uint32_t warp_peers(uint32_t d, bool valid) {
 // (decoupled look-back) and scatters keys and values.  Keys and values are read once
 // and written once per pass.
 //
-// Look-back words: bits 31..30 = 0 (not yet published), 1 (this partition's count),
-// 2 (inclusive prefix over partitions 0..p); bits 29..0 = the count.  A block waits only
+// Look-back words: top two bits = 0 (not yet published), 1 (this partition's count),
+// 2 (inclusive prefix over partitions 0..p); the bits below = the count.  A block waits only
 // on earlier partitions, which took their index earlier and wait only on theirs, so the
 // waits end; each wait is still bounded (OS_SPIN_LIMIT polls), after which the block
 // sets the timeout flag and goes on with a wrong offset instead of hanging.
 // ---------------------------------------------------------------------------------
-constexpr uint32_t OS_AGG = 1u << 30;
-constexpr uint32_t OS_INC = 2u << 30;
-constexpr uint32_t OS_VALUE = OS_AGG - 1u;
+// Look-back word of W bits: flags in the top two bits, the count below.  32-bit words
+// serve segments below 2^30 keys (half the memset and look-back traffic), 64-bit ones
+// the rest.
+template <typename W>
+struct LookWord {
+    static constexpr W AGG = (W)1 << (sizeof(W) * 8 - 2);
+    static constexpr W INC = (W)2 << (sizeof(W) * 8 - 2);
+    static constexpr W VALUE = AGG - 1;
+};
 constexpr int OS_SPIN_LIMIT = 1 << 22;
 constexpr int OS_LOOK = 8;  // look-back words read per round trip
 constexpr int OS_MAX_PASSES = 4;
 constexpr int OS_HIST_BLOCKS = 1184;  // 148 SMs x 8
 
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -153,10 +167,12 @@ constexpr int OS_THREADS = 512;
 constexpr int OS_ITEMS = RS_TILE / OS_THREADS;
 constexpr int OS_WARPS = OS_THREADS / 32;
 
+template <typename W>
 __global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ ghist,
-    uint32_t* look, uint32_t* counter, unsigned int* timeout) {
+    W* look, uint32_t* counter, unsigned int* timeout) {
+    using LW = LookWord<W>;
     __shared__ uint32_t s_keys[RS_TILE];
     __shared__ uint32_t s_vals[RS_TILE];
     // The warps' digit counts live in s_vals until the keys are placed.
@@ -214,8 +230,8 @@ __global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
         }
     }
     // Publish this partition's count as early as possible.
-    uint32_t* my = look + (size_t)p * 256 + (owner ? d : 0);
-    if (owner) st_relaxed(my, (p == 0 ? OS_INC : OS_AGG) | cnt);
+    W* my = look + (size_t)p * 256 + (owner ? d : 0);
+    if (owner) st_relaxed(my, (W)((p == 0 ? LW::INC : LW::AGG) | (W)cnt));
     {
         uint32_t tot;
         const uint32_t gex = block_excl_scan<OS_THREADS>(owner ? ghist[d] : 0u, s_tmp, tot);
@@ -249,22 +265,22 @@ __global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
         int spins = 0;
         bool done = false;
         while (!done) {
-            uint32_t w[OS_LOOK];
+            W w[OS_LOOK];
 #pragma unroll
-            for (int t = 0; t < OS_LOOK; t++) w[t] = q - t >= 0 ? ld_relaxed(look + (size_t)(q - t) * 256 + d) : OS_INC;
+            for (int t = 0; t < OS_LOOK; t++) w[t] = q - t >= 0 ? ld_relaxed(look + (size_t)(q - t) * 256 + d) : LW::INC;
             int used = 0;
             bool stop = false;
 #pragma unroll
             for (int t = 0; t < OS_LOOK; t++) {
                 if (stop) continue;
-                const uint32_t flag = w[t] & ~OS_VALUE;
-                if (flag == 0u) {
+                const W flag = w[t] & ~LW::VALUE;
+                if (flag == 0) {
                     stop = true;
                     continue;
                 }
-                excl += w[t] & OS_VALUE;
+                excl += (uint32_t)(w[t] & LW::VALUE);
                 used++;
-                if (flag == OS_INC) {
+                if (flag == LW::INC) {
                     stop = true;
                     done = true;
                 }
@@ -278,7 +294,7 @@ __global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
                 __nanosleep(32);
             }
         }
-        st_relaxed(my, OS_INC | (excl + cnt));
+        st_relaxed(my, (W)(LW::INC | (W)(excl + cnt)));
         s_global[d] += excl;
     }
     __syncthreads();  // every warp has read its row of s_warp
@@ -309,12 +325,23 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
     radix_hist_all<<<min(grid, OS_HIST_BLOCKS), RS_THREADS, 0, s>>>(a.keys, a.seg, a.begin_bit, passes, ghist);
     uint32_t* kb[2] = {a.keys, a.keys_alt};
     uint32_t* vb[2] = {a.vals, a.vals_alt};
+    // The largest key count this buffer can hold decides the look-back word width.
+    const bool wide = (long long)grid * RS_TILE >= (1ll << 30);
     for (int p = 0; p < passes; p++) {
         const int in = p & 1, out = in ^ 1;
-        cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
-        radix_onesweep<<<grid, OS_THREADS, 0, s>>>(kb[in], (p == 0 && a.iota) ? nullptr : vb[in], kb[out], vb[out],
-                                                    a.seg, a.begin_bit + p * step, ghist + p * 256, a.hist,
-                                                    counters + p, a.timeout);
+        const uint32_t* vin = (p == 0 && a.iota) ? nullptr : vb[in];
+        if (wide) {
+            cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(unsigned long long), s);
+            radix_onesweep<unsigned long long><<<grid, OS_THREADS, 0, s>>>(
+                kb[in], vin, kb[out], vb[out], a.seg, a.begin_bit + p * step, ghist + p * 256,
+                reinterpret_cast<unsigned long long*>(a.hist), counters + p, a.timeout);
+        } else {
+            cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
+            radix_onesweep<uint32_t><<<grid, OS_THREADS, 0, s>>>(kb[in], vin, kb[out], vb[out], a.seg,
+                                                                  a.begin_bit + p * step, ghist + p * 256,
+                                                                  reinterpret_cast<uint32_t*>(a.hist), counters + p,
+                                                                  a.timeout);
+        }
     }
 }
 

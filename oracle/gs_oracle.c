@@ -325,14 +325,17 @@ EXPORT int64_t orc32_bin(const float* splats, int n, int W, int H, int rect_mode
     return total;
 }
 
-/* alphaAt (trainer/gpu.js:91-103).  Returns alpha, or 0 when the splat is skipped. */
+/* alphaAt (trainer/gpu.js:91-103).  Returns alpha, or 0 when the splat is skipped.
+ * WGSL leaves exp's last bits to the implementation (a few ulp); this restatement uses
+ * the specified exp (spec_expf) that the CUDA path also uses wherever alpha decides a
+ * skip, so that the two agree even when alpha is within an ulp of 1/255. */
 static inline float alpha_at(const float* s, float px, float py, float amax, float amin, float* dxo, float* dyo) {
     const float dx = px - s[0], dy = py - s[1];
     const float r = s[6];
     if (fabsf(dx) > r || fabsf(dy) > r) return 0.0f;
     const float power = -0.5f * (s[2] * dx * dx + s[4] * dy * dy) - s[3] * dx * dy;
     if (power > 0.0f) return 0.0f;
-    float alpha = s[5] * expf(power);
+    float alpha = s[5] * spec_expf(power);
     if (alpha > amax) alpha = amax;
     if (alpha < amin) return 0.0f;
     *dxo = dx;
