@@ -488,7 +488,8 @@ def main():
             line = dict(metric=METRIC, value=cb["value"], unit="steps/s", n_gpus=args.gpus, steps=cb["samples"],
                         warmup=args.warmup, ms_per_step=1000.0 / cb["value"], higher_is_better=True, scaling="weak",
                         vs_baseline=None, dtype="f32", data="synthetic", impl="reference",
-                        config=dict(workload=WORKLOAD, gaussians=1_000_000, views=8, sh_degree=3),
+                        config=dict(workload=WORKLOAD, gaussians=1_000_000, views=8, pixels=9157632, sh_degree=3,
+                                    near=0.01, ssim_lambda=0.2, window="11-tap gaussian"),
                         cpu_baseline=cb,
                         e2e=dict(value=cb["value"], unit="steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
             print(json.dumps(line), flush=True)
