@@ -360,7 +360,7 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
 constexpr int EM_THREADS = 256;
 constexpr int EM_ITEMS = 8;
 constexpr int EM_CHUNK = EM_THREADS * EM_ITEMS;
-constexpr int EM_OUT = 2048;
+constexpr int EM_OUT = 1024;
 
 int emit_chunk_items() { return EM_CHUNK; }
 int emit_out_items() { return EM_OUT; }
@@ -485,7 +485,10 @@ __device__ __forceinline__ uint32_t block_incl_max(uint32_t v, uint32_t* s_tmp) 
     return max(prefix, x);
 }
 
-constexpr size_t EM_EXPAND_SMEM = (size_t)(EM_OUT + 1) * (4 + 4 + 8 + 16) + (size_t)EM_OUT * 4;
+// s_head is padded by one word per 32 (HP): each thread walks PER consecutive entries,
+// and without the padding threads t and t + 32 / PER would hit the same bank.
+__device__ __forceinline__ uint32_t HP(uint32_t i) { return i + (i >> 5); }
+constexpr size_t EM_EXPAND_SMEM = (size_t)(EM_OUT + 1) * (4 + 4 + 8 + 16) + (size_t)(EM_OUT + EM_OUT / 32) * 4;
 
 __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
     constexpr int PER = EM_OUT / EM_THREADS;  // instances per thread
@@ -510,7 +513,7 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
         // needs at most EM_OUT + 1 pairs (the bound matters for the last block when the
         // capacity clamped the instance count).
         const uint32_t np = min(p_hi - p_lo + 1, (uint32_t)EM_OUT + 1);
-        for (uint32_t j = threadIdx.x; j < EM_OUT; j += EM_THREADS) s_head[j] = 0u;
+        for (uint32_t j = threadIdx.x; j < EM_OUT + EM_OUT / 32; j += EM_THREADS) s_head[j] = 0u;
         for (uint32_t j = threadIdx.x; j < np; j += EM_THREADS) {
             const uint32_t pair = __ldg(a.sorted_pairs + base + p_lo + j);
             const uint4* er = reinterpret_cast<const uint4*>(a.erec + pair);
@@ -525,13 +528,13 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
         // a running max then gives every instance its pair.
         for (uint32_t j = 1 + threadIdx.x; j < np; j += EM_THREADS) {
             const uint32_t pos = s_off[j] - o0;
-            if (pos < (uint32_t)EM_OUT) s_head[pos] = j;
+            if (pos < (uint32_t)EM_OUT) s_head[HP(pos)] = j;
         }
         __syncthreads();
         uint32_t run = 0, loc[PER];
 #pragma unroll
         for (int k = 0; k < PER; k++) {
-            run = max(run, s_head[threadIdx.x * PER + k]);
+            run = max(run, s_head[HP(threadIdx.x * PER + k)]);
             loc[k] = run;
         }
         const uint32_t prefix = block_incl_max<EM_THREADS>(run, s_tmp);
@@ -575,15 +578,15 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
                     t -= len;
                 }
             }
-            s_head[ol] = tile;
+            s_head[HP(ol)] = tile;
         }
         __syncthreads();
-        for (uint32_t ol = threadIdx.x; ol < o1 - o0; ol += EM_THREADS) a.inst_keys[inst_base + o0 + ol] = s_head[ol];
+        for (uint32_t ol = threadIdx.x; ol < o1 - o0; ol += EM_THREADS) a.inst_keys[inst_base + o0 + ol] = s_head[HP(ol)];
         __syncthreads();
 #pragma unroll
-        for (int k = 0; k < PER; k++) s_head[threadIdx.x * PER + k] = s_pair[jj[k]];
+        for (int k = 0; k < PER; k++) s_head[HP(threadIdx.x * PER + k)] = s_pair[jj[k]];
         __syncthreads();
-        for (uint32_t ol = threadIdx.x; ol < o1 - o0; ol += EM_THREADS) a.inst_vals[inst_base + o0 + ol] = s_head[ol];
+        for (uint32_t ol = threadIdx.x; ol < o1 - o0; ol += EM_THREADS) a.inst_vals[inst_base + o0 + ol] = s_head[HP(ol)];
         __syncthreads();
     }
 }
