@@ -105,3 +105,26 @@ def test_blend_count_matches_state(hmp, oracle):
     ref = oracle.render_ref(cam, rec, 0, near=0.2)
     ref_blends = int(ref["state"][1::2].astype(np.int64).sum())
     assert abs(blends - ref_blends) <= 1e-3 * ref_blends
+
+
+def test_split_step_reduces_densify_stats(hmp):
+    """With statistics on, the step-local statistics travel in the reduced buffer: both
+    replicas end with the statistics of all views, equal to one context's."""
+    rec, cams, imgs = scene(hmp)
+    with hmp.createRenderer(sh_degree=1) as whole:
+        load(whole, rec, cams, imgs)
+        whole.set_densify_stats(True)
+        whole.train_step(ssim=0.2, window=1)
+        ref_sums, ref_counts = whole.densify_stats()
+    with hmp.createRenderer(sh_degree=1) as a, hmp.createRenderer(sh_degree=1) as b:
+        load(a, rec, cams, imgs)
+        load(b, rec, cams, imgs)
+        a.set_densify_stats(True)
+        b.set_densify_stats(True)
+        reduce_and_apply([a, b], [(0, 2), (2, 2)])
+        sa, ca = a.densify_stats()
+        sb, cb = b.densify_stats()
+    np.testing.assert_array_equal(sa, sb)
+    np.testing.assert_array_equal(ca, cb)
+    np.testing.assert_array_equal(ca, ref_counts)
+    np.testing.assert_allclose(sa, ref_sums, rtol=1e-4, atol=1e-10)
