@@ -189,7 +189,7 @@ void launch_project_fwd(const ProjectArgs& a, cudaStream_t s) {
 // Backward.
 // ---------------------------------------------------------------------------------
 template <int DEG>
-__global__ void __launch_bounds__(128) project_bwd_kernel(ProjectBwdArgs a) {
+__global__ void __launch_bounds__(128, 4) project_bwd_kernel(ProjectBwdArgs a) {
     constexpr int NK = (DEG + 1) * (DEG + 1) - 1;
     constexpr int P = 14 + 3 * NK;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
