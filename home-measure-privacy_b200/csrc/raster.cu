@@ -308,7 +308,7 @@ __device__ __forceinline__ float warp_sum8_transposed(float v[8]) {
 }
 
 template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT, 4 * PPT) raster_bwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(256 / PPT, PPT == 2 ? 7 : 4) raster_bwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
