@@ -168,8 +168,8 @@ def run_b200(args, rank, local, world, dist):
     ad = hmp.adam_config()
     res = {}
 
-    def setup(batched):
-        r = hmp.createRenderer(sh_degree=c["degree"], near=c["near"], batched=batched, use_graph=True,
+    def setup(batched, use_graph=True):
+        r = hmp.createRenderer(sh_degree=c["degree"], near=c["near"], batched=batched, use_graph=use_graph,
                                device=device)
         r.set_gaussians(c["records"])
         r.set_views(cams)
@@ -267,6 +267,11 @@ def run_b200(args, rank, local, world, dist):
         plain = 1000.0 / (t_p / max(3, args.steps // 2))
         res["plain_stages"] = rp.stage_times()
         rp.close()
+        # the same plain path launched directly (no graph), as a per-view trainer would
+        rd = setup(False, use_graph=False)
+        t_d = timed(rd, max(3, args.steps // 4), 2)
+        res["plain_direct"] = 1000.0 / (t_d / max(3, args.steps // 4))
+        rd.close()
     res.update(ms_step=ms_step, plain=plain, e2e=e2e, tuned=tuned, n=n, V=V, pixels=pixels)
     res["bytes"] = algorithmic_bytes(st, n, hmp.stride(c["degree"]), V, pixels, int(st["tiles"]))
     return res
@@ -514,6 +519,7 @@ def main():
                         parallelism=(f"dp{world}: 8 own views per GPU, gradients summed by one NCCL all-reduce "
                                      f"per step" if dist else "dp1: one GPU, 8 views")),
             plain_steps_per_s=round(res["plain"], 4) if res["plain"] else None,
+            plain_direct_steps_per_s=round(res["plain_direct"], 4) if res.get("plain_direct") else None,
             batched_over_plain=round(value / world / res["plain"], 4) if res["plain"] else None,
             instances_per_step=int(res["stats"]["instances"]),
             stages_ms_per_step={k: round(v / steps, 4) for k, v in res["stages"]["ms"].items()},
