@@ -141,6 +141,13 @@ struct GsContext {
     DevBuf status;
     DevStatus* status_host = nullptr;
     cudaEvent_t status_event = nullptr;
+    // gs_train_step_host_async: a copy stream, two staging buffers for the step's photos,
+    // and per slot the events "photos copied", "staging buffer free", "step done".
+    cudaStream_t copy_stream = nullptr;
+    DevBuf stage[2];
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr};
+    bool pipe_pending[2] = {false, false};
+    int pipe_slot = 0;
     bool status_pending = false;
     int64_t skipped_steps = 0;
     // last forward
@@ -980,7 +987,8 @@ int gs_destroy(GsContext* c) {
                       &c->rgb, &c->erec, &c->pcount, &c->pkeys, &c->pvals, &c->pkeys_alt, &c->pvals_alt, &c->sg8, &c->sg1,
                       &c->ikeys, &c->ivals, &c->ikeys_alt, &c->ivals_alt, &c->hist, &c->totals, &c->block_sums,
                       &c->pair_offsets, &c->block_first_pair,
-                      &c->segs, &c->visible, &c->acc, &c->scratch16, &c->status};
+                      &c->segs, &c->visible, &c->acc, &c->scratch16, &c->status, &c->stats, &c->dn_scratch,
+                      &c->nb_scratch, &c->stage[0], &c->stage[1]};
     for (DevBuf* b : bufs) release(*b);
     for (cudaEvent_t e : c->capture_events) cudaEventDestroy(e);
     for (auto& sl : c->slots)
@@ -988,6 +996,15 @@ int gs_destroy(GsContext* c) {
     for (int k = 0; k < 64; k++)
         if (c->user_events[k]) cudaEventDestroy(c->user_events[k]);
     if (c->status_event) cudaEventDestroy(c->status_event);
+    for (int k = 0; k < 2; k++) {
+        if (c->ev_copied[k]) cudaEventDestroy(c->ev_copied[k]);
+        if (c->ev_free[k]) cudaEventDestroy(c->ev_free[k]);
+        if (c->ev_done[k]) cudaEventDestroy(c->ev_done[k]);
+    }
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
     if (c->status_host) cudaFreeHost(c->status_host);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1472,6 +1489,31 @@ static int poll_status(GsContext* c, bool wait) {
     return GS_OK;
 }
 
+// The whole step on the context's stream: its graph (captured on first use) or the direct
+// launches.
+static int launch_step(GsContext* c, const GsAdamConfig& ad, const GsLossConfig& lc, int first, int count,
+                       bool batched, int kind) {
+    if (c->cfg.use_graph) {
+        GraphKey key;
+        memset(&key, 0, sizeof key);
+        key.first = first;
+        key.count = count;
+        key.batched = batched;
+        key.window = lc.window;
+        key.kind = kind;
+        memcpy(&key.loss_lambda_bits, &lc.ssim_lambda, 4);
+        key.adam = ad;
+        StepGraph& g = c->graphs[key];
+        if (!g.exec || g.generation != c->generation) CKI(capture_step(c, g, ad, lc, first, count, batched, kind));
+        CKI(launch_graph(c, g));
+    } else {
+        CKI(begin_record(c));
+        CKI(enqueue_step(c, ad, lc, first, count, batched, kind));
+        CKI(end_record(c));
+    }
+    return GS_OK;
+}
+
 static int train_step_impl(GsContext* c, const GsAdamConfig* ad, const GsLossConfig* lc, int first, int count,
                            const uint8_t* host_targets, float* loss_out) {
     CTX_CHECK(c);
@@ -1496,24 +1538,7 @@ static int train_step_impl(GsContext* c, const GsAdamConfig* ad, const GsLossCon
             CK(cudaMemcpyAsync(c->target_u8.as<uint8_t>() + (size_t)a.pixel_offset * 3, host_targets, px * 3,
                                cudaMemcpyHostToDevice, c->stream));
         }
-        if (c->cfg.use_graph) {
-            GraphKey key;
-            memset(&key, 0, sizeof key);
-            key.first = first;
-            key.count = count;
-            key.batched = batched;
-            key.window = lc->window;
-            key.kind = kind;
-            memcpy(&key.loss_lambda_bits, &lc->ssim_lambda, 4);
-            key.adam = *ad;
-            StepGraph& g = c->graphs[key];
-            if (!g.exec || g.generation != c->generation) CKI(capture_step(c, g, *ad, *lc, first, count, batched, kind));
-            CKI(launch_graph(c, g));
-        } else {
-            CKI(begin_record(c));
-            CKI(enqueue_step(c, *ad, *lc, first, count, batched, kind));
-            CKI(end_record(c));
-        }
+        CKI(launch_step(c, *ad, *lc, first, count, batched, kind));
         CK(cudaMemcpyAsync(c->status_host, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaEventRecord(c->status_event, c->stream));
         c->status_pending = true;
@@ -1616,6 +1641,66 @@ int gs_get_stream(GsContext* c, void** stream_out) {
     CTX_CHECK(c);
     if (!stream_out) return fail(GS_ERR_INVALID_ARG, "stream_out is null");
     *stream_out = (void*)c->stream;
+    return GS_OK;
+}
+
+int gs_train_step_host_async(GsContext* c, const GsAdamConfig* ad, const GsLossConfig* lc, int32_t first,
+                             int32_t count, const uint8_t* targets_u8, float* loss_out) {
+    CTX_CHECK(c);
+    CKI(check_adam(ad));
+    CKI(check_loss(lc));
+    CKI(check_range(c, first, count, false));
+    if (!targets_u8 || !loss_out) return fail(GS_ERR_INVALID_ARG, "null targets or loss buffer");
+    if (!c->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; k++) {
+            CK(cudaEventCreateWithFlags(&c->ev_copied[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->ev_free[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->ev_done[k], cudaEventDisableTiming));
+        }
+    }
+    const int slot = c->pipe_slot;
+    // At most two steps in flight: the one queued two calls ago must be done before its
+    // staging buffer and loss slot are reused (its loss is then in the caller's buffer).
+    if (c->pipe_pending[slot]) {
+        CK(cudaEventSynchronize(c->ev_done[slot]));
+        c->pipe_pending[slot] = false;
+    }
+    CKI(ensure(c->target_u8, (size_t)c->total_pixels * 3, c));
+    for (int v = first; v < first + count; v++) c->target_kind[v] = 1;
+    int kind;
+    CKI(targets_kind(c, first, count, &kind));
+    CKI(size_pairs(c, count));
+    CKI(poll_status(c, false));
+    CKI(ensure_capacity(c, first, count));
+    const ViewDesc& va = c->vdesc[first];
+    const ViewDesc& vb = c->vdesc[first + count - 1];
+    const size_t bytes = (size_t)(vb.pixel_offset + (int64_t)vb.width * vb.height - va.pixel_offset) * 3;
+    if (c->stage[slot].bytes < bytes) {
+        CK(cudaStreamSynchronize(c->copy_stream));  // the other slot's copy may still read nothing of this one
+        CKI(ensure(c->stage[slot], bytes, c));
+    }
+    // Photos: host -> staging buffer on the copy stream (overlapping the step before),
+    // then staging -> target buffer on the compute stream, right before the step.
+    CK(cudaStreamWaitEvent(c->copy_stream, c->ev_free[slot], 0));
+    CK(cudaMemcpyAsync(c->stage[slot].p, targets_u8, bytes, cudaMemcpyHostToDevice, c->copy_stream));
+    CK(cudaEventRecord(c->ev_copied[slot], c->copy_stream));
+    CK(cudaStreamWaitEvent(c->stream, c->ev_copied[slot], 0));
+    CK(cudaMemcpyAsync(c->target_u8.as<uint8_t>() + (size_t)va.pixel_offset * 3, c->stage[slot].p, bytes,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaEventRecord(c->ev_free[slot], c->stream));
+    CKI(launch_step(c, *ad, *lc, first, count, c->cfg.batched != 0, kind));
+    CK(cudaMemcpyAsync(loss_out, &c->status.as<DevStatus>()->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->status_host, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->status_event, c->stream));
+    CK(cudaEventRecord(c->ev_done[slot], c->stream));
+    c->status_pending = true;
+    c->pipe_pending[slot] = true;
+    c->pipe_slot = slot ^ 1;
+    c->last_first = first;
+    c->last_count = count;
+    c->last_batched = c->cfg.batched != 0;
+    c->have_loss = true;
     return GS_OK;
 }
 

@@ -435,6 +435,15 @@ class Renderer:
         N.check(self.lib.gs_step_apply(self.ctx, ctypes.byref(ad), ctypes.byref(v), ctypes.byref(sk)))
         return v.value, bool(sk.value)
 
+    def train_step_async(self, host_targets, loss_ptr, adam=None, ssim=0.2, window=1, first=0, count=None):
+        """gs_train_step_host_async: queue a step whose photos come from host memory
+        (a pointer, ideally pinned) and whose loss lands at loss_ptr (pinned) when done."""
+        count = len(self._views) - first if count is None else count
+        ad = adam if adam is not None else adam_config()
+        lc = N.GsLossConfig(float(ssim), int(window))
+        N.check(self.lib.gs_train_step_host_async(self.ctx, ctypes.byref(ad), ctypes.byref(lc), first, count,
+                                                  host_targets, loss_ptr))
+
     def stats(self):
         s = N.GsStats()
         N.check(self.lib.gs_get_stats(self.ctx, ctypes.byref(s)))

@@ -221,6 +221,19 @@ GS_API int gs_train_step_host(GsContext* ctx, const GsAdamConfig* adam, const Gs
                        int32_t first_view, int32_t num_views, const uint8_t* targets_u8,
                        float* loss_out);
 
+/* gs_train_step_host, pipelined: the step's photos go host -> device on a separate copy
+ * stream while the previous step still runs, and the loss comes back by an asynchronous
+ * copy into loss_out when the step completes; the call returns once the step is queued.
+ * At most two steps are in flight: a call first waits for the step queued two calls
+ * earlier, so after call k returns the loss of step k - 2 is in its buffer and that
+ * step's targets_u8 may be reused.  targets_u8 and loss_out should be pinned
+ * (gs_host_alloc) for the copies to overlap.  A step whose key instances overflow skips
+ * its update; the buffers grow before the next step (no redo).  gs_synchronize waits for
+ * all. */
+GS_API int gs_train_step_host_async(GsContext* ctx, const GsAdamConfig* adam, const GsLossConfig* loss,
+                                    int32_t first_view, int32_t num_views, const uint8_t* targets_u8,
+                                    float* loss_out);
+
 /* train() (trainer/gpu.js:846-878): `steps` steps of L1 loss, one view per step in
  * order, through the plain per-pixel path; losses_out[steps] gets each step's mean
  * L1 (the reference reads the image back every step). */

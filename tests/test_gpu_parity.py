@@ -373,3 +373,40 @@ def test_capacity_overflow_skips_update_grows_and_redoes(hmp):
     assert ref[1000][2] >= 1 and ref[0][2] == 0
     assert abs(ref[0][0] - ref[1000][0]) < 1e-6 * max(1.0, abs(ref[0][0]))
     assert np.abs(ref[0][1] - ref[1000][1]).max() < 1e-5
+
+
+def test_pipelined_host_step_matches_synchronous(hmp):
+    """gs_train_step_host_async (photos on a copy stream, loss copied back when done)
+    trains like gs_train_step_host."""
+    import ctypes
+    rec = hmp.synthetic_scene(20_000, 1, 8, "normal", (-4.0, 0.6), (0.0, 1.5))
+    cams = hmp.ring_cameras([(256, 192), (320, 200)], 4.0)
+    tg = hmp.synthetic_scene(20_000, 1, 9, "normal", (-4.0, 0.6), (0.0, 1.5))
+    with make(hmp, 1) as t:
+        t.set_gaussians(tg)
+        t.set_views(cams)
+        photos = np.round(np.clip(t.forward(0, 2), 0, 1) * 255).astype(np.uint8)
+    res = {}
+    for mode in ("sync", "async"):
+        with make(hmp, 1) as r:
+            r.set_gaussians(rec)
+            r.set_views(cams)
+            lib = r.lib
+            host = ctypes.c_void_p()
+            assert lib.gs_host_alloc(photos.nbytes, ctypes.byref(host)) == 0
+            ctypes.memmove(host.value, photos.ctypes.data, photos.nbytes)
+            losses = ctypes.c_void_p()
+            assert lib.gs_host_alloc(4 * 8, ctypes.byref(losses)) == 0
+            if mode == "sync":
+                got = [r.train_step(ssim=0.2, window=1, host_targets=host) for _ in range(4)]
+            else:
+                for k in range(4):
+                    r.train_step_async(host, losses.value + 4 * k, ssim=0.2, window=1)
+                r.synchronize()
+                got = list(np.ctypeslib.as_array(ctypes.cast(losses.value, ctypes.POINTER(ctypes.c_float)), (4,)))
+            res[mode] = (np.array(got), r.get_gaussians(), r.step_count())
+            lib.gs_host_free(losses)
+            lib.gs_host_free(host)
+    np.testing.assert_allclose(res["async"][0], res["sync"][0], rtol=1e-5)
+    assert res["async"][2] == res["sync"][2] == 4
+    assert np.abs(res["async"][1] - res["sync"][1]).max() < 1e-4
