@@ -5,16 +5,20 @@
 // and channel, SSIM and its partials a, b, d by the window mean, mean of squares and
 // mean of products) and LOSS_GRAD (:374-409: each pixel sums a + 2 x b + y d over the
 // windows that cover it, 49 taps each, reading the coefficients back from HBM).  Here
-// one CTA owns a 32 x 32 block of output pixels and keeps everything in shared memory:
-// it loads image and target with a 2R halo, forms the five window moments with a
-// separable (horizontal then vertical) filter, turns them into the coefficients
-// a, b, d at every window centre that can reach the block, and filters those
-// coefficients back (again separably) to get each pixel's SSIM gradient.  Every pass
-// gives each thread a short strip of outputs computed from a register window, so one
-// shared-memory load feeds up to 2R + 1 filter taps.  Windows are
-// the reference's: centres whose whole window lies inside the image (7x7 box, R = 3),
-// or the 11-tap Gaussian (sigma 1.5, R = 5) with the same rule.  The kernel also sums
-// |x - y| and the SSIM of the windows centred in its block for the loss value.
+// one CTA owns one colour channel of a 32 x 32 block of output pixels (the three
+// channel CTAs of a block are neighbours in the grid, so they share the interleaved
+// RGB lines in L2) and keeps everything in shared memory: it loads image and target
+// with a 2R halo, forms the window moments with a separable (horizontal then
+// vertical) filter, turns them into the coefficients a, b, d at every window centre
+// that can reach the block, and filters those coefficients back (again separably) to
+// get each pixel's SSIM gradient.  Only four moments are kept: the SSIM denominator
+// needs the two means of squares only as their sum.  Each pass gives every thread a
+// strip of outputs and streams the strip's inputs once, adding each input to every
+// output whose window holds it, so the registers hold the strip's accumulators and not
+// a window of inputs.  Windows are the reference's: centres whose whole window lies
+// inside the image (7x7 box, R = 3), or the 11-tap Gaussian (sigma 1.5, R = 5) with the
+// same rule.  The kernel also sums |x - y| and the SSIM of the windows centred in its
+// block for the loss value.
 #include "internal.h"
 
 namespace gs {
@@ -22,11 +26,6 @@ namespace gs {
 constexpr int LB_W = 32;
 constexpr int LB_H = 32;
 constexpr int LB_THREADS = 256;
-// Strip lengths of the four separable passes (outputs per thread task).
-constexpr int S1 = 7;   // horizontal moments
-constexpr int S2 = 4;   // vertical moments -> SSIM coefficients
-constexpr int S3 = 4;   // horizontal coefficients
-constexpr int S4 = 4;   // vertical coefficients -> gradient
 
 struct LossWeights {
     float w[11];
@@ -34,16 +33,36 @@ struct LossWeights {
 
 template <int R>
 struct LossDims {
+    static constexpr int K = 2 * R + 1;
     static constexpr int RW = LB_W + 4 * R;   // region with halo 2R
     static constexpr int RH = LB_H + 4 * R;
     static constexpr int HW = LB_W + 2 * R;   // window centres reaching the block
     static constexpr int CH = LB_H + 2 * R;
-    static constexpr int X_OFF = 0;
-    static constexpr int Y_OFF = RH * RW;
-    static constexpr int HM_OFF = 2 * RH * RW;               // 5 moments, RH x HW
-    static constexpr int C_OFF = HM_OFF + 5 * RH * HW;       // 3 coefficients, CH x HW
-    static constexpr int HC_OFF = HM_OFF;                    // 3 filtered coefs, CH x LB_W (aliases moments)
-    static constexpr int FLOATS = C_OFF + 3 * CH * HW;
+    static constexpr int HMP = HW + 2;        // row pitches chosen against bank conflicts
+    static constexpr int CFP = HW + 1;
+    // Strips: P1 horizontal moments, P2 vertical moments -> coefficients, P3 horizontal
+    // coefficients, P4 vertical coefficients -> gradient.  One task per thread each.
+    static constexpr int S1 = (HW + 3) / 4;                 // 4 strips per region row
+    static constexpr int NS1 = 4;
+    static constexpr int S2 = 7;
+    static constexpr int NS2 = (CH + S2 - 1) / S2;
+    static constexpr int S3 = 6;
+    static constexpr int NS3 = (LB_W + S3 - 1) / S3;
+    static constexpr int S4 = 4;
+    static constexpr int NS4 = LB_H / S4;
+    // Region A: image and target with halo, later the coefficients (X, Y are dead once
+    // the horizontal moments exist; the gradient pass reads its own pixels from HBM).
+    static constexpr int XY = 2 * RH * RW;
+    static constexpr int CF = 3 * CH * CFP;
+    static constexpr int A = XY > CF ? XY : CF;
+    // Region B: horizontal moments, later the horizontally filtered coefficients.
+    static constexpr int HM = 4 * RH * HMP;
+    static constexpr int HC = 3 * CH * LB_W;
+    static constexpr int B = HM > HC ? HM : HC;
+    static constexpr int FLOATS = A + B;
+    static_assert(RH * NS1 <= LB_THREADS && HW * NS2 <= LB_THREADS && CH * NS3 <= LB_THREADS &&
+                      LB_W * NS4 <= LB_THREADS,
+                  "one task per thread per pass");
 };
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -64,13 +83,14 @@ __device__ __forceinline__ float load_target<float>(const float* t, size_t idx) 
 }
 
 template <int R, typename TT>
-__global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const TT* __restrict__ target,
+__global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const TT* __restrict__ target,
                                                           LossWeights wts) {
     using D = LossDims<R>;
-    constexpr int K = 2 * R + 1;
+    constexpr int K = D::K;
     extern __shared__ float sm[];
     __shared__ float s_red[2][LB_THREADS / 32];
-    const int blk = a.block_first + blockIdx.x;
+    const int blk = a.block_first + (int)(blockIdx.x / 3u);
+    const int c = (int)(blockIdx.x % 3u);
     int vi = a.view_first;
     const int vend = a.view_first + a.num_views;
     while (vi + 1 < vend && a.views[vi + 1].loss_block_offset <= blk) vi++;
@@ -87,181 +107,190 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
     const bool use_ssim = a.lambda > 0.0f && windows > 0.0f;
     // Filter taps stay in the kernel-parameter constant bank (FFMA operands).
     const float* w = wts.w;
-    float* X = sm + D::X_OFF;
-    float* Y = sm + D::Y_OFF;
-    float* HM = sm + D::HM_OFF;
-    float* CF = sm + D::C_OFF;
-    float* HC = sm + D::HC_OFF;
+    float* X = sm;
+    float* Y = sm + D::RH * D::RW;
+    float* CF = sm;
+    float* HM = sm + D::A;
+    float* HC = sm + D::A;
     float l1 = 0.f, ssim_sum = 0.f;
     const float C1 = 1e-4f, C2 = 9e-4f;
-    constexpr int NS1 = (D::HW + S1 - 1) / S1;
-    constexpr int NS2 = (D::CH + S2 - 1) / S2;
-    constexpr int NS3 = LB_W / S3;
-    constexpr int NS4 = LB_H / S4;
-    for (int c = 0; c < 3; c++) {
-        if (use_ssim) {
-            for (int idx = threadIdx.x; idx < D::RH * D::RW; idx += LB_THREADS) {
-                const int ry = idx / D::RW, rx = idx % D::RW;
-                const int gx = bx0 - 2 * R + rx, gy = by0 - 2 * R + ry;
-                float xv = 0.f, yv = 0.f;
-                if (gx >= 0 && gy >= 0 && gx < W && gy < H) {
-                    const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
-                    xv = a.image[q];
-                    yv = load_target<TT>(target, q);
-                }
-                X[idx] = xv;
-                Y[idx] = yv;
-            }
-            __syncthreads();
-            // P1: horizontal moments, S1 centre columns per task from a register window.
-            for (int task = threadIdx.x; task < D::RH * NS1; task += LB_THREADS) {
-                const int r = task / NS1, c0 = (task % NS1) * S1;
-                // Products formed once per window element, not once per tap.
-                float xs[S1 + 2 * R], ys[S1 + 2 * R], xx[S1 + 2 * R], yy[S1 + 2 * R], xy[S1 + 2 * R];
-#pragma unroll
-                for (int t = 0; t < S1 + 2 * R; t++) {
-                    const int col = c0 + t;
-                    xs[t] = col < D::RW ? X[r * D::RW + col] : 0.f;
-                    ys[t] = col < D::RW ? Y[r * D::RW + col] : 0.f;
-                    xx[t] = xs[t] * xs[t];
-                    yy[t] = ys[t] * ys[t];
-                    xy[t] = xs[t] * ys[t];
-                }
-#pragma unroll
-                for (int k = 0; k < S1; k++) {
-                    if (c0 + k >= D::HW) break;
-                    float mx = 0.f, my = 0.f, sxx = 0.f, syy = 0.f, sxy = 0.f;
-#pragma unroll
-                    for (int t = 0; t < K; t++) {
-                        const float wt = w[t];
-                        mx = fmaf(wt, xs[k + t], mx);
-                        my = fmaf(wt, ys[k + t], my);
-                        sxx = fmaf(wt, xx[k + t], sxx);
-                        syy = fmaf(wt, yy[k + t], syy);
-                        sxy = fmaf(wt, xy[k + t], sxy);
-                    }
-                    const int o = r * D::HW + c0 + k;
-                    HM[0 * D::RH * D::HW + o] = mx;
-                    HM[1 * D::RH * D::HW + o] = my;
-                    HM[2 * D::RH * D::HW + o] = sxx;
-                    HM[3 * D::RH * D::HW + o] = syy;
-                    HM[4 * D::RH * D::HW + o] = sxy;
-                }
-            }
-            __syncthreads();
-            // P2: vertical moments at S2 window centres per task -> SSIM coefficients.
-            for (int task = threadIdx.x; task < D::HW * NS2; task += LB_THREADS) {
-                const int hc = task % D::HW, h0 = (task / D::HW) * S2;
-                float m[5][S2 + 2 * R];
-#pragma unroll
-                for (int q = 0; q < 5; q++)
-#pragma unroll
-                    for (int t = 0; t < S2 + 2 * R; t++) {
-                        const int row = h0 + t;
-                        m[q][t] = row < D::RH ? HM[q * D::RH * D::HW + row * D::HW + hc] : 0.f;
-                    }
-#pragma unroll
-                for (int k = 0; k < S2; k++) {
-                    const int hr = h0 + k;
-                    if (hr >= D::CH) break;
-                    const int gx = bx0 - R + hc, gy = by0 - R + hr;
-                    float ca = 0.f, cb = 0.f, cd = 0.f;
-                    if (gx >= R && gy >= R && gx < W - R && gy < H - R) {
-                        float mm[5];
-#pragma unroll
-                        for (int q = 0; q < 5; q++) {
-                            float acc = 0.f;
-#pragma unroll
-                            for (int t = 0; t < K; t++) acc += w[t] * m[q][k + t];
-                            mm[q] = acc;
-                        }
-                        const float mx = mm[0], my = mm[1], sxx = mm[2], syy = mm[3], sxy = mm[4];
-                        const float a1 = 2.0f * mx * my + C1;
-                        const float a2 = 2.0f * (sxy - mx * my) + C2;
-                        const float b1 = mx * mx + my * my + C1;
-                        const float b2 = (sxx - mx * mx) + (syy - my * my) + C2;
-                        // The approximate reciprocal instruction (about 1 ulp) without flushing
-                        // subnormals; a1, b1 >= C1 and b2 >= C2 (variances are >= 0 up to
-                        // rounding), a2 = 2 cov + C2 may take either sign.
-                        const float ia1 = rcp_approx(a1), ia2 = rcp_approx(a2);
-                        const float ib1 = rcp_approx(b1), ib2 = rcp_approx(b2);
-                        const float ssim = a1 * a2 * ib1 * ib2;
-                        ca = 2.0f * ssim * (my * ia1 - my * ia2 - mx * ib1 + mx * ib2);
-                        cb = -ssim * ib2;
-                        cd = 2.0f * ssim * ia2;
-                        if (gx >= bx0 && gx < bx0 + LB_W && gy >= by0 && gy < by0 + LB_H) ssim_sum += ssim;
-                    }
-                    const int o = hr * D::HW + hc;
-                    CF[0 * D::CH * D::HW + o] = ca;
-                    CF[1 * D::CH * D::HW + o] = cb;
-                    CF[2 * D::CH * D::HW + o] = cd;
-                }
-            }
-            __syncthreads();
-            // P3: filter the coefficients back, horizontal ...
-            for (int task = threadIdx.x; task < D::CH * NS3; task += LB_THREADS) {
-                const int hr = task / NS3, o0 = (task % NS3) * S3;
-                float cf[3][S3 + 2 * R];
-#pragma unroll
-                for (int q = 0; q < 3; q++)
-#pragma unroll
-                    for (int t = 0; t < S3 + 2 * R; t++) cf[q][t] = CF[q * D::CH * D::HW + hr * D::HW + o0 + t];
-#pragma unroll
-                for (int k = 0; k < S3; k++)
-#pragma unroll
-                    for (int q = 0; q < 3; q++) {
-                        float acc = 0.f;
-#pragma unroll
-                        for (int t = 0; t < K; t++) acc += w[t] * cf[q][k + t];
-                        HC[q * D::CH * LB_W + hr * LB_W + o0 + k] = acc;
-                    }
-            }
-            __syncthreads();
-        }
-        // P4: ... and vertical, then the per-pixel gradient (with the L1 term).
-        for (int task = threadIdx.x; task < LB_W * NS4; task += LB_THREADS) {
-            const int ox = task % LB_W, oy0 = (task / LB_W) * S4;
-            const int gx = bx0 + ox;
-            float hc[3][S4 + 2 * R];
-            if (use_ssim) {
-#pragma unroll
-                for (int q = 0; q < 3; q++)
-#pragma unroll
-                    for (int t = 0; t < S4 + 2 * R; t++) hc[q][t] = HC[q * D::CH * LB_W + (oy0 + t) * LB_W + ox];
-            }
-#pragma unroll
-            for (int k = 0; k < S4; k++) {
-                const int oy = oy0 + k, gy = by0 + oy;
-                if (gx >= W || gy >= H) continue;
+    const int tid = threadIdx.x;
+    if (use_ssim) {
+        for (int idx = tid; idx < D::RH * D::RW; idx += LB_THREADS) {
+            const int ry = idx / D::RW, rx = idx % D::RW;
+            const int gx = bx0 - 2 * R + rx, gy = by0 - 2 * R + ry;
+            float xv = 0.f, yv = 0.f;
+            if (gx >= 0 && gy >= 0 && gx < W && gy < H) {
                 const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
-                float xv, yv;
-                if (use_ssim) {
-                    xv = X[(oy + 2 * R) * D::RW + ox + 2 * R];
-                    yv = Y[(oy + 2 * R) * D::RW + ox + 2 * R];
-                } else {
-                    xv = a.image[q];
-                    yv = load_target<TT>(target, q);
-                }
-                const float diff = xv - yv;
-                float g = l1_scale * (float)((diff > 0.f) - (diff < 0.f));
-                l1 += fabsf(diff);
-                if (use_ssim) {
-                    float sa = 0.f, sb = 0.f, sd = 0.f;
+                xv = a.image[q];
+                yv = load_target<TT>(target, q);
+            }
+            X[idx] = xv;
+            Y[idx] = yv;
+        }
+        __syncthreads();
+        // P1: horizontal moments (x, y, x^2 + y^2, xy) at the centre columns of a strip.
+        if (tid < D::RH * D::NS1) {
+            const int r = tid / D::NS1, c0 = (tid % D::NS1) * D::S1;
+            float acc[D::S1][4];
 #pragma unroll
-                    for (int t = 0; t < K; t++) {
-                        sa += w[t] * hc[0][k + t];
-                        sb += w[t] * hc[1][k + t];
-                        sd += w[t] * hc[2][k + t];
-                    }
-                    g -= ssim_scale * (sa + 2.0f * xv * sb + yv * sd);
+            for (int k = 0; k < D::S1; k++)
+#pragma unroll
+                for (int m = 0; m < 4; m++) acc[k][m] = 0.f;
+#pragma unroll
+            for (int j = 0; j < D::S1 + 2 * R; j++) {
+                const int col = c0 + j;
+                const float xv = col < D::RW ? X[r * D::RW + col] : 0.f;
+                const float yv = col < D::RW ? Y[r * D::RW + col] : 0.f;
+                const float ss = fmaf(xv, xv, yv * yv), xy = xv * yv;
+#pragma unroll
+                for (int k = 0; k < D::S1; k++) {
+                    if (j - k < 0 || j - k >= K) continue;
+                    const float wt = w[j - k];
+                    acc[k][0] = fmaf(wt, xv, acc[k][0]);
+                    acc[k][1] = fmaf(wt, yv, acc[k][1]);
+                    acc[k][2] = fmaf(wt, ss, acc[k][2]);
+                    acc[k][3] = fmaf(wt, xy, acc[k][3]);
                 }
-                a.dl[q] = g;
+            }
+#pragma unroll
+            for (int k = 0; k < D::S1; k++) {
+                if (c0 + k >= D::HW) break;
+#pragma unroll
+                for (int m = 0; m < 4; m++) HM[m * D::RH * D::HMP + r * D::HMP + c0 + k] = acc[k][m];
+            }
+        }
+        __syncthreads();
+        // P2: vertical moments at a strip of window centres -> SSIM coefficients.
+        const bool p2 = tid < D::HW * D::NS2;
+        const int hc = tid % D::HW, h0 = (tid / D::HW) * D::S2;
+        float acc2[D::S2][4];
+#pragma unroll
+        for (int k = 0; k < D::S2; k++)
+#pragma unroll
+            for (int m = 0; m < 4; m++) acc2[k][m] = 0.f;
+        if (p2) {
+#pragma unroll
+            for (int j = 0; j < D::S2 + 2 * R; j++) {
+                const int row = h0 + j;
+                float v[4];
+#pragma unroll
+                for (int m = 0; m < 4; m++) v[m] = row < D::RH ? HM[m * D::RH * D::HMP + row * D::HMP + hc] : 0.f;
+#pragma unroll
+                for (int k = 0; k < D::S2; k++) {
+                    if (j - k < 0 || j - k >= K) continue;
+                    const float wt = w[j - k];
+#pragma unroll
+                    for (int m = 0; m < 4; m++) acc2[k][m] = fmaf(wt, v[m], acc2[k][m]);
+                }
+            }
+        }
+        // CF aliases X and Y, which only P1 read.
+        if (p2) {
+            const int gx = bx0 - R + hc;
+            const bool col_ok = gx >= R && gx < W - R;
+            const bool col_in = gx >= bx0 && gx < bx0 + LB_W;
+#pragma unroll
+            for (int k = 0; k < D::S2; k++) {
+                const int hr = h0 + k;
+                if (hr >= D::CH) break;
+                const int gy = by0 - R + hr;
+                float ca = 0.f, cb = 0.f, cd = 0.f;
+                if (col_ok && gy >= R && gy < H - R) {
+                    const float mx = acc2[k][0], my = acc2[k][1], s2 = acc2[k][2], sxy = acc2[k][3];
+                    const float a1 = 2.0f * mx * my + C1;
+                    const float a2 = 2.0f * (sxy - mx * my) + C2;
+                    const float b1 = mx * mx + my * my + C1;
+                    const float b2 = (s2 - mx * mx - my * my) + C2;
+                    // The approximate reciprocal instruction (about 1 ulp) without flushing
+                    // subnormals; a1, b1 >= C1 and b2 >= C2 (variances are >= 0 up to
+                    // rounding), a2 = 2 cov + C2 may take either sign.
+                    const float ia1 = rcp_approx(a1), ia2 = rcp_approx(a2);
+                    const float ib1 = rcp_approx(b1), ib2 = rcp_approx(b2);
+                    const float ssim = a1 * a2 * ib1 * ib2;
+                    ca = 2.0f * ssim * (my * ia1 - my * ia2 - mx * ib1 + mx * ib2);
+                    cb = -ssim * ib2;
+                    cd = 2.0f * ssim * ia2;
+                    if (col_in && gy >= by0 && gy < by0 + LB_H) ssim_sum += ssim;
+                }
+                const int o = hr * D::CFP + hc;
+                CF[0 * D::CH * D::CFP + o] = ca;
+                CF[1 * D::CH * D::CFP + o] = cb;
+                CF[2 * D::CH * D::CFP + o] = cd;
+            }
+        }
+        __syncthreads();
+        // P3: filter the coefficients back, horizontal ...
+        if (tid < D::CH * D::NS3) {
+            const int hr = tid / D::NS3, o0 = (tid % D::NS3) * D::S3;
+            float acc[D::S3][3];
+#pragma unroll
+            for (int k = 0; k < D::S3; k++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) acc[k][q] = 0.f;
+#pragma unroll
+            for (int j = 0; j < D::S3 + 2 * R; j++) {
+                const int col = o0 + j;
+                float v[3];
+#pragma unroll
+                for (int q = 0; q < 3; q++) v[q] = col < D::HW ? CF[q * D::CH * D::CFP + hr * D::CFP + col] : 0.f;
+#pragma unroll
+                for (int k = 0; k < D::S3; k++) {
+                    if (j - k < 0 || j - k >= K) continue;
+                    const float wt = w[j - k];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) acc[k][q] = fmaf(wt, v[q], acc[k][q]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < D::S3; k++) {
+                if (o0 + k >= LB_W) break;
+#pragma unroll
+                for (int q = 0; q < 3; q++) HC[q * D::CH * LB_W + hr * LB_W + o0 + k] = acc[k][q];
             }
         }
         __syncthreads();
     }
+    // P4: ... and vertical, then the per-pixel gradient (with the L1 term).
+    if (tid < LB_W * D::NS4) {
+        const int ox = tid % LB_W, oy0 = (tid / LB_W) * D::S4;
+        const int gx = bx0 + ox;
+        float acc[D::S4][3];
+#pragma unroll
+        for (int k = 0; k < D::S4; k++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) acc[k][q] = 0.f;
+        if (use_ssim) {
+#pragma unroll
+            for (int j = 0; j < D::S4 + 2 * R; j++) {
+                float v[3];
+#pragma unroll
+                for (int q = 0; q < 3; q++) v[q] = HC[q * D::CH * LB_W + (oy0 + j) * LB_W + ox];
+#pragma unroll
+                for (int k = 0; k < D::S4; k++) {
+                    if (j - k < 0 || j - k >= K) continue;
+                    const float wt = w[j - k];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) acc[k][q] = fmaf(wt, v[q], acc[k][q]);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < D::S4; k++) {
+            const int gy = by0 + oy0 + k;
+            if (gx >= W || gy >= H) continue;
+            const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
+            const float xv = a.image[q];
+            const float yv = load_target<TT>(target, q);
+            const float diff = xv - yv;
+            float g = l1_scale * (float)((diff > 0.f) - (diff < 0.f));
+            l1 += fabsf(diff);
+            if (use_ssim) g -= ssim_scale * (acc[k][0] + 2.0f * xv * acc[k][1] + yv * acc[k][2]);
+            a.dl[q] = g;
+        }
+    }
     // Block sums of |x - y| and SSIM -> per-view accumulators.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         l1 += __shfl_xor_sync(0xffffffffu, l1, o);
@@ -272,7 +301,7 @@ __global__ void __launch_bounds__(LB_THREADS, 2) loss_kernel(LossArgs a, const T
         s_red[1][warp] = ssim_sum;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         double t0 = 0.0, t1 = 0.0;
         for (int k = 0; k < LB_THREADS / 32; k++) {
             t0 += s_red[0][k];
@@ -302,7 +331,7 @@ static LossWeights make_weights(int window) {
 template <int R, typename TT>
 static void loss_launch(const LossArgs& a, const TT* target, const LossWeights& w, cudaStream_t s) {
     const size_t smem = LossDims<R>::FLOATS * sizeof(float);
-    loss_kernel<R, TT><<<a.num_blocks, LB_THREADS, smem, s>>>(a, target, w);
+    loss_kernel<R, TT><<<(unsigned)a.num_blocks * 3u, LB_THREADS, smem, s>>>(a, target, w);
 }
 
 void launch_loss(const LossArgs& a, cudaStream_t s) {

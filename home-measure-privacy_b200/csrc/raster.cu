@@ -173,8 +173,13 @@ __device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1,
     return splat_reaches_box(g0.x, g0.y, g0.z, g0.w, g1.x, g1.z, g1.w, ti.wx0, ti.wx1, ti.wy0, ti.wy1);
 }
 
+// Resident CTAs per SM the register allocation is sized for (64 threads with 4 pixels
+// each get more registers per thread than 16 CTAs would leave them).
+constexpr int fwd_min_ctas(int ppt) { return ppt == 4 ? 12 : 4 * ppt; }
+constexpr int bwd_min_ctas(int ppt) { return ppt == 4 ? 10 : (ppt == 2 ? 7 : 4); }
+
 template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT, 4 * PPT) raster_fwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -308,7 +313,7 @@ __device__ __forceinline__ float warp_sum8_transposed(float v[8]) {
 }
 
 template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT, PPT == 2 ? 7 : 4) raster_bwd_kernel(RasterArgs a) {
+__global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kernel(RasterArgs a) {
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -484,7 +489,13 @@ static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
 
 #define RASTER_SWITCH(FN, batch, ppt, ...)                   \
     do {                                                     \
-        if ((ppt) == 2) {                                    \
+        if ((ppt) == 4) {                                    \
+            switch (batch) {                                 \
+                case 64: FN<64, 4>(__VA_ARGS__); break;      \
+                case 128: FN<128, 4>(__VA_ARGS__); break;    \
+                default: FN<256, 4>(__VA_ARGS__); break;     \
+            }                                                \
+        } else if ((ppt) == 2) {                             \
             switch (batch) {                                 \
                 case 64: FN<64, 2>(__VA_ARGS__); break;      \
                 case 128: FN<128, 2>(__VA_ARGS__); break;    \

@@ -163,6 +163,37 @@ def test_batched_equals_plain(hmp):
     assert np.array_equal(out[True], out[False])
 
 
+@pytest.mark.parametrize("ppt", [1, 2, 4])
+def test_raster_variants_agree(hmp, ppt):
+    """Every (shared-memory batch, pixels per thread) variant the autotuner may pick,
+    persistent over four uneven views: the same images bit for bit (each pixel blends the
+    same splats in the same order) and the same gradients up to atomic order."""
+    rec = hmp.synthetic_scene(50_000, 3, 3, "normal", (-4.5, 0.7), (0.0, 1.5))
+    tg = hmp.scene.jitter_means(rec, 5)
+    cams = hmp.ring_cameras([(320, 240), (400, 300), (512, 384), (640, 360)], 4.0)
+
+    def run(batch, p):
+        with make(hmp, 3, raster_batch=batch, raster_ppt=p) as r:
+            r.set_gaussians(tg)
+            r.set_views(cams)
+            timgs = r.forward(0, 4)
+            off = 0
+            for v, c in enumerate(cams):
+                px = c["width"] * c["height"] * 3
+                r.set_target(v, timgs[off:off + px])
+                off += px
+            r.set_gaussians(rec)
+            img = r.forward(0, 4)
+            r.loss(ssim=0.2, window=1)
+            return img, r.backward()
+
+    ref_img, ref_g = run(256, 1)
+    for batch in (64, 128, 256):
+        img, g = run(batch, ppt)
+        assert np.array_equal(img, ref_img), batch
+        assert rel_err(g, ref_g) < 1e-5, batch
+
+
 # ---------------------------------------------------------------------------------- loss
 def test_loss_gradient_golden(hmp):
     g = golden("ssim_test.npz")
