@@ -71,14 +71,17 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
+// Targets as floats: u8 photos through a per-CTA table of v / 255 (the correctly
+// rounded quotient, equal to the reference's double quotient rounded to float for every
+// byte), float targets as they are.
 template <typename TT>
-__device__ __forceinline__ float load_target(const TT* t, size_t idx);
+__device__ __forceinline__ float load_target(const TT* t, size_t idx, const float* lut);
 template <>
-__device__ __forceinline__ float load_target<uint8_t>(const uint8_t* t, size_t idx) {
-    return (float)t[idx] / 255.0f;
+__device__ __forceinline__ float load_target<uint8_t>(const uint8_t* t, size_t idx, const float* lut) {
+    return lut[t[idx]];
 }
 template <>
-__device__ __forceinline__ float load_target<float>(const float* t, size_t idx) {
+__device__ __forceinline__ float load_target<float>(const float* t, size_t idx, const float*) {
     return t[idx];
 }
 
@@ -89,6 +92,8 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
     constexpr int K = D::K;
     extern __shared__ float sm[];
     __shared__ float s_red[2][LB_THREADS / 32];
+    __shared__ float s_lut[256];
+    if (sizeof(TT) == 1) s_lut[threadIdx.x] = (float)threadIdx.x / 255.0f;
     const int blk = a.block_first + (int)(blockIdx.x / 3u);
     const int c = (int)(blockIdx.x % 3u);
     int vi = a.view_first;
@@ -115,18 +120,31 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
     float l1 = 0.f, ssim_sum = 0.f;
     const float C1 = 1e-4f, C2 = 9e-4f;
     const int tid = threadIdx.x;
+    __syncthreads();  // byte table
     if (use_ssim) {
-        for (int idx = tid; idx < D::RH * D::RW; idx += LB_THREADS) {
+        // All of a thread's region loads are issued before the first shared-memory store.
+        constexpr int NL = (D::RH * D::RW + LB_THREADS - 1) / LB_THREADS;
+        float xl[NL], yl[NL];
+#pragma unroll
+        for (int i = 0; i < NL; i++) {
+            const int idx = tid + i * LB_THREADS;
             const int ry = idx / D::RW, rx = idx % D::RW;
             const int gx = bx0 - 2 * R + rx, gy = by0 - 2 * R + ry;
-            float xv = 0.f, yv = 0.f;
-            if (gx >= 0 && gy >= 0 && gx < W && gy < H) {
+            xl[i] = 0.f;
+            yl[i] = 0.f;
+            if (idx < D::RH * D::RW && gx >= 0 && gy >= 0 && gx < W && gy < H) {
                 const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
-                xv = a.image[q];
-                yv = load_target<TT>(target, q);
+                xl[i] = a.image[q];
+                yl[i] = load_target<TT>(target, q, s_lut);
             }
-            X[idx] = xv;
-            Y[idx] = yv;
+        }
+#pragma unroll
+        for (int i = 0; i < NL; i++) {
+            const int idx = tid + i * LB_THREADS;
+            if (idx < D::RH * D::RW) {
+                X[idx] = xl[i];
+                Y[idx] = yl[i];
+            }
         }
         __syncthreads();
         // P1: horizontal moments (x, y, x^2 + y^2, xy) at the centre columns of a strip.
@@ -281,7 +299,7 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
             if (gx >= W || gy >= H) continue;
             const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
             const float xv = a.image[q];
-            const float yv = load_target<TT>(target, q);
+            const float yv = load_target<TT>(target, q, s_lut);
             const float diff = xv - yv;
             float g = l1_scale * (float)((diff > 0.f) - (diff < 0.f));
             l1 += fabsf(diff);
