@@ -69,18 +69,6 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_tmp,
     return prefix + x - v;
 }
 
-// Lanes (among `valid` ones) holding the same 8-bit digit as this lane: one ballot per
-// digit bit, unrolled.
-__device__ __forceinline__ uint32_t warp_peers(uint32_t d, bool valid) {
-    uint32_t peers = __ballot_sync(FULL, valid);
-#pragma unroll
-    for (int b = 0; b < 8; b++) {
-        const uint32_t bal = __ballot_sync(FULL, (d >> b) & 1u);
-        peers &= ((d >> b) & 1u) ? bal : ~bal;
-    }
-    return peers;
-}
-
 // ---------------------------------------------------------------------------------
 // Radix sort, one sweep per digit (the Onesweep scheme of Adinets and Merrill): one
 // kernel counts the digits of every pass over the whole segment; each pass is then a
@@ -187,33 +175,50 @@ __global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
     if (threadIdx.x == 0) s_part = atomicAdd(counter, 1u);
-    for (int d = threadIdx.x; d < OS_WARPS * 256; d += OS_THREADS) (&s_warp[0][0])[d] = 0u;
+    for (int d = threadIdx.x; d < OS_WARPS * 256; d += OS_THREADS) {
+        (&s_warp[0][0])[d] = 0u;
+        s_keys[d] = 0u;
+    }
     __syncthreads();
     const uint32_t p = s_part;
     if (p >= P) return;
     const uint32_t part_start = p * RS_TILE;
     const uint32_t warp_start = part_start + warp * (OS_ITEMS * 32);
-    uint32_t k[OS_ITEMS], pos[OS_ITEMS], peers[OS_ITEMS];
+    uint32_t k[OS_ITEMS], pos[OS_ITEMS];
 #pragma unroll
     for (int j = 0; j < OS_ITEMS; j++) {
         const uint32_t idx = warp_start + j * 32 + lane;
         k[j] = idx < n ? __ldg(keys_in + base + idx) : 0xffffffffu;
     }
-    // Equal digits by ballot for every item first (independent), then the running
-    // counts in the warp's row, item by item.
-#pragma unroll
-    for (int j = 0; j < OS_ITEMS; j++) peers[j] = warp_peers((k[j] >> shift) & 0xffu, warp_start + j * 32 + lane < n);
+    // Item by item: the lanes holding the same digit (each lane ORs its bit into the
+    // digit's word of the warp's match row, then reads the word back; a warp whose valid
+    // lanes all hold one digit skips that), then the running counts in the warp's row.
+    // The match rows live in s_keys until the keys are placed; they start zeroed and
+    // each group's first lane clears its word again.
+    uint32_t* s_match = s_keys + warp * 256;
 #pragma unroll
     for (int j = 0; j < OS_ITEMS; j++) {
         const bool valid = warp_start + j * 32 + lane < n;
         const uint32_t d = (k[j] >> shift) & 0xffu;
-        uint32_t prev = 0;
-        if (valid) {
-            prev = s_warp[warp][d];
-            pos[j] = prev + __popc(peers[j] & lt_mask);
+        const uint32_t d0 = __shfl_sync(FULL, d, 0);
+        const uint32_t vmask = __ballot_sync(FULL, valid);
+        uint32_t pm;
+        const bool uniform = __all_sync(FULL, !valid || d == d0);
+        if (uniform) {
+            pm = valid ? vmask : 0u;
+        } else {
+            if (valid) atomicOr(&s_match[d], 1u << lane);
+            __syncwarp();
+            pm = valid ? s_match[d] : 0u;
         }
+        const uint32_t prev = valid ? s_warp[warp][d] : 0u;
         __syncwarp();
-        if (valid && (peers[j] & lt_mask) == 0u) s_warp[warp][d] = prev + __popc(peers[j]);
+        const bool leader = valid && (pm & lt_mask) == 0u;
+        if (leader) {
+            if (!uniform) s_match[d] = 0u;
+            s_warp[warp][d] = prev + __popc(pm);
+        }
+        pos[j] = prev + __popc(pm & lt_mask);
         __syncwarp();
     }
     __syncthreads();
