@@ -241,8 +241,11 @@ def run_b200(args, rank, local, world, dist):
     # ---- e2e through the public API: pinned host targets in, loss out, every step
     e2e = None
     if not args.no_e2e:
+        # The same trajectory as the timed loop above: the scene and optimiser restart from
+        # the initial records, then the same warm-up and timed step counts.
+        r.set_gaussians(c["records"])
         if dp:
-            t_e = timed(r, args.steps, 2, host=targets)
+            t_e = timed(r, args.steps, args.warmup, host=targets)
         else:
             # pinned photos in, every step's loss out (pinned), copies overlapping the
             # previous step (gs_train_step_host_async)
@@ -251,8 +254,8 @@ def run_b200(args, rank, local, world, dist):
             ctypes.memmove(host.value, targets.ctypes.data, targets.nbytes)
             losses = ctypes.c_void_p()
             N.check(r.lib.gs_host_alloc(4 * (args.steps + 8), ctypes.byref(losses)))
-            for k in range(2):
-                r.train_step_async(host, losses.value + 4 * k, ad, lam, window)
+            for k in range(args.warmup):
+                r.train_step_async(host, losses.value + 4 * (k % 8), ad, lam, window)
             r.synchronize()
             if dist:
                 dist.barrier()

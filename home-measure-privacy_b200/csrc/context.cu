@@ -962,7 +962,7 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if ((rc = ensure(c->status, sizeof(DevStatus), c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->visible, sizeof(unsigned) * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->acc, sizeof(double) * 2 * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
-    if ((rc = ensure(c->totals, 8192, c)) != GS_OK) return bail(rc);
+    if ((rc = ensure(c->totals, 16384, c)) != GS_OK) return bail(rc);
     if ((rc = ensure(c->views_d, sizeof(ViewDesc) * (GS_MAX_VIEWS + 1), c)) != GS_OK) return bail(rc);
     if (cudaMemset(c->status.p, 0, sizeof(DevStatus)) != cudaSuccess) return bail(fail(GS_ERR_CUDA, "memset"));
     if (cudaMallocHost((void**)&c->status_host, sizeof(DevStatus)) != cudaSuccess)

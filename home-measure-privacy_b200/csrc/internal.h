@@ -89,7 +89,7 @@ struct RadixSortArgs {
     const SegInfo* seg;
     int begin_bit, end_bit;  // bits to sort
     unsigned long long* hist;  // look-back words, 256 * max_parts
-    uint32_t* totals;        // digit counts of every pass and partition counters (>= 1028 words)
+    uint32_t* totals;        // digit counts and offsets of every pass, partition counters (>= 2053 words)
     int max_parts;
     unsigned int* timeout;   // set when a look-back wait gave up
 };

@@ -119,7 +119,8 @@ __device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
 // atomics into per-warp rows (equal digits within a warp serialise in hardware, which
 // costs little even when a byte is constant), four keys per thread per round.
 __global__ void __launch_bounds__(RS_THREADS) radix_hist_all(const uint32_t* __restrict__ keys, const SegInfo* seg,
-                                                             int begin_bit, int passes, uint32_t* __restrict__ ghist) {
+                                                             int begin_bit, int passes, uint32_t* __restrict__ ghist,
+                                                             uint32_t* __restrict__ gex, uint32_t* blocks_done) {
     __shared__ uint32_t wh[OS_MAX_PASSES][RS_WARPS][256];
     const uint32_t base = seg->base, n = seg->count;
     const int warp = threadIdx.x >> 5;
@@ -147,18 +148,34 @@ __global__ void __launch_bounds__(RS_THREADS) radix_hist_all(const uint32_t* __r
         for (int w = 0; w < RS_WARPS; w++) s += wh[p][w][d];
         if (s) atomicAdd(ghist + i, s);
     }
+    // The last block to finish turns the counts into each pass's exclusive digit offsets.
+    __shared__ uint32_t s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(blocks_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    __shared__ uint32_t s_tmp[32];
+    for (int p = 0; p < passes; p++) {
+        uint32_t tot;
+        const uint32_t c = threadIdx.x < 256 ? __ldcg(ghist + p * 256 + threadIdx.x) : 0u;
+        const uint32_t ex = block_excl_scan<RS_THREADS>(c, s_tmp, tot);
+        if (threadIdx.x < 256) gex[p * 256 + threadIdx.x] = ex;
+    }
 }
 
-// One partition of OS_THREADS x OS_ITEMS = RS_TILE keys per block: more, shorter
-// ranking chains (one per warp) than 256 threads x 16 items.
-constexpr int OS_THREADS = 512;
+// One partition of OS_THREADS x OS_ITEMS = RS_TILE keys per block; 256 threads of 16
+// keys leave room for four resident partitions per SM, which hides more of each
+// partition's load, look-back and scatter latency than two blocks of 512 threads.
+constexpr int OS_THREADS = 256;
 constexpr int OS_ITEMS = RS_TILE / OS_THREADS;
 constexpr int OS_WARPS = OS_THREADS / 32;
 
 template <typename W>
-__global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
+__global__ void __launch_bounds__(OS_THREADS, 4) radix_onesweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
-    uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ ghist,
+    uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ gex,
     W* look, uint32_t* counter, unsigned int* timeout) {
     using LW = LookWord<W>;
     __shared__ uint32_t s_keys[RS_TILE];
@@ -237,10 +254,9 @@ __global__ void __launch_bounds__(OS_THREADS, 2) radix_onesweep(
     // Publish this partition's count as early as possible.
     W* my = look + (size_t)p * 256 + (owner ? d : 0);
     if (owner) st_relaxed(my, (W)((p == 0 ? LW::INC : LW::AGG) | (W)cnt));
+    if (owner) s_global[d] = __ldg(gex + d);
     {
         uint32_t tot;
-        const uint32_t gex = block_excl_scan<OS_THREADS>(owner ? ghist[d] : 0u, s_tmp, tot);
-        if (owner) s_global[d] = gex;
         const uint32_t lex = block_excl_scan<OS_THREADS>(cnt, s_tmp, tot);
         if (owner) s_digit_start[d] = lex;
     }
@@ -324,10 +340,13 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
     int passes, step;
     pass_plan(a.begin_bit, a.end_bit, passes, step);
     const int grid = a.max_parts > 0 ? a.max_parts : 1;
-    uint32_t* ghist = a.totals;                           // [passes][256]
-    uint32_t* counters = a.totals + OS_MAX_PASSES * 256;  // one partition counter per pass
-    cudaMemsetAsync(a.totals, 0, (OS_MAX_PASSES * 256 + OS_MAX_PASSES) * sizeof(uint32_t), s);
-    radix_hist_all<<<min(grid, OS_HIST_BLOCKS), RS_THREADS, 0, s>>>(a.keys, a.seg, a.begin_bit, passes, ghist);
+    uint32_t* ghist = a.totals;                               // [passes][256] digit counts
+    uint32_t* gex = a.totals + OS_MAX_PASSES * 256;           // [passes][256] exclusive offsets
+    uint32_t* counters = a.totals + 2 * OS_MAX_PASSES * 256;  // one partition counter per pass
+    uint32_t* blocks_done = counters + OS_MAX_PASSES;
+    cudaMemsetAsync(a.totals, 0, (2 * OS_MAX_PASSES * 256 + OS_MAX_PASSES + 1) * sizeof(uint32_t), s);
+    radix_hist_all<<<min(grid, OS_HIST_BLOCKS), RS_THREADS, 0, s>>>(a.keys, a.seg, a.begin_bit, passes, ghist, gex,
+                                                                    blocks_done);
     uint32_t* kb[2] = {a.keys, a.keys_alt};
     uint32_t* vb[2] = {a.vals, a.vals_alt};
     // The largest key count this buffer can hold decides the look-back word width.
@@ -338,12 +357,12 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
         if (wide) {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(unsigned long long), s);
             radix_onesweep<unsigned long long><<<grid, OS_THREADS, 0, s>>>(
-                kb[in], vin, kb[out], vb[out], a.seg, a.begin_bit + p * step, ghist + p * 256,
+                kb[in], vin, kb[out], vb[out], a.seg, a.begin_bit + p * step, gex + p * 256,
                 reinterpret_cast<unsigned long long*>(a.hist), counters + p, a.timeout);
         } else {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
             radix_onesweep<uint32_t><<<grid, OS_THREADS, 0, s>>>(kb[in], vin, kb[out], vb[out], a.seg,
-                                                                  a.begin_bit + p * step, ghist + p * 256,
+                                                                  a.begin_bit + p * step, gex + p * 256,
                                                                   reinterpret_cast<uint32_t*>(a.hist), counters + p,
                                                                   a.timeout);
         }
