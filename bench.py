@@ -304,13 +304,13 @@ def run_b200(args, rank, local, world, dist):
 def profile_case(args):
     """Small case for ncu captures (one kernel, few launches, ~2 GB on the device): the
     benchmark scene (1M Gaussians, SH3) seen by its three largest views, raster variants
-    fixed at batch 256, 2 pixels per thread (the tuned backward variant), three
+    fixed at batch 128, 4 pixels per thread (the tuned backward variant), three
     graph-replayed training steps."""
     hmp = importlib.import_module("home-measure-privacy_b200")
     c = hmp.config(3)
     cams = c["cameras"][-3:]
     targets = make_targets(hmp, c, cams, 0)
-    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=256, raster_ppt=2,
+    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=128, raster_ppt=4,
                             device=0) as r:
         r.set_gaussians(c["records"])
         r.set_views(cams)
