@@ -1821,7 +1821,8 @@ int gs_get_stats(GsContext* c, GsStats* out) {
     out->kernel_launches_per_step = c->last_step_launches;
     out->raster_batch = c->batch_bwd;
     out->raster_threads = 256 / c->ppt_bwd;
-    out->raster_variant = c->batch_fwd | (c->ppt_fwd << 12) | (c->batch_bwd << 16) | (c->ppt_bwd << 28);
+    out->raster_variant = (int32_t)((uint32_t)c->batch_fwd | ((uint32_t)c->ppt_fwd << 12) |
+                                    ((uint32_t)c->batch_bwd << 16) | ((uint32_t)c->ppt_bwd << 28));
     out->overflow = (int32_t)c->skipped_steps;
     return GS_OK;
 }
