@@ -304,13 +304,14 @@ def run_b200(args, rank, local, world, dist):
 def profile_case(args):
     """Small case for ncu captures (one kernel, few launches, ~2 GB on the device): the
     benchmark scene (1M Gaussians, SH3) seen by its three largest views, raster variants
-    fixed at batch 128, 4 pixels per thread (the tuned backward variant), three
-    graph-replayed training steps."""
+    fixed at batch 128 and --profile-ppt pixels per thread (default 4, the tuned
+    backward variant; 2 is the tuned forward variant), three graph-replayed training
+    steps."""
     hmp = importlib.import_module("home-measure-privacy_b200")
     c = hmp.config(3)
     cams = c["cameras"][-3:]
     targets = make_targets(hmp, c, cams, 0)
-    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=128, raster_ppt=4,
+    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=128, raster_ppt=args.profile_ppt,
                             device=0) as r:
         r.set_gaussians(c["records"])
         r.set_views(cams)
@@ -487,6 +488,8 @@ def main():
                     help="use the data-parallel step (gradients, NCCL all-reduce, update) even on one GPU")
     ap.add_argument("--autotune-cache", default=None,
                     help="file caching the raster variant choice (a profiled run then uses the unprofiled choice)")
+    ap.add_argument("--profile-ppt", type=int, default=4, choices=(1, 2, 4),
+                    help="pixels per raster thread in --profile-case")
     ap.add_argument("--profile-case", action="store_true",
                     help="run the small ncu capture case instead of the benchmark")
     args = ap.parse_args()
