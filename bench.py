@@ -3,13 +3,18 @@
 up to 1920x1080, fused L1 + D-SSIM loss, Adam; steps/s on B200 beside the plain
 one-view-per-launch path and the reference's algorithm on the host CPU.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config 2|3|4]
 
 Prints one JSON line (rank 0).  value = whole-job training steps per second (each step
 = forward + loss + backward + Adam over one rank's 8 views, summed over ranks), device
 time measured with CUDA events on the library's stream; e2e = the same step through the
 public C ABI with this step's target photos copied host->device (pinned) and the loss
-copied back every step.
+copied back every step.  --config 2 / 4 time the single-view 200k-Gaussian step and the
+heavy-tailed 3M-Gaussian 8 x 1080p step the same way (the headline is config 3).
+
+--impl reference times the reference's step on the host CPU: its per-view trainScene
+step (trainer/gpu.js:915-933) restated in C (oracle/gs_oracle.c, FP32, OpenMP over all
+host threads, per-tile cap 1,024), run over the same workload's views.
 """
 import argparse
 import ctypes
@@ -29,7 +34,12 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 METRIC = "train steps/s, 1M splats x 8 views@1080p: batched adjoint vs plain; grad err vs FP64"
-WORKLOAD = "1M Gaussians SH3, 8 views 640x480..1920x1080 (9,157,632 px), L1+D-SSIM(11-tap), Adam"
+WORKLOADS = {
+    3: "1M Gaussians SH3, 8 views 640x480..1920x1080 (9,157,632 px), L1+D-SSIM(11-tap), Adam",
+    2: "200k Gaussians SH3, 1 view 1024x768 (786,432 px), L1+D-SSIM(11-tap), Adam",
+    4: "3M heavy-tailed Gaussians SH3 (50 blobs), 8 views 1920x1080 (16,588,800 px), L1+D-SSIM(11-tap), Adam",
+}
+L2_BYTES = 126 * 1024 * 1024
 
 
 def env_rank():
@@ -90,17 +100,37 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------------------
-def workload(hmp, rank, world):
-    """Config 3: scene (seed 3) and ring cameras; rank r sees the ring rotated by r/N of a
-    camera spacing (its own 8 views)."""
-    c = hmp.config(3)
+def workload(hmp, index, rank, world):
+    """Scene and cameras of a benchmark configuration (config 3 by default: 1M Gaussians,
+    seed 3, ring cameras); with N ranks, rank r sees the ring rotated by r/N of a camera
+    spacing (its own views)."""
+    c = hmp.config(index)
     cams = c["cameras"]
-    if world > 1:
-        cams = []
-        for i, (w, h) in enumerate(hmp.scene.CONFIG3_RESOLUTIONS):
-            a = 2 * math.pi * (i + rank / world) / 8
-            cams.append(hmp.look_at([4 * math.sin(a), 0.0, 4 * math.cos(a)], [0, 0, 0], w, h, 900.0 / 1024.0 * w))
+    if world > 1 and len(cams) > 1:
+        k = len(cams)
+        out = []
+        for i, cm in enumerate(cams):
+            w, h = cm["width"], cm["height"]
+            a = 2 * math.pi * (i + rank / world) / k
+            out.append(hmp.look_at([4 * math.sin(a), 0.0, 4 * math.cos(a)], [0, 0, 0], w, h, 900.0 / 1024.0 * w))
+        cams = out
     return c, cams
+
+
+def config_dict(hmp, c, cams, index, world):
+    """The workload's `config` object: the same for both arms of one run."""
+    n = c["records"].shape[0]
+    P = hmp.stride(c["degree"]) * 4
+    resident = 4 * n * P
+    pairs = n * len(cams) * 48
+    return dict(workload=WORKLOADS[index], gaussians=n, views=len(cams),
+                pixels=sum(cm["width"] * cm["height"] for cm in cams), sh_degree=c["degree"], near=c["near"],
+                ssim_lambda=c["ssim_lambda"], window="11-tap gaussian" if c["window"] == 1 else "7x7 box",
+                l2=(f"inputs larger than L2 (126 MB): params+moments+grads {resident / 1e6:.0f} MB, "
+                    f"pair records {pairs / 1e6:.0f} MB per step"
+                    if resident > L2_BYTES else "inputs smaller than L2"),
+                parallelism=(f"dp{world}: own views per GPU, gradients summed by one NCCL all-reduce per step"
+                             if world > 1 else "dp1: one GPU, all views"))
 
 
 def make_targets(hmp, c, cams, device):
@@ -138,18 +168,27 @@ def algorithmic_bytes(st, n, planes, views, pixels, tiles):
     }
 
 
-def profiled_traffic(kernel):
-    """DRAM bytes per launch of `kernel` on the benchmark workload, from the committed
-    ncu summary profiles/<kernel>_1M_sh3_8views_dram.md (line 'traffic per launch: B
-    bytes'); None when there is none."""
-    path = os.path.join(REPO, "profiles", f"{kernel}_1M_sh3_8views_dram.md")
+def profiled_traffic(kernel, bytes_full):
+    """DRAM bytes per launch of `kernel` on this workload: the ratio of DRAM bytes to
+    algorithmic bytes measured by ncu on the small capture case (profiles/traffic.json,
+    one kernel, one launch), applied to this launch's algorithmic bytes; None when the
+    kernel was not captured."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
     try:
-        for line in open(path):
-            if line.startswith("traffic per launch:"):
-                return int(line.split(":")[1].split()[0])
-    except OSError:
-        pass
-    return None
+        k = json.load(open(path))["kernels"][kernel]
+        return int(round(k["dram_bytes"] / k["algorithmic_bytes"] * bytes_full))
+    except (OSError, KeyError, ValueError, ZeroDivisionError):
+        return None
+
+
+def profiled_issue(kernel):
+    """Warp instructions and FP32 operations per blend of `kernel` (ncu on the small
+    capture case, profiles/traffic.json), or None."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        return json.load(open(path))["kernels"][kernel].get("per_blend")
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def run_b200(args, rank, local, world, dist):
@@ -159,7 +198,7 @@ def run_b200(args, rank, local, world, dist):
     DP = import_module("home-measure-privacy_b200.data_parallel")
     dp = dist is not None
     device = local
-    c, cams = workload(hmp, rank, world)
+    c, cams = workload(hmp, args.config, rank, world)
     targets = make_targets(hmp, c, cams, device)
     n = c["records"].shape[0]
     V = len(cams)
@@ -202,11 +241,17 @@ def run_b200(args, rank, local, world, dist):
             dist.barrier()
         r.synchronize()
 
-    def timed(r, steps, warmup, host=None):
+    def counters(r):
+        # Adam updates applied so far and steps whose key instances overflowed (those
+        # skip their update; a step that must return its loss is then redone).
+        return r.step_count(), int(r.stats()["overflow"])
+
+    def timed(r, steps, warmup, host=None, tag=None):
         for _ in range(warmup):
             one_step(r, host, False)
         r.synchronize()
         r.stage_times_reset()
+        t0, o0 = counters(r)
         sync_all(r)
         lib, ctx = r.lib, r.ctx
         N.check(lib.gs_event_record(ctx, 0))
@@ -216,6 +261,9 @@ def run_b200(args, rank, local, world, dist):
         ms = ctypes.c_float(0.0)
         N.check(lib.gs_event_elapsed(ctx, 0, 1, ctypes.byref(ms)))
         r.synchronize()
+        if tag:
+            t1, o1 = counters(r)
+            res[tag] = dict(skipped_steps=steps - (t1 - t0), overflow=o1 - o0)
         t = ms.value
         if dist:
             import torch
@@ -230,7 +278,7 @@ def run_b200(args, rank, local, world, dist):
     clocks = Clocks(device)
     clocks.start()
     time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
-    t_b = timed(r, args.steps, args.warmup)
+    t_b = timed(r, args.steps, args.warmup, tag="counts")
     res["clocks"] = clocks.stop()
     stages = r.stage_times()
     st = r.stats()
@@ -245,7 +293,7 @@ def run_b200(args, rank, local, world, dist):
         # the initial records, then the same warm-up and timed step counts.
         r.set_gaussians(c["records"])
         if dp:
-            t_e = timed(r, args.steps, args.warmup, host=targets)
+            t_e = timed(r, args.steps, args.warmup, host=targets, tag="e2e_counts")
         else:
             # pinned photos in, every step's loss out (pinned), copies overlapping the
             # previous step (gs_train_step_host_async)
@@ -257,6 +305,7 @@ def run_b200(args, rank, local, world, dist):
             for k in range(args.warmup):
                 r.train_step_async(host, losses.value + 4 * (k % 8), ad, lam, window)
             r.synchronize()
+            t0, o0 = counters(r)
             if dist:
                 dist.barrier()
             N.check(r.lib.gs_event_record(r.ctx, 0))
@@ -267,6 +316,8 @@ def run_b200(args, rank, local, world, dist):
             ms = ctypes.c_float(0.0)
             N.check(r.lib.gs_event_elapsed(r.ctx, 0, 1, ctypes.byref(ms)))
             t_e = ms.value
+            t1, o1 = counters(r)
+            res["e2e_counts"] = dict(skipped_steps=args.steps - (t1 - t0), overflow=o1 - o0)
             got = np.ctypeslib.as_array(ctypes.cast(losses.value, ctypes.POINTER(ctypes.c_float)), (args.steps,))
             res["e2e_losses_finite"] = bool(np.isfinite(got).all())
             N.check(r.lib.gs_host_free(losses))
@@ -274,13 +325,15 @@ def run_b200(args, rank, local, world, dist):
         e2e = dict(value=world * 1000.0 / (t_e / args.steps), unit="steps/s", h2d_bytes_per_step=int(targets.nbytes),
                    d2h_bytes_per_step=4 if not dp else 64,
                    how=("pinned photos copied host->device on a copy stream overlapping the previous step, "
-                        "each step's loss copied back" if not dp else "photos uploaded per view, loss read back"))
+                        "each step's loss copied back" if not dp else "photos uploaded per view, loss read back"),
+                   **res.get("e2e_counts", {}))
+    extras = not args.no_densify and not dp and args.config == 3
     # ---- scene file load / save at the benchmark size, after the timed region
-    if not args.no_densify and not dp:
+    if extras:
         res["scene_io"] = scene_io_measure(r, args)
         res["init"] = init_measure(r, args)
     # ---- densification on the device (trainScene's settings), after the timed region
-    if not args.no_densify and not dp:
+    if extras:
         res["densify"] = densify_measure(hmp, r, c, cams, ad, lam, window, args)
     r.close()
     # ---- plain: one view per launch per stage, same step
@@ -296,7 +349,7 @@ def run_b200(args, rank, local, world, dist):
         t_d = timed(rd, max(3, args.steps // 4), 2)
         res["plain_direct"] = 1000.0 / (t_d / max(3, args.steps // 4))
         rd.close()
-    res.update(ms_step=ms_step, plain=plain, e2e=e2e, tuned=tuned, n=n, V=V, pixels=pixels)
+    res.update(ms_step=ms_step, plain=plain, e2e=e2e, tuned=tuned, n=n, V=V, pixels=pixels, c=c, cams=cams)
     res["bytes"] = algorithmic_bytes(st, n, hmp.stride(c["degree"]), V, pixels, int(st["tiles"]))
     return res
 
@@ -324,8 +377,12 @@ def profile_case(args):
         for _ in range(3):
             loss = r.train_step(ad, c["ssim_lambda"], c["window"])
         st = r.stats()
+        pixels = sum(cm["width"] * cm["height"] for cm in cams)
+        nb = algorithmic_bytes(st, c["records"].shape[0], hmp.stride(c["degree"]), len(cams), pixels,
+                               int(st["tiles"]))
         print(json.dumps(dict(case="profile", views=len(cams), pixels=int(st["pixels"]),
-                              instances=int(st["instances"]), loss=float(loss),
+                              instances=int(st["instances"]), visible_pairs=int(st["visible_pairs"]),
+                              blends=int(r.blend_count()), loss=float(loss), algorithmic_bytes=nb,
                               stages_ms=r.stage_times()["ms"])), flush=True)
 
 
@@ -407,48 +464,125 @@ def densify_measure(hmp, r, c, cams, ad, lam, window, args):
     return out
 
 
-def cpu_baseline(hmp, steps=1, warmup=0, budget_s=150.0):
-    """The reference's step restated in C (FP32, OpenMP, all host threads) on a bounded
-    sample: each step is one full step of view 0 (640x480) with all 1M Gaussians, and the
-    8-view step time is that view's time scaled by the views' pixel counts.  Runs
-    `warmup` untimed and then `steps` timed samples, fewer when they would exceed
-    budget_s (the count timed is in `sample`)."""
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
-    import oracle as O
-    O.build()
-    c = hmp.config(3)
-    cams = c["cameras"]
-    cam = cams[0]
-    rec = c["records"].copy()
-    m = np.zeros_like(rec)
-    v = np.zeros_like(rec)
-    tgt = np.zeros(cam["width"] * cam["height"] * 3, np.float32) + 0.5
-    lr = [0.025, 0.05, 0.002, 0.005, 0.001, 0.025 / 20]
-    for _ in range(warmup):
-        O.step(cam, rec, m, v, 3, tgt, 0.2, 1, 1, lr, near=c["near"], cap=1024)
-    times = []
-    t_start = time.perf_counter()
-    for k in range(max(1, steps)):
+class CpuReference:
+    """The reference's per-view trainScene step (trainer/gpu.js:915-933) restated in C
+    (oracle/gs_oracle.c: FP32, OpenMP over all host threads, the reference's per-tile cap
+    of 1,024), run over the workload's views with parameters, Adam moments and
+    densification statistics kept across steps.  The reference has no multi-view step:
+    one step over the workload's V views is V of its steps, one per view, each with its
+    own Adam update.  Targets are the workload's own photos (the seed-2 jittered scene
+    rendered by the oracle's FP32 pipeline, quantised to bytes); each step converts its
+    photo's bytes to floats as trainScene does (:921)."""
+    LR = [0.025, 0.05, 0.002, 0.005, 0.001, 0.025 / 20]   # trainScene rates (:891); SH bands lr/20
+
+    def __init__(self, hmp, c, cams):
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle as O
+        O.build()
+        self.O, self.c, self.cams = O, c, cams
+        self.rec = c["records"].copy()
+        self.m = np.zeros_like(self.rec)
+        self.v = np.zeros_like(self.rec)
+        self.stats = np.zeros((self.rec.shape[0], 2), np.float32)
+        jit = hmp.scene.jitter_means(c["records"], 2)
+        self.targets = []
+        for cm in cams:
+            img = O.render_ref(cm, jit, c["degree"], near=c["near"])["image"]
+            self.targets.append(np.round(np.clip(img, 0.0, 1.0) * 255.0).astype(np.uint8))
+        self.t = 1
+        self.view_s = [[] for _ in cams]
+
+    def run(self, views):
+        """Reference steps over `views` (indices), in order; returns the wall seconds."""
         t0 = time.perf_counter()
-        O.step(cam, rec, m, v, 3, tgt, 0.2, 1, k + 1, lr, near=c["near"], cap=1024)
-        times.append(time.perf_counter() - t0)
-        if time.perf_counter() - t_start + times[-1] > budget_s:
-            break
-    dt = statistics.mean(times)
-    px0 = cam["width"] * cam["height"]
-    total = sum(cm["width"] * cm["height"] for cm in cams)
-    step_s = dt * total / px0
-    return dict(value=1.0 / step_s, unit="steps/s", cores=O.num_threads(), kind="port",
-                sample=f"{len(times)} timed reference steps (FP32 C restatement, per-tile cap 1024) on view 0 "
-                       f"(640x480) with all 1,000,000 Gaussians, mean {dt:.3f} s; 8-view step time scaled by "
-                       f"pixel count ({total}/{px0})", samples=len(times))
+        _, secs = self.O.train_views([self.cams[k] for k in views], np.concatenate([self.targets[k] for k in views]),
+                                     self.rec, self.m, self.v, self.c["degree"], self.c["ssim_lambda"],
+                                     self.c["window"], self.t, self.LR, near=self.c["near"], cap=1024,
+                                     stats=self.stats)
+        wall = time.perf_counter() - t0
+        self.t += len(views)
+        for k, sec in zip(views, secs):
+            self.view_s[k].append(float(sec))
+        return wall
+
+    def step_s(self):
+        """Seconds of one step over all views: the sum of each view's mean step time."""
+        return sum(statistics.mean(t) for t in self.view_s)
+
+    def threads(self):
+        return self.O.num_threads()
 
 
-def roofline(res, peaks):
+def cpu_baseline(hmp, c, cams, samples=2):
+    """`samples` timed steps over all of the workload's views (the reference's step run
+    once per view), after one untimed single-view step that pages the buffers in."""
+    ref = CpuReference(hmp, c, cams)
+    ref.run([0])
+    ref.view_s = [[] for _ in cams]
+    walls = [ref.run(list(range(len(cams)))) for _ in range(samples)]
+    return dict(value=1.0 / ref.step_s(), unit="steps/s", cores=ref.threads(), kind="port",
+                sample=(f"{samples} timed steps over all {len(cams)} views of the workload (the reference's "
+                        f"per-view trainScene step restated in C, FP32, per-tile cap 1024, run once per view, "
+                        f"{ref.rec.shape[0]:,} Gaussians), {statistics.mean(walls):.2f} s per step"),
+                samples=samples)
+
+
+def reference_arm(hmp, c, cams, steps, warmup, budget_s=240.0):
+    """--impl reference: `warmup` untimed single-view reference steps (the first pages
+    the buffers in; views in turn), then `steps` timed steps.  A timed step covers all of
+    the workload's views when `steps` of them fit in budget_s (estimated from the
+    warm-up views' times); otherwise each timed step takes the next few views in rotation,
+    and the full step time is the sum of the views' mean times."""
+    ref = CpuReference(hmp, c, cams)
+    V = len(cams)
+    px = [cm["width"] * cm["height"] for cm in cams]
+    for w in range(max(1, warmup)):
+        ref.run([w % V])
+    # Full-step estimate for sizing: a + b px fitted to the warm-up views (the first one,
+    # which pages the buffers in, is left out when others exist).
+    pts = [(px[w % V], ref.view_s[w % V][-1] if w >= V else ref.view_s[w % V][0]) for w in range(max(1, warmup))]
+    pts = pts[1:] if len(pts) > 1 else pts
+    xs = np.array([p[0] for p in pts], np.float64)
+    ys = np.array([p[1] for p in pts], np.float64)
+    if len(set(xs.tolist())) >= 2:
+        b, a = np.polyfit(xs, ys, 1)
+        est_full = max(0.0, a) * V + max(0.0, b) * sum(px)
+    else:
+        est_full = ys.mean() / xs.mean() * sum(px)
+    per_step = V if steps * est_full <= budget_s else max(1, min(V, int(V * budget_s / (steps * est_full))))
+    ref.view_s = [[] for _ in cams]
+    walls = []
+    nxt = 0
+    for _ in range(steps):
+        views = [(nxt + j) % V for j in range(per_step)]
+        nxt = (nxt + per_step) % V
+        walls.append(ref.run(views))
+    missing = [k for k in range(V) if not ref.view_s[k]]
+    for k in missing:  # fewer timed views than the workload has: time the rest once, untimed in `walls`
+        ref.run([k])
+    step_s = ref.step_s()
+    sample = (f"{steps} timed steps of {per_step} of the workload's {V} views each (the reference's per-view "
+              f"trainScene step restated in C, FP32, per-tile cap 1024, {ref.rec.shape[0]:,} Gaussians); "
+              + (f"each timed step covers all {V} views" if per_step == V else
+                 f"the {V}-view step time is the sum of the views' mean step times")
+              + f"; {warmup} untimed single-view warm-up steps")
+    return dict(value=1.0 / step_s, ms_per_step=1000.0 * statistics.mean(walls), step_s=step_s,
+                cores=ref.threads(), sample=sample, views_per_step=per_step)
+
+
+B200_SMS = 148          # SMs of one B200
+SMSP_PER_SM = 4         # warp schedulers per SM, one warp instruction each per clock
+FP32_LANES_PER_SM = 128
+
+
+def roofline(res, peaks, clock_mhz):
     """Roofline of the dominant kernel (the stage with the largest device time: the
     raster backward, one launch per step) against the measured HBM copy bandwidth, with
-    its blends per second; and the same ratio for every stage with an algorithmic byte
-    count."""
+    its blends per second and, for the raster kernels, the roofs that bind them: warp
+    instruction issue (4 per SM per clock) and FP32 throughput (128 lanes x 2 FLOP per
+    SM per clock), from the instructions and FP32 operations per blend that ncu counted
+    on the small capture case (profiles/traffic.json); and the HBM ratio for every stage
+    with an algorithmic byte count."""
     stages = res["stages"]
     steps = max(1, stages["steps"])
     hbm = peaks.get("hbm_gbs", 6650.0)
@@ -463,14 +597,25 @@ def roofline(res, peaks):
         return None, per
     name = max(per, key=lambda k: per[k]["ms"])
     d = per[name]
-    traffic = profiled_traffic(name)
     out = dict(kernel=name, bound="hbm", achieved=d["gbs"], peak=hbm, unit="GB/s", frac=d["frac"],
-               traffic=traffic, bytes_per_launch=d["bytes"], ms_per_launch=d["ms"], peak_source=src)
+               traffic=profiled_traffic(name, d["bytes"]), bytes_per_launch=d["bytes"], ms_per_launch=d["ms"],
+               peak_source=src)
     if name.startswith("raster") and res.get("blends"):
+        bps = res["blends"] / (d["ms"] * 1e-3)
         out["blends_per_launch"] = int(res["blends"])
-        out["blends_per_s"] = float(f"{res['blends'] / (d['ms'] * 1e-3):.4g}")
-        out["note"] = ("issue-bound FP32/ALU kernel (per-pixel alpha blending and its adjoint), "
-                       "not bandwidth-bound: see profiles/raster_bwd_1M_sh3_3views_full.md")
+        out["blends_per_s"] = float(f"{bps:.4g}")
+        pb = profiled_issue(name)
+        clock = (clock_mhz or 1965.0) * 1e6
+        if pb:
+            ipeak = B200_SMS * SMSP_PER_SM * clock
+            fpeak = B200_SMS * FP32_LANES_PER_SM * 2 * clock
+            out["issue"] = dict(inst_per_blend=pb["warp_inst"], achieved=round(bps * pb["warp_inst"] / 1e9, 1),
+                                peak=round(ipeak / 1e9, 1), unit="G warp-inst/s",
+                                frac=round(bps * pb["warp_inst"] / ipeak, 4))
+            out["fp32"] = dict(flop_per_blend=pb["fp32_flop"], achieved=round(bps * pb["fp32_flop"] / 1e12, 2),
+                               peak=round(fpeak / 1e12, 2), unit="TFLOP/s", frac=round(bps * pb["fp32_flop"] / fpeak, 4))
+        out["note"] = ("the raster kernels blend per pixel and reduce per splat: bound by instruction issue, "
+                       "not by HBM (issue and fp32 give those roofs)")
     return out, per
 
 
@@ -480,6 +625,8 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", type=int, default=3, choices=(2, 3, 4),
+                    help="workload: 3 (headline), 2 (200k Gaussians, one 1024x768 view), 4 (3M heavy-tailed, 8 x 1080p)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -516,14 +663,16 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            cb = cpu_baseline(hmp, args.steps, args.warmup)
-            line = dict(metric=METRIC, value=cb["value"], unit="steps/s", n_gpus=args.gpus, steps=cb["samples"],
-                        warmup=args.warmup, ms_per_step=1000.0 / cb["value"], higher_is_better=True, scaling="weak",
+            c, cams = workload(hmp, args.config, 0, world)
+            ra = reference_arm(hmp, c, cams, args.steps, args.warmup)
+            line = dict(metric=METRIC, value=ra["value"], unit="steps/s", n_gpus=args.gpus, steps=args.steps,
+                        warmup=args.warmup, ms_per_step=ra["ms_per_step"], higher_is_better=True, scaling="weak",
                         vs_baseline=None, dtype="f32", data="synthetic", impl="reference",
-                        config=dict(workload=WORKLOAD, gaussians=1_000_000, views=8, pixels=9157632, sh_degree=3,
-                                    near=0.01, ssim_lambda=0.2, window="11-tap gaussian"),
-                        cpu_baseline=cb,
-                        e2e=dict(value=cb["value"], unit="steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+                        config=config_dict(hmp, c, cams, args.config, world),
+                        step_s=ra["step_s"], views_per_timed_step=ra["views_per_step"],
+                        cpu_baseline=dict(value=ra["value"], unit="steps/s", cores=ra["cores"], kind="port",
+                                          sample=ra["sample"]),
+                        e2e=dict(value=ra["value"], unit="steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
             print(json.dumps(line), flush=True)
         return
 
@@ -533,18 +682,16 @@ def main():
         value = world * 1000.0 / ms
         launches = res["stages"]["launches"]
         steps = max(1, res["stages"]["steps"])
-        rl, per_stage = roofline(res, peaks)
+        rl, per_stage = roofline(res, peaks, res["clocks"].get("sm_mhz"))
         line = dict(
             metric=METRIC, value=round(value, 4), unit="steps/s", n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True, scaling="weak",
             vs_baseline=None, dtype="f32", data="synthetic",
-            config=dict(workload=WORKLOAD, gaussians=res["n"], views=res["V"], pixels=res["pixels"], sh_degree=3,
-                        near=0.01, ssim_lambda=0.2, window="11-tap gaussian",
-                        raster_variant=dict(fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1]),
-                                            bwd=dict(batch=res["tuned"]["bwd"][0], pixels_per_thread=res["tuned"]["bwd"][1])),
-                        l2="inputs larger than L2: params+moments+grads 944 MB, pair records 384 MB per step",
-                        parallelism=(f"dp{world}: 8 own views per GPU, gradients summed by one NCCL all-reduce "
-                                     f"per step" if dist else "dp1: one GPU, 8 views")),
+            config=config_dict(hmp, res["c"], res["cams"], args.config, world),
+            raster_variant=dict(fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1]),
+                                bwd=dict(batch=res["tuned"]["bwd"][0], pixels_per_thread=res["tuned"]["bwd"][1])),
+            skipped_steps=res["counts"]["skipped_steps"],
+            overflow=res["counts"]["overflow"],
             plain_steps_per_s=round(res["plain"], 4) if res["plain"] else None,
             plain_direct_steps_per_s=round(res["plain_direct"], 4) if res.get("plain_direct") else None,
             batched_over_plain=round(value / world / res["plain"], 4) if res["plain"] else None,
@@ -566,7 +713,7 @@ def main():
             ps = res["plain_stages"]
             line["plain_stages_ms_per_step"] = {k: round(v / max(1, ps["steps"]), 4) for k, v in ps["ms"].items()}
         if not args.no_cpu and world == 1:
-            line["cpu_baseline"] = cpu_baseline(hmp, steps=3, warmup=0)
+            line["cpu_baseline"] = cpu_baseline(hmp, res["c"], res["cams"])
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -103,6 +103,7 @@ SIGNATURES = {
                                           c_int32, c_int32, VP, ctypes.POINTER(c_float)]),
     "gs_train": (ctypes.c_int, [CTX, c_int32, ctypes.POINTER(GsAdamConfig), VP]),
     "gs_get_step": (ctypes.c_int, [CTX, ctypes.POINTER(c_int32)]),
+    "gs_debug_lookback_wait": (ctypes.c_int, [CTX, c_int32]),
     "gs_train_step_host_async": (ctypes.c_int, [CTX, ctypes.POINTER(GsAdamConfig), ctypes.POINTER(GsLossConfig),
                                                 c_int32, c_int32, VP, VP]),
     "gs_step_gradients": (ctypes.c_int, [CTX, ctypes.POINTER(GsLossConfig), c_int32, c_int32,

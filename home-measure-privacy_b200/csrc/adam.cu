@@ -34,7 +34,7 @@ __device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, flo
 __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
     // Skip the update when this step's instances overflowed -- on every replica at once
     // when the gradients were reduced across replicas (the tail's overflow count).
-    if (a.skip ? (*a.skip > 0.f) : (a.status->overflow != 0u)) return;
+    if (a.skip ? (*a.skip > 0.f) : (a.status->overflow != 0u || a.status->sort_timeout != 0u)) return;
     const int groups = a.n_pad / 4;
     const int units_per_group = a.planes - 3;  // planes other than 6..9, plus one rotation unit
     const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -124,8 +124,9 @@ __global__ void step_end_kernel(DevStatus* st, const double* acc, const ViewDesc
     const float loss = step_loss(acc, views, view_first, num_views, lambda, window);
     st->loss = loss;
     st->nonfinite = isfinite(loss) ? 0 : 1;
-    st->skipped = st->overflow ? 1 : 0;
-    if (advance && !st->overflow) st->step_t += 1;
+    const bool skip = st->overflow || st->sort_timeout;  // truncated lists or unsure sort offsets
+    st->skipped = skip ? 1 : 0;
+    if (advance && !skip) st->step_t += 1;
 }
 
 void launch_step_end(DevStatus* status, const double* acc, const ViewDesc* views, int view_first, int num_views,
@@ -145,7 +146,7 @@ __global__ void grad_tail_kernel(const DevStatus* st, const double* acc, const V
                                  int num_views, float lambda, int window, float* tail) {
     const int t = threadIdx.x;
     if (t == 0) tail[0] = step_loss(acc, views, view_first, num_views, lambda, window) * (float)num_views;
-    else if (t == 1) tail[1] = st->overflow ? 1.f : 0.f;
+    else if (t == 1) tail[1] = (st->overflow || st->sort_timeout) ? 1.f : 0.f;
     else if (t == 2) tail[2] = (float)num_views;
     else if (t < GS_GRAD_TAIL_FLOATS) tail[t] = 0.f;
 }

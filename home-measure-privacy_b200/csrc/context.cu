@@ -150,6 +150,7 @@ struct GsContext {
     int pipe_slot = 0;
     bool status_pending = false;
     int64_t skipped_steps = 0;
+    unsigned int debug_wait_host = 0;   // source of gs_debug_lookback_wait's copy
     // last forward
     int last_first = -1, last_count = 0, last_batched = 1;
     bool have_loss = false;
@@ -514,6 +515,8 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ra.hist = c->hist.as<unsigned long long>();
     ra.totals = c->totals.as<uint32_t>();
     ra.timeout = &c->status.as<DevStatus>()->sort_timeout;
+    ra.debug_wait = &c->status.as<DevStatus>()->debug_wait;
+    ra.never_set = &c->status.as<DevStatus>()->never_set;
     ra.max_parts = (int)(((int64_t)vcount * c->n_pad + radix_tile_items() - 1) / radix_tile_items());
     launch_radix_sort(ra, c->stream, c->num_sms);
     count_launches(c, ST_SORT_PAIRS, 1 + radix_sort_passes(0, 31));
@@ -812,10 +815,20 @@ static int launch_graph(GsContext* c, StepGraph& g) {
 // ---------------------------------------------------------------------------------
 // Capacity: the first forward of a scene/view set measures the key instances it needs.
 // ---------------------------------------------------------------------------------
+// A radix look-back wait that gave up: the step that saw it skipped its update (its
+// tile lists may be wrong).  The flag is cleared once reported, so the context goes on
+// with the next call.
+static int sort_timed_out(GsContext* c) {
+    c->status_host->sort_timeout = 0;
+    CK(cudaMemsetAsync(&c->status.as<DevStatus>()->sort_timeout, 0, sizeof(unsigned int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return fail(GS_ERR_CUDA, "radix sort look-back wait timed out; the step's update was skipped");
+}
+
 static int read_status(GsContext* c) {
     CK(cudaMemcpyAsync(c->status_host, c->status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    if (c->status_host->sort_timeout) return fail(GS_ERR_CUDA, "radix sort look-back wait timed out");
+    if (c->status_host->sort_timeout) return sort_timed_out(c);
     return GS_OK;
 }
 
@@ -1482,7 +1495,7 @@ static int poll_status(GsContext* c, bool wait) {
         return GS_OK;
     }
     c->status_pending = false;
-    if (c->status_host->sort_timeout) return fail(GS_ERR_CUDA, "radix sort look-back wait timed out");
+    if (c->status_host->sort_timeout) return sort_timed_out(c);
     if (c->status_host->overflow) {
         c->skipped_steps++;
         CKI(grow_instances(c, c->status_host->instances_needed));
@@ -1727,6 +1740,16 @@ int gs_get_step(GsContext* c, int32_t* t_out) {
     if (!t_out) return fail(GS_ERR_INVALID_ARG, "t_out is null");
     CKI(read_status(c));
     *t_out = c->status_host->step_t;
+    return GS_OK;
+}
+
+int gs_debug_lookback_wait(GsContext* c, int32_t polls) {
+    CTX_CHECK(c);
+    if (polls < 0) return fail(GS_ERR_INVALID_ARG, "polls must be >= 0");
+    c->debug_wait_host = (unsigned int)polls;
+    CK(cudaMemcpyAsync(&c->status.as<DevStatus>()->debug_wait, &c->debug_wait_host, sizeof(unsigned int),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return GS_OK;
 }
 

@@ -27,7 +27,7 @@ constexpr int DN_THREADS = 256;
 
 __global__ void stats_commit_kernel(float* __restrict__ stats, const float* __restrict__ step, int n_pad,
                                     const DevStatus* status, const float* skip) {
-    if (skip ? (*skip > 0.f) : (status->overflow != 0u)) return;
+    if (skip ? (*skip > 0.f) : (status->overflow != 0u || status->sort_timeout != 0u)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 2 * n_pad) return;
     const float v = step[i];

@@ -51,7 +51,9 @@ struct DevStatus {
     float loss;                           // mean loss of the last step over its views
     int nonfinite;                        // last loss was not finite
     unsigned int sort_timeout;            // a radix look-back wait gave up (never expected)
-    unsigned int pad[5];
+    unsigned int debug_wait;              // test hook: polls of an extra wait in each sort pass (0 = off)
+    unsigned int never_set;               // the word that extra wait polls: no code writes it
+    unsigned int pad[3];
 };
 #define GS_STATUS_FORWARD_BYTES 24
 

@@ -92,6 +92,9 @@ struct RadixSortArgs {
     uint32_t* totals;        // digit counts and offsets of every pass, partition counters (>= 2053 words)
     int max_parts;
     unsigned int* timeout;   // set when a look-back wait gave up
+    const unsigned int* debug_wait;  // test hook (device word): partition 1 of every pass first
+                                     // polls *never_set this many times, then gives up
+    const unsigned int* never_set;
 };
 int radix_sort_passes(int begin_bit, int end_bit);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms);

@@ -1,9 +1,7 @@
 // Loss gradient that allocates nothing: gs_loss_gradient_noalloc (include/gsb200.h).
 //
 // Some callers cannot allocate device memory: an engine that owns every byte of the
-// GPU through its own pool, a path recorded into a CUDA graph by the caller (where a
-// cudaMalloc would break the capture), or a real-time loop that must not stall on the
-// allocator.  They pass device buffers for the inputs and outputs; the little scratch
+// GPU through its own pool, or a real-time loop that must not stall on the allocator.  They pass device buffers for the inputs and outputs; the little scratch
 // the loss kernel needs besides them -- the images' view descriptors and the per-image
 // sums of |x - y| and SSIM -- lives in the file-scope array below, sized for at most
 // GS_NOALLOC_MAX_IMAGES images per call.  Every GPU that loads the library holds the
@@ -14,6 +12,8 @@
 // the array and it keeps the last call's contents, so every call clears what must start
 // at zero, and calls that overlap on the GPU (different streams, or different host
 // threads on one device) race on it.
+#include <atomic>
+
 #include "../../include/gsb200.h"
 #include "internal.h"
 
@@ -56,7 +56,10 @@ __global__ void noalloc_loss_kernel(const NoallocScratch* s, int count, float la
 
 using namespace gs;
 
-static NoallocScratch* g_scratch_addr[GS_MAX_VIEWS] = {};
+// Device address of the array, per device ordinal; looked up on the first call on each
+// device.  Threads racing on that first call store the same address.
+constexpr int GS_NOALLOC_MAX_DEVICES = 64;
+static std::atomic<NoallocScratch*> g_scratch_addr[GS_NOALLOC_MAX_DEVICES];
 
 extern "C" GS_API int gs_loss_gradient_noalloc(const float* image, const float* target, int32_t num_images,
                                                int32_t width, int32_t height, float ssim_lambda, int32_t window,
@@ -66,14 +69,18 @@ extern "C" GS_API int gs_loss_gradient_noalloc(const float* image, const float* 
     if (width < 1 || height < 1 || width > 16384 || height > 16384) return GS_ERR_INVALID_ARG;
     if ((long long)width * height * num_images * 3 > 0x7fffffffLL) return GS_ERR_CAPACITY;
     if (!(ssim_lambda >= 0.f && ssim_lambda <= 1.f) || (window != 0 && window != 1)) return GS_ERR_INVALID_ARG;
+    // An error the caller's own work left pending stays the caller's: report it without
+    // clearing it, before launching anything.
+    if (cudaPeekAtLastError() != cudaSuccess) return GS_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return GS_ERR_NO_DEVICE;
     }
-    if (dev < 0 || dev >= GS_MAX_VIEWS) return GS_ERR_INVALID_ARG;
+    if (dev < 0 || dev >= GS_NOALLOC_MAX_DEVICES) return GS_ERR_INVALID_ARG;
     // Once per device, with that device current: the array's device address.
-    if (!g_scratch_addr[dev]) {
+    NoallocScratch* s = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!s) {
         void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
             cudaGetLastError();
@@ -83,9 +90,9 @@ extern "C" GS_API int gs_loss_gradient_noalloc(const float* image, const float* 
             cudaGetLastError();
             return GS_ERR_CUDA;
         }
-        g_scratch_addr[dev] = reinterpret_cast<NoallocScratch*>(p);
+        s = reinterpret_cast<NoallocScratch*>(p);
+        g_scratch_addr[dev].store(s, std::memory_order_release);
     }
-    NoallocScratch* s = g_scratch_addr[dev];
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     NoallocViews views;
     memset(&views, 0, sizeof views);

@@ -176,7 +176,8 @@ template <typename W>
 __global__ void __launch_bounds__(OS_THREADS, 4) radix_onesweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ gex,
-    W* look, uint32_t* counter, unsigned int* timeout) {
+    W* look, uint32_t* counter, unsigned int* timeout, const unsigned int* debug_wait,
+    const unsigned int* never_set) {
     using LW = LookWord<W>;
     __shared__ uint32_t s_keys[RS_TILE];
     __shared__ uint32_t s_vals[RS_TILE];
@@ -278,6 +279,19 @@ __global__ void __launch_bounds__(OS_THREADS, 4) radix_onesweep(
         const uint32_t idx = warp_start + j * 32 + lane;
         v[j] = (idx < n) ? (vals_in ? __ldg(vals_in + base + idx) : base + idx) : 0u;
     }
+    if (p == 1 && d == 0 && debug_wait) {
+        // Failure-detection test hook: a wait on a word nothing writes, given up after the
+        // armed number of polls exactly as a look-back wait gives up (the flag is set and
+        // the block carries on; the look-back below still finds the true offsets).
+        const uint32_t polls = ld_relaxed(debug_wait);
+        for (uint32_t s = 0; polls && ld_relaxed(never_set) == 0u; s++) {
+            if (s >= polls) {
+                atomicOr(timeout, 1u);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
     if (p > 0 && owner) {
         // Walk back OS_LOOK partitions per round trip: sum published counts until an
         // inclusive prefix; re-poll from the first partition that has published nothing.
@@ -358,13 +372,13 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(unsigned long long), s);
             radix_onesweep<unsigned long long><<<grid, OS_THREADS, 0, s>>>(
                 kb[in], vin, kb[out], vb[out], a.seg, a.begin_bit + p * step, gex + p * 256,
-                reinterpret_cast<unsigned long long*>(a.hist), counters + p, a.timeout);
+                reinterpret_cast<unsigned long long*>(a.hist), counters + p, a.timeout, a.debug_wait, a.never_set);
         } else {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
             radix_onesweep<uint32_t><<<grid, OS_THREADS, 0, s>>>(kb[in], vin, kb[out], vb[out], a.seg,
                                                                   a.begin_bit + p * step, gex + p * 256,
                                                                   reinterpret_cast<uint32_t*>(a.hist), counters + p,
-                                                                  a.timeout);
+                                                                  a.timeout, a.debug_wait, a.never_set);
         }
     }
 }

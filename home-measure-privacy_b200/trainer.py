@@ -463,6 +463,12 @@ class Renderer:
     def synchronize(self):
         N.check(self.lib.gs_synchronize(self.ctx))
 
+    def debug_lookback_wait(self, polls):
+        """Failure-detection hook: every radix pass first makes one block wait `polls`
+        polls on a word nothing writes, then give up as a stuck look-back wait would
+        (0 = off); see gs_debug_lookback_wait."""
+        N.check(self.lib.gs_debug_lookback_wait(self.ctx, int(polls)))
+
     def autotune(self, cache_path=None):
         """Picks the raster variants; returns {fwd: (batch, ppt), bwd: (batch, ppt)}."""
         N.check(self.lib.gs_autotune(self.ctx, cache_path.encode() if cache_path else None))

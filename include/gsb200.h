@@ -362,6 +362,16 @@ GS_API int gs_scene_extent(const GsCamera* cams, int32_t count, float* extent_ou
 /* Step counter t (number of Adam updates applied since gs_set_gaussians). */
 GS_API int gs_get_step(GsContext* ctx, int32_t* t_out);
 
+/* Failure-detection hook (no counterpart in the reference, whose WebGPU kernels never
+ * wait on one another).  The radix sort's decoupled look-back is the one place where a
+ * block waits for another; each such wait gives up after a bounded number of polls,
+ * sets a flag and lets the block finish, the step then skips its Adam update, and the
+ * call that reads the step's status returns GS_ERR_CUDA ("look-back wait timed out")
+ * and clears the flag so the context goes on.  With polls > 0 every radix pass run on
+ * this context first makes one block wait on a device word that nothing writes, giving
+ * up after `polls` polls: the same path, on demand, with no fault.  0 turns it off. */
+GS_API int gs_debug_lookback_wait(GsContext* ctx, int32_t polls);
+
 /* ---- memory, timing and diagnostics ---------------------------------------------- */
 
 /* Page-locked host memory for per-step uploads (freed with gs_host_free). */
@@ -432,9 +442,8 @@ GS_API int gs_autotune(GsContext* ctx, const char* cache_path);
 
 /* ---- loss gradient without allocation ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device memory: an
- * engine that hands out all GPU memory from its own pool, code being recorded into a
- * CUDA graph by the caller (a cudaMalloc would end the capture), or a real-time loop
- * that must not wait on the allocator.  Same result as gs_loss_gradient for each image,
+ * engine that hands out all GPU memory from its own pool (memory it did not hand out
+ * does not exist for it), or a real-time loop that must not wait on the allocator.  Same result as gs_loss_gradient for each image,
  * but image, target, grad and loss are caller-owned DEVICE buffers and the call only
  * queues work on `stream` (a cudaStream_t; NULL = the legacy default stream): read the
  * outputs after synchronising it.  num_images images of width x height (RGB floats,
@@ -447,8 +456,10 @@ GS_API int gs_autotune(GsContext* ctx, const char* cache_path);
  * raises the loss kernel's shared-memory limit), so make the first call on each device
  * outside any stream capture.  All calls share the array and it keeps the last call's
  * contents; each call clears the sums it accumulates, and calls that overlap on the GPU
- * (other streams or host threads on the same device) race on it.  Returns GS_OK or a
- * status code; it does not set gs_last_error. */
+ * (other streams or host threads on the same device) race on it.  A CUDA error already
+ * pending on the calling thread (left by the caller's own work) is left pending and the
+ * call returns GS_ERR_CUDA without launching anything.  Returns GS_OK or a status code;
+ * it does not set gs_last_error. */
 #define GS_NOALLOC_MAX_IMAGES 8
 #define GS_NOALLOC_SCRATCH_BYTES 4096
 GS_API int gs_loss_gradient_noalloc(const float* image, const float* target, int32_t num_images,

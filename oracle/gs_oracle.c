@@ -259,6 +259,92 @@ static int cmp_depth_idx(const void* pa, const void* pb) {
     return (a->idx > b->idx) - (a->idx < b->idx);
 }
 
+/* Per-tile buckets of BIN + SORT: each tile's entries (depth, splat index), first filled
+ * in splat-index order, then the first min(count, cap) of them sorted by (depth, index).
+ * The rectangles and the per-tile sorts run in parallel; the fill is sequential, so the
+ * bucket order (and with it which entries a cap keeps) does not depend on threads. */
+typedef struct {
+    DepthIdx* buf;
+    int64_t* start;
+    int64_t* count;   /* entries kept per tile (capped) */
+    int64_t total;    /* sum of count */
+    int tiles;
+} Bins;
+
+static void bins_build(Bins* b, const float* splats, int n, int W, int H, int rect_mode, int cap) {
+    const int tx = (W + 15) / 16, ty = (H + 15) / 16, tiles = tx * ty;
+    int32_t* rect = (int32_t*)malloc(sizeof(int32_t) * 4 * (size_t)(n > 0 ? n : 1));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) {
+        const float* s = splats + (size_t)i * 12;
+        int32_t* r = rect + (size_t)i * 4;
+        if (s[11] < 0.5f) {
+            r[0] = r[1] = r[2] = r[3] = 0;
+            continue;
+        }
+        int x0, x1, y0, y1;
+        rect32(s[0], s[1], s[6], tx, ty, rect_mode, &x0, &x1, &y0, &y1);
+        r[0] = x0; r[1] = x1; r[2] = y0; r[3] = y1;
+    }
+    int64_t* all = (int64_t*)calloc((size_t)tiles + 1, sizeof(int64_t));
+    for (int i = 0; i < n; i++) {
+        const int32_t* r = rect + (size_t)i * 4;
+        for (int y = r[2]; y < r[3]; y++)
+            for (int x = r[0]; x < r[1]; x++) all[y * tx + x]++;
+    }
+    b->tiles = tiles;
+    b->start = (int64_t*)calloc((size_t)tiles + 1, sizeof(int64_t));
+    b->count = (int64_t*)calloc((size_t)tiles + 1, sizeof(int64_t));
+    int64_t run = 0;
+    b->total = 0;
+    for (int t = 0; t < tiles; t++) {
+        b->start[t] = run;
+        run += all[t];
+        b->count[t] = (cap > 0 && all[t] > cap) ? cap : all[t];
+        b->total += b->count[t];
+    }
+    b->buf = (DepthIdx*)malloc(sizeof(DepthIdx) * (size_t)(run > 0 ? run : 1));
+    memset(all, 0, sizeof(int64_t) * ((size_t)tiles + 1));
+    for (int i = 0; i < n; i++) {
+        const int32_t* r = rect + (size_t)i * 4;
+        const DepthIdx e = {splats[(size_t)i * 12 + 7], (uint32_t)i};
+        for (int y = r[2]; y < r[3]; y++)
+            for (int x = r[0]; x < r[1]; x++) {
+                const int t = y * tx + x;
+                b->buf[b->start[t] + all[t]++] = e;
+            }
+    }
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int t = 0; t < tiles; t++) qsort(b->buf + b->start[t], (size_t)b->count[t], sizeof(DepthIdx), cmp_depth_idx);
+    free(all);
+    free(rect);
+}
+
+static void bins_free(Bins* b) {
+    free(b->buf);
+    free(b->start);
+    free(b->count);
+}
+
+/* Compact list, [start, end) per tile and (optional) keys tile << 32 | depth bits. */
+static void bins_write(const Bins* b, uint32_t* list_out, uint32_t* ranges_out, uint64_t* keys_out) {
+    int64_t pos = 0;
+    for (int t = 0; t < b->tiles; t++) {
+        ranges_out[2 * t] = (uint32_t)pos;
+        pos += b->count[t];
+        ranges_out[2 * t + 1] = (uint32_t)pos;
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int t = 0; t < b->tiles; t++) {
+        int64_t o = ranges_out[2 * t];
+        for (int64_t k = 0; k < b->count[t]; k++, o++) {
+            const DepthIdx e = b->buf[b->start[t] + k];
+            if (list_out) list_out[o] = e.idx;
+            if (keys_out) keys_out[o] = ((uint64_t)t << 32) | float_bits(e.depth);
+        }
+    }
+}
+
 /* BIN + SORT (trainer/gpu.js:616-685) or tileLists (:450-481): per tile, the valid splats
  * whose rectangle covers it, in (depth, splat index) order.  cap > 0 keeps the first
  * `cap` splats of a tile in splat-index order (the reference keeps the first `cap` to
@@ -267,61 +353,15 @@ static int cmp_depth_idx(const void* pa, const void* pb) {
  * the entry count, or -(needed) when list_cap is too small. */
 EXPORT int64_t orc32_bin(const float* splats, int n, int W, int H, int rect_mode, int cap, uint32_t* list_out,
                          uint32_t* ranges_out, uint64_t* keys_out, int64_t list_cap) {
-    const int tx = (W + 15) / 16, ty = (H + 15) / 16, tiles = tx * ty;
-    int64_t* counts = (int64_t*)calloc((size_t)tiles + 1, sizeof(int64_t));
-    for (int i = 0; i < n; i++) {
-        const float* s = splats + (size_t)i * 12;
-        if (s[11] < 0.5f) continue;
-        int x0, x1, y0, y1;
-        rect32(s[0], s[1], s[6], tx, ty, rect_mode, &x0, &x1, &y0, &y1);
-        for (int y = y0; y < y1; y++)
-            for (int x = x0; x < x1; x++) counts[y * tx + x]++;
-    }
-    int64_t total = 0;
-    for (int t = 0; t < tiles; t++) total += (cap > 0 && counts[t] > cap) ? cap : counts[t];
+    Bins b;
+    bins_build(&b, splats, n, W, H, rect_mode, cap);
+    const int64_t total = b.total;
     if (total > list_cap) {
-        free(counts);
+        bins_free(&b);
         return -total;
     }
-    /* Per-tile buckets in splat-index order, then a stable per-tile depth sort. */
-    int64_t* start = (int64_t*)calloc((size_t)tiles + 1, sizeof(int64_t));
-    int64_t* fill = (int64_t*)calloc((size_t)tiles + 1, sizeof(int64_t));
-    int64_t all = 0;
-    for (int t = 0; t < tiles; t++) {
-        start[t] = all;
-        all += counts[t];
-    }
-    DepthIdx* buf = (DepthIdx*)malloc(sizeof(DepthIdx) * (size_t)(all > 0 ? all : 1));
-    for (int i = 0; i < n; i++) {
-        const float* s = splats + (size_t)i * 12;
-        if (s[11] < 0.5f) continue;
-        int x0, x1, y0, y1;
-        rect32(s[0], s[1], s[6], tx, ty, rect_mode, &x0, &x1, &y0, &y1);
-        for (int y = y0; y < y1; y++)
-            for (int x = x0; x < x1; x++) {
-                const int t = y * tx + x;
-                DepthIdx e = {s[7], (uint32_t)i};
-                buf[start[t] + fill[t]++] = e;
-            }
-    }
-    int64_t pos = 0;
-    for (int t = 0; t < tiles; t++) {
-        int64_t cnt = counts[t];
-        if (cap > 0 && cnt > cap) cnt = cap;
-        qsort(buf + start[t], (size_t)cnt, sizeof(DepthIdx), cmp_depth_idx);
-        ranges_out[2 * t] = (uint32_t)pos;
-        for (int64_t k = 0; k < cnt; k++) {
-            const DepthIdx e = buf[start[t] + k];
-            if (list_out) list_out[pos] = e.idx;
-            if (keys_out) keys_out[pos] = ((uint64_t)t << 32) | float_bits(e.depth);
-            pos++;
-        }
-        ranges_out[2 * t + 1] = (uint32_t)pos;
-    }
-    free(buf);
-    free(fill);
-    free(start);
-    free(counts);
+    bins_write(&b, list_out, ranges_out, keys_out);
+    bins_free(&b);
     return total;
 }
 
@@ -585,36 +625,58 @@ EXPORT void orc32_adam(float* params, const float* grads, float* m, float* v, in
     }
 }
 
-/* One training step of the reference's trainScene for one view (trainer/gpu.js:919-933):
- * preprocess, BIN + SORT (cap as given), forward, loss gradient, backward, SHAPE by
- * finite differences, Adam.  Colour grads for SH bands >= 1 come from the colour grad
- * and the basis (the extension above).  target: RGB floats.  Returns the step's loss.
- * Scratch buffers are allocated per call. */
-EXPORT double orc32_step(const OrcCamera* cam, float* params, float* m, float* v, int n, int degree, const float* target,
-                         float lambda, int window, int t, const float* lr, float near, int cap) {
+/* Buffers of the per-view step, sized for the largest view and reused across steps
+ * (the reference keeps its step buffers in a scratch pool, trainer/gpu.js:764-772). */
+typedef struct {
+    float *splats, *image, *state, *dl, *g16, *shape, *grads, *target;
+    size_t npx_cap;
+} StepWork;
+
+static void work_init(StepWork* w, int n, int S, size_t npx) {
+    w->splats = (float*)malloc(sizeof(float) * 12 * (size_t)n);
+    w->g16 = (float*)malloc(sizeof(float) * 16 * (size_t)n);
+    w->shape = (float*)malloc(sizeof(float) * 10 * (size_t)n);
+    w->grads = (float*)malloc(sizeof(float) * (size_t)S * n);
+    w->image = (float*)malloc(sizeof(float) * npx * 3);
+    w->state = (float*)malloc(sizeof(float) * npx * 2);
+    w->dl = (float*)malloc(sizeof(float) * npx * 3);
+    w->target = (float*)malloc(sizeof(float) * npx * 3);
+    w->npx_cap = npx;
+}
+
+static void work_free(StepWork* w) {
+    free(w->splats); free(w->g16); free(w->shape); free(w->grads);
+    free(w->image); free(w->state); free(w->dl); free(w->target);
+}
+
+/* One step of trainScene on one view (trainer/gpu.js:915-933): PREPROCESS, BIN + SORT
+ * (cap as given), FORWARD, loss gradient, BACKWARD, SHAPE by finite differences, STATS
+ * (optional, :484-497) and ADAM at step t.  Colour grads of SH bands >= 1 come from the
+ * colour grad and the basis (the extension above).  target: RGB floats. */
+static double step_view(StepWork* w, const OrcCamera* cam, float* params, float* m, float* v, float* stats, int n,
+                        int degree, const float* target, float lambda, int window, int t, const float* lr, float near,
+                        int cap) {
     const int W = cam->width, H = cam->height, S = orc_stride(degree), NK = nk_of(degree);
-    const size_t npx = (size_t)W * H;
-    const int tiles = ((W + 15) / 16) * ((H + 15) / 16);
-    float* splats = (float*)malloc(sizeof(float) * 12 * (size_t)n);
-    orc32_preprocess(cam, params, n, degree, near, 0.3f, splats);
-    int64_t need = -orc32_bin(splats, n, W, H, 0, cap, NULL, (uint32_t*)calloc((size_t)tiles * 2, 4), NULL, 0);
-    uint32_t* ranges = (uint32_t*)calloc((size_t)tiles * 2, 4);
-    uint32_t* list = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(need > 0 ? need : 1));
-    orc32_bin(splats, n, W, H, 0, cap, list, ranges, NULL, need);
-    float* image = (float*)malloc(sizeof(float) * npx * 3);
-    float* state = (float*)malloc(sizeof(float) * npx * 2);
-    float* dl = (float*)malloc(sizeof(float) * npx * 3);
-    orc32_forward(splats, list, ranges, W, H, 0.99f, 1.0f / 255.0f, 1e-4f, image, state);
+    orc32_preprocess(cam, params, n, degree, near, 0.3f, w->splats);
+    Bins b;
+    bins_build(&b, w->splats, n, W, H, 0, cap);
+    uint32_t* ranges = (uint32_t*)malloc(sizeof(uint32_t) * 2 * (size_t)b.tiles);
+    uint32_t* list = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(b.total > 0 ? b.total : 1));
+    bins_write(&b, list, ranges, NULL);
+    bins_free(&b);
+    orc32_forward(w->splats, list, ranges, W, H, 0.99f, 1.0f / 255.0f, 1e-4f, w->image, w->state);
     double loss = 0.0;
-    orc32_loss_grad(image, target, W, H, lambda, window, dl, &loss);
-    float* g16 = (float*)calloc((size_t)n * 16, sizeof(float));
-    orc32_backward(splats, list, ranges, state, dl, W, H, 0.99f, 1.0f / 255.0f, g16);
-    float* shape = (float*)malloc(sizeof(float) * 10 * (size_t)n);
-    orc32_shape_fd(cam, params, n, degree, near, 0.3f, g16, shape);
-    float* grads = (float*)calloc((size_t)n * S, sizeof(float));
+    orc32_loss_grad(w->image, target, W, H, lambda, window, w->dl, &loss);
+    memset(w->g16, 0, sizeof(float) * 16 * (size_t)n);
+    orc32_backward(w->splats, list, ranges, w->state, w->dl, W, H, 0.99f, 1.0f / 255.0f, w->g16);
+    orc32_shape_fd(cam, params, n, degree, near, 0.3f, w->g16, w->shape);
     const float* vm = cam->view;
     float campos[3];
     for (int j = 0; j < 3; j++) campos[j] = -(vm[0 + j] * vm[3] + vm[4 + j] * vm[7] + vm[8 + j] * vm[11]);
+    float* grads = w->grads;
+    const float* g16 = w->g16;
+    const float* shape = w->shape;
+    const float* splats = w->splats;
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; i++) {
         float* g = grads + (size_t)i * S;
@@ -630,10 +692,66 @@ EXPORT double orc32_step(const OrcCamera* cam, float* params, float* m, float* v
             for (int c = 0; c < 3; c++)
                 for (int k = 0; k < NK; k++) g[14 + c * NK + k] = Y[k] * g16[(size_t)i * 16 + c];
         }
+        if (stats && splats[(size_t)i * 12 + 11] >= 0.5f) {
+            const float gu = g16[(size_t)i * 16 + 4], gv = g16[(size_t)i * 16 + 5];
+            stats[(size_t)i * 2] += sqrtf(gu * gu + gv * gv);
+            stats[(size_t)i * 2 + 1] += 1.0f;
+        }
     }
     orc32_adam(params, grads, m, v, n, degree, t, lr, 0.9f, 0.999f, 1e-8f);
-    free(grads); free(shape); free(g16); free(dl); free(state); free(image); free(list); free(ranges); free(splats);
+    free(list);
+    free(ranges);
     return loss;
+}
+
+/* One training step of the reference's trainScene for one view (in place on params, m,
+ * v); returns the step's loss.  target: RGB floats. */
+EXPORT double orc32_step(const OrcCamera* cam, float* params, float* m, float* v, int n, int degree, const float* target,
+                         float lambda, int window, int t, const float* lr, float near, int cap) {
+    StepWork w;
+    work_init(&w, n, orc_stride(degree), (size_t)cam->width * cam->height);
+    const double loss = step_view(&w, cam, params, m, v, NULL, n, degree, target, lambda, window, t, lr, near, cap);
+    work_free(&w);
+    return loss;
+}
+
+/* trainScene (trainer/gpu.js:894-933) over `nviews` views in the given order, one
+ * reference step per view (steps t0, t0 + 1, ...): each step converts the view's RGB
+ * bytes to floats (v / 255, :921), then runs the per-view step above with STATS into
+ * `stats` (n x 2, optional).  targets_u8: the views' photos concatenated.  losses_out
+ * (optional) gets each step's loss, seconds_out (optional) each step's wall time.  Buffers
+ * are allocated once for all the steps. */
+EXPORT void orc32_train_views(const OrcCamera* cams, int nviews, const uint8_t* targets_u8, float* params, float* m,
+                              float* v, float* stats, int n, int degree, float lambda, int window, int t0,
+                              const float* lr, float near, int cap, double* losses_out, double* seconds_out) {
+    size_t npx_max = 0;
+    for (int k = 0; k < nviews; k++) {
+        const size_t npx = (size_t)cams[k].width * cams[k].height;
+        if (npx > npx_max) npx_max = npx;
+    }
+    StepWork w;
+    work_init(&w, n, orc_stride(degree), npx_max > 0 ? npx_max : 1);
+    size_t off = 0;
+    for (int k = 0; k < nviews; k++) {
+        const size_t cnt = (size_t)cams[k].width * cams[k].height * 3;
+#ifdef _OPENMP
+        const double t_start = omp_get_wtime();
+#endif
+        const uint8_t* src = targets_u8 + off;
+        float* dst = w.target;
+#pragma omp parallel for schedule(static)
+        for (long long j = 0; j < (long long)cnt; j++) dst[j] = (float)((double)src[j] / 255.0);  /* JS: f64, then f32 */
+        const double loss =
+            step_view(&w, &cams[k], params, m, v, stats, n, degree, w.target, lambda, window, t0 + k, lr, near, cap);
+        if (losses_out) losses_out[k] = loss;
+#ifdef _OPENMP
+        if (seconds_out) seconds_out[k] = omp_get_wtime() - t_start;
+#else
+        if (seconds_out) seconds_out[k] = 0.0;
+#endif
+        off += cnt;
+    }
+    work_free(&w);
 }
 
 EXPORT int orc_num_threads(void) {
@@ -825,11 +943,22 @@ static uint64_t fnv(uint64_t h, uint64_t v) {
     return h;
 }
 
+/* Candidate grid of the FP64 render: for each 16 x 16 block of pixels, the positions k
+ * (into `order`, ascending) of the valid splats whose bounding square |dx|, |dy| <= radius
+ * can reach a pixel of the block (with a one-pixel margin).  Every other splat fails
+ * alpha64's box test at every pixel of the block, so walking a block's candidates in
+ * order gives the same contributors as walking all valid splats. */
+#define D64_BLOCK 16
+
 typedef struct {
     int n, W, H;
     P64* P;
     int* order;   /* valid splats by (depth, index) */
     int nvalid;
+    int nbx, nby;
+    int64_t* cand_start;  /* [blocks + 1] */
+    int* cand;            /* positions k into order */
+    int64_t cand_max;     /* longest block list */
 } Scene64;
 
 static void scene64(Scene64* sc, const OrcCamera* cam, const double* params, int n, int degree, double near, double dil) {
@@ -853,11 +982,56 @@ static void scene64(Scene64* sc, const OrcCamera* cam, const double* params, int
     for (int k = 0; k < nv; k++) sc->order[k] = tmp[k].idx;
     sc->nvalid = nv;
     free(tmp);
+    const int nbx = (sc->W + D64_BLOCK - 1) / D64_BLOCK, nby = (sc->H + D64_BLOCK - 1) / D64_BLOCK;
+    const int blocks = nbx * nby;
+    sc->nbx = nbx;
+    sc->nby = nby;
+    int* rect = (int*)malloc(sizeof(int) * 4 * (size_t)(nv > 0 ? nv : 1));
+    int64_t* cnt = (int64_t*)calloc((size_t)blocks + 1, sizeof(int64_t));
+    for (int k = 0; k < nv; k++) {
+        const P64* q = &sc->P[sc->order[k]];
+        /* pixel x passes |x + 0.5 - u| <= r only for x in [u - r - 0.5, u + r - 0.5] */
+        double bx0 = floor((q->u - q->radius - 1.5) / D64_BLOCK), bx1 = floor((q->u + q->radius + 0.5) / D64_BLOCK);
+        double by0 = floor((q->v - q->radius - 1.5) / D64_BLOCK), by1 = floor((q->v + q->radius + 0.5) / D64_BLOCK);
+        bx0 = fmax(bx0, 0.0); by0 = fmax(by0, 0.0);
+        bx1 = fmin(bx1, (double)(nbx - 1)); by1 = fmin(by1, (double)(nby - 1));
+        int* r = rect + (size_t)k * 4;
+        if (!(bx0 <= bx1 && by0 <= by1)) {
+            r[0] = r[1] = r[2] = r[3] = 0;
+            continue;
+        }
+        r[0] = (int)bx0; r[1] = (int)bx1 + 1; r[2] = (int)by0; r[3] = (int)by1 + 1;
+        for (int by = r[2]; by < r[3]; by++)
+            for (int bx = r[0]; bx < r[1]; bx++) cnt[by * nbx + bx]++;
+    }
+    sc->cand_start = (int64_t*)malloc(sizeof(int64_t) * ((size_t)blocks + 1));
+    int64_t run = 0;
+    sc->cand_max = 0;
+    for (int b = 0; b < blocks; b++) {
+        sc->cand_start[b] = run;
+        run += cnt[b];
+        if (cnt[b] > sc->cand_max) sc->cand_max = cnt[b];
+        cnt[b] = 0;
+    }
+    sc->cand_start[blocks] = run;
+    sc->cand = (int*)malloc(sizeof(int) * (size_t)(run > 0 ? run : 1));
+    for (int k = 0; k < nv; k++) {
+        const int* r = rect + (size_t)k * 4;
+        for (int by = r[2]; by < r[3]; by++)
+            for (int bx = r[0]; bx < r[1]; bx++) {
+                const int b = by * nbx + bx;
+                sc->cand[sc->cand_start[b] + cnt[b]++] = k;
+            }
+    }
+    free(cnt);
+    free(rect);
 }
 
 static void scene64_free(Scene64* sc) {
     free(sc->P);
     free(sc->order);
+    free(sc->cand_start);
+    free(sc->cand);
 }
 
 static inline double alpha64(const P64* s, double px, double py, double amax, double amin, double* dx, double* dy,
@@ -877,9 +1051,9 @@ static inline double alpha64(const P64* s, double px, double py, double amax, do
     return a;
 }
 
-/* FP64 render.  Every pixel walks all valid splats in (depth, index) order (equal to
- * walking its tile's list: the tile rectangle contains every pixel that passes the
- * bounding-box test).  signature: a hash of every discrete decision (validity, radius,
+/* FP64 render.  Every pixel walks the valid splats in (depth, index) order, skipping only
+ * those whose bounding square cannot reach it (the candidate grid above; the result is
+ * that of walking all of them).  signature: a hash of every discrete decision (validity, radius,
  * contributors, clamps, stop points) so finite differences can skip kinks. */
 EXPORT void d64_render(const OrcCamera* cam, const double* params, int n, int degree, double near, double dil,
                        double amax, double amin, double tmin, double* image, uint64_t* signature) {
@@ -895,11 +1069,11 @@ EXPORT void d64_render(const OrcCamera* cam, const double* params, int n, int de
         for (int x = 0; x < W; x++) {
             const double px = x + 0.5, py = y + 0.5;
             double T = 1.0, rgb[3] = {0, 0, 0};
-            for (int k = 0; k < sc.nvalid; k++) {
-                if (T <= tmin) {
-                    hr = fnv(hr, 0xfeedull + (uint64_t)k);
-                    break;
-                }
+            const int blk = (y / D64_BLOCK) * sc.nbx + x / D64_BLOCK;
+            int klast = -1;
+            for (int64_t j = sc.cand_start[blk]; j < sc.cand_start[blk + 1]; j++) {
+                if (T <= tmin) break;
+                const int k = sc.cand[j];
                 const P64* s = &sc.P[sc.order[k]];
                 double dx, dy;
                 int cl = 0;
@@ -908,7 +1082,11 @@ EXPORT void d64_render(const OrcCamera* cam, const double* params, int n, int de
                 hr = fnv(hr, (uint64_t)sc.order[k] * 2 + (uint64_t)cl);
                 for (int c = 0; c < 3; c++) rgb[c] += s->rgb[c] * a * T;
                 T *= 1.0 - a;
+                klast = k;
             }
+            /* stop point: the walk over all valid splats stops at the one after the
+             * last contributor once T <= tmin */
+            if (T <= tmin && klast + 1 < sc.nvalid) hr = fnv(hr, 0xfeedull + (uint64_t)(klast + 1));
             for (int c = 0; c < 3; c++) image[((size_t)y * W + x) * 3 + c] = rgb[c];
         }
         rowh[y] = hr;
@@ -928,20 +1106,26 @@ EXPORT void d64_grad(const OrcCamera* cam, const double* params, int n, int degr
     scene64(&sc, cam, params, n, degree, near, dil);
     const int W = cam->width, H = cam->height, S = orc_stride(degree), nk = nk_of(degree);
     double* sg = (double*)calloc((size_t)(n > 0 ? n : 1) * 9, sizeof(double));
-    int* contrib = (int*)malloc(sizeof(int) * (size_t)(sc.nvalid > 0 ? sc.nvalid : 1));
-    double* alph = (double*)malloc(sizeof(double) * (size_t)(sc.nvalid > 0 ? sc.nvalid : 1));
-    double* Ts = (double*)malloc(sizeof(double) * (size_t)(sc.nvalid > 0 ? sc.nvalid : 1));
-    double* dxs = (double*)malloc(sizeof(double) * (size_t)(sc.nvalid > 0 ? sc.nvalid : 1) * 2);
-    int* cls = (int*)malloc(sizeof(int) * (size_t)(sc.nvalid > 0 ? sc.nvalid : 1));
+    const size_t cap = (size_t)(sc.cand_max > 0 ? sc.cand_max : 1);
+#pragma omp parallel
+    {
+    int* contrib = (int*)malloc(sizeof(int) * cap);
+    double* alph = (double*)malloc(sizeof(double) * cap);
+    double* Ts = (double*)malloc(sizeof(double) * cap);
+    double* dxs = (double*)malloc(sizeof(double) * cap * 2);
+    int* cls = (int*)malloc(sizeof(int) * cap);
+#pragma omp for schedule(dynamic, 2)
     for (int y = 0; y < H; y++)
         for (int x = 0; x < W; x++) {
             const double px = x + 0.5, py = y + 0.5;
             const double* g = dl + ((size_t)y * W + x) * 3;
+            const int blk = (y / D64_BLOCK) * sc.nbx + x / D64_BLOCK;
             /* Forward with the transmittance before every contributor kept. */
             double T = 1.0;
             int m = 0;
-            for (int k = 0; k < sc.nvalid; k++) {
+            for (int64_t j = sc.cand_start[blk]; j < sc.cand_start[blk + 1]; j++) {
                 if (T <= tmin) break;
+                const int k = sc.cand[j];
                 const P64* s = &sc.P[sc.order[k]];
                 double dx, dy;
                 int cl = 0;
@@ -963,25 +1147,33 @@ EXPORT void d64_grad(const OrcCamera* cam, const double* params, int n, int degr
                 const int i = contrib[q];
                 const P64* s = &sc.P[i];
                 const double a = alph[q], Tk = Ts[q];
-                double* o = sg + (size_t)i * 9;
-                for (int c = 0; c < 3; c++) o[c] += g[c] * a * Tk;
+                double v9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                for (int c = 0; c < 3; c++) v9[c] = g[c] * a * Tk;
                 double dA = 0;
                 for (int c = 0; c < 3; c++) dA += g[c] * (s->rgb[c] * Tk - behind[c] / (1.0 - a));
                 for (int c = 0; c < 3; c++) behind[c] += s->rgb[c] * a * Tk;
                 if (!cls[q]) {
                     /* a = op exp(power) */
                     const double dP = dA * a;
-                    o[3] += dA * a * (1.0 - s->opacity);
+                    v9[3] = dA * a * (1.0 - s->opacity);
                     const double dx = dxs[2 * q], dy = dxs[2 * q + 1];
                     /* power = -0.5 (A dx^2 + C dy^2) - B dx dy, dx = px - u */
-                    o[4] += dP * (s->A * dx + s->B * dy);
-                    o[5] += dP * (s->C * dy + s->B * dx);
-                    o[6] += dP * (-0.5 * dx * dx);
-                    o[7] += dP * (-dx * dy);
-                    o[8] += dP * (-0.5 * dy * dy);
+                    v9[4] = dP * (s->A * dx + s->B * dy);
+                    v9[5] = dP * (s->C * dy + s->B * dx);
+                    v9[6] = dP * (-0.5 * dx * dx);
+                    v9[7] = dP * (-dx * dy);
+                    v9[8] = dP * (-0.5 * dy * dy);
                 }
+                double* o = sg + (size_t)i * 9;
+                for (int c = 0; c < 9; c++)
+                    if (v9[c] != 0.0) {
+#pragma omp atomic
+                        o[c] += v9[c];
+                    }
             }
         }
+    free(contrib); free(alph); free(Ts); free(dxs); free(cls);
+    }
     double Wm[3][3], tv[3], cpos[3];
     cam64(cam, Wm, tv, cpos);
     for (int i = 0; i < n; i++) {
@@ -1107,11 +1299,6 @@ EXPORT void d64_grad(const OrcCamera* cam, const double* params, int n, int degr
         const double dq = gq[0] * qn[0] + gq[1] * qn[1] + gq[2] * qn[2] + gq[3] * qn[3];
         for (int k = 0; k < 4; k++) out[6 + k] = (gq[k] - qn[k] * dq) / ql;
     }
-    free(cls);
-    free(dxs);
-    free(Ts);
-    free(alph);
-    free(contrib);
     free(sg);
     scene64_free(&sc);
 }

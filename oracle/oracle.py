@@ -62,6 +62,9 @@ def lib():
         L.orc32_adam.argtypes = [F32P, F32P, F32P, F32P, i, i, i, F32P, f, f, f]
         L.orc32_step.argtypes = [CP, F32P, F32P, F32P, i, i, F32P, f, i, i, F32P, f, i]
         L.orc32_step.restype = d
+        L.orc32_train_views.argtypes = [ctypes.c_void_p, i, ctypes.c_void_p, F32P, F32P, F32P, ctypes.c_void_p, i, i,
+                                        f, i, i, F32P, f, i, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc32_train_views.restype = None
         L.orc_num_threads.restype = i
         L.orc_set_threads.argtypes = [i]
         L.d64_render.argtypes = [CP, F64P, i, i, d, d, d, d, d, F64P, ctypes.POINTER(ctypes.c_uint64)]
@@ -197,6 +200,24 @@ def step(cam, params, m, v, degree, target, lam, window, t, lr6, near=0.2, cap=1
     return lib().orc32_step(ctypes.byref(camera(cam)), params.reshape(-1), m.reshape(-1), v.reshape(-1), n,
                             degree, np.ascontiguousarray(target, np.float32).reshape(-1), lam, window, t,
                             np.asarray(lr6, np.float32), near, cap)
+
+
+def train_views(cams, targets_u8, params, m, v, degree, lam, window, t0, lr6, near=0.2, cap=1024, stats=None):
+    """trainScene over `cams` in order, one reference step per view (in place on params,
+    m, v and the optional n x 2 stats); targets_u8: the views' RGB bytes concatenated.
+    Returns the steps' losses and wall times (seconds)."""
+    arr = (OrcCamera * len(cams))(*[camera(c) for c in cams])
+    tg = np.ascontiguousarray(targets_u8, np.uint8).reshape(-1)
+    need = sum(int(c["width"]) * int(c["height"]) * 3 for c in cams)
+    assert tg.size >= need
+    losses = np.zeros(len(cams), np.float64)
+    secs = np.zeros(len(cams), np.float64)
+    n = params.shape[0]
+    st = None if stats is None else stats.ctypes.data
+    lib().orc32_train_views(ctypes.cast(arr, ctypes.c_void_p), len(cams), tg.ctypes.data, params.reshape(-1),
+                            m.reshape(-1), v.reshape(-1), st, n, degree, lam, window, t0,
+                            np.asarray(lr6, np.float32), near, cap, losses.ctypes.data, secs.ctypes.data)
+    return losses, secs
 
 
 def render_ref(cam, params, degree, near=0.2, rect_mode=0, cap=0):

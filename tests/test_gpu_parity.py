@@ -274,8 +274,12 @@ def test_parameter_gradients_larger_scene(hmp, oracle, degree):
         r.set_views([cam])
         r.forward(0, 1, images=False)
         g = r.backward(dl.astype(np.float32))
-    for name, ks in dict(mean=range(0, 3), logscale=range(3, 6), rotation=range(6, 10), opacity=[10],
-                         colour=range(11, 14)).items():
+    S = g.shape[1]
+    groups = dict(mean=range(0, 3), logscale=range(3, 6), rotation=range(6, 10), opacity=[10],
+                  colour=range(11, 14))
+    if degree > 0:
+        groups["sh"] = range(14, S)  # the 45 band coefficients of degrees 1-3
+    for name, ks in groups.items():
         assert rel_err(g[:, list(ks)], g64[:, list(ks)]) < GRAD_TOL, name
 
 

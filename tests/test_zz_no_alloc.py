@@ -1,5 +1,5 @@
 """gs_loss_gradient_noalloc: the loss gradient for callers that cannot allocate device
-memory (their own memory pool, a CUDA graph being captured, a real-time loop).  It takes
+memory (an engine that hands out all GPU memory from its own pool, a real-time loop).  It takes
 caller-owned device buffers and keeps its scratch in a static device array; its results
 must equal the allocating gs_loss_gradient's, call after call (the array is shared and
 keeps the previous call's contents, so a second call checks that it is cleared).
