@@ -941,8 +941,8 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if (cfg.raster_batch != 64 && cfg.raster_batch != 128 && cfg.raster_batch != 256)
         return fail(GS_ERR_INVALID_ARG, "raster_batch must be 64, 128 or 256");
     if (cfg.raster_ppt == 0) cfg.raster_ppt = 1;
-    if (cfg.raster_ppt != 1 && cfg.raster_ppt != 2 && cfg.raster_ppt != 4)
-        return fail(GS_ERR_INVALID_ARG, "raster_ppt must be 1, 2 or 4");
+    if (cfg.raster_ppt != 1 && cfg.raster_ppt != 2 && cfg.raster_ppt != 4 && cfg.raster_ppt != 8)
+        return fail(GS_ERR_INVALID_ARG, "raster_ppt must be 1, 2, 4 or 8");
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) {
@@ -2259,7 +2259,7 @@ int gs_autotune(GsContext* c, const char* cache_path) {
                 *bar = 0;
                 if (strcmp(line, key) == 0 && sscanf(bar + 1, "%d %d %d %d", &bf, &pf, &bb, &pb) == 4 &&
                     (bf == 64 || bf == 128 || bf == 256) && (bb == 64 || bb == 128 || bb == 256) &&
-                    (pf == 1 || pf == 2 || pf == 4) && (pb == 1 || pb == 2 || pb == 4)) {
+                    (pf == 1 || pf == 2 || pf == 4 || pf == 8) && (pb == 1 || pb == 2 || pb == 4 || pb == 8)) {
                     fclose(f);
                     apply(bf, pf, bb, pb);
                     return GS_OK;
@@ -2282,7 +2282,7 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     RasterArgs r = raster_args(c, 0, c->V);
     if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
     for (int bi = 0; bi < 3; bi++)
-        for (int ppt = 1; ppt <= 4; ppt *= 2)
+        for (int ppt = 1; ppt <= 8; ppt *= 2)
             for (int backward = 0; backward < 2; backward++) {
                 const int ctas = c->num_sms * raster_max_ctas_per_sm(batches[bi], ppt, backward != 0);
                 float total = 0.f;

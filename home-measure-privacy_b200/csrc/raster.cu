@@ -1,24 +1,32 @@
 // Tiled alpha blending, forward and backward.
 //
-// One CTA of 256 threads owns one 16 x 16 pixel tile (one pixel per thread).  The
-// tile's depth-ordered list is walked in batches: the CTA stages a batch of splat
-// records (32-byte geometry + 16-byte colour, gathered by pair index) in shared memory
-// with cp.async, double-buffered so the next batch's gather overlaps the current
-// batch's blending, then every thread blends its pixel against the batch.
+// A 16 x 16 pixel tile is 8 groups of 8 x 4 pixels (group g = 4 xh + yq: x half xh, y
+// quarter yq); lane l of a warp holds pixel (l & 7, l >> 3) of each group the warp owns.
+// With PPT pixels per thread a CTA of 256 / PPT threads owns one tile and warp w owns PPT
+// groups: all eight (PPT 8, one warp per tile), or x half w & 1 and quarters
+// (w >> 1) PPT ... (w >> 1) PPT + PPT - 1.  The tile's depth-ordered list is walked in
+// batches: the CTA stages a batch of splat records (32-byte geometry + 16-byte colour,
+// gathered by pair index) in shared memory with cp.async, double-buffered so the next
+// batch's gather overlaps the current batch's blending.  Each warp then takes the staged
+// splats 32 at a time, a lane per splat, and finds for each the warp's groups that its
+// alpha >= alpha_min ellipse (clipped to its bounding square) can reach and whose pixels
+// are still live; the splats with any such group are blended in order, group by group,
+// and only those groups are evaluated.  Skipped groups have alpha = 0 at every pixel, so
+// results are those of evaluating every pixel against every splat.
 //
 // Forward = FORWARD (trainer/gpu.js:105-137) with alphaAt (:91-103): square bounding-box
 // test, Gaussian power, alpha = min(0.99, opacity * exp(power)), skip below 1/255, stop
-// once T <= 1e-4, keep (final T, last contributor + 1).  A pixel that stopped retires;
-// the CTA stops when all 256 have (one __syncthreads_count per batch).
+// once T <= 1e-4, keep (final T, last contributor + 1).  Pixels that stopped retire their
+// group once all 32 have; the tile stops when every group has.
 //
 // Backward = BACKWARD_SG (trainer/gpu.js:208-293): the tile walks its list back to front
-// from the largest `last` of its pixels; each pixel rebuilds T before every splat from
-// the stored final T (T_k = T / (1 - alpha)) and its running `behind` colour.  The nine
-// gradients (colour, opacity logit, u, v, conic) of one splat are summed over the warp
-// with a transposed butterfly (8 values in 9 shuffles, plus 5 for the ninth), after
-// which 8 lanes issue one 32-byte vector of float reductions and lane 0 a ninth: one
-// global atomic transaction per (warp, splat) instead of nine CAS loops per pixel
-// (the reference's addF, :148-157).
+// from the largest `last` of its pixels (each group from the largest `last` of its own
+// pixels); each pixel rebuilds T before every splat from the stored final T
+// (T_k = T / (1 - alpha)) and its running `behind` colour.  The nine gradients (colour,
+// opacity logit, u, v, conic) of one splat are summed over the warp with a transposed
+// butterfly (8 values in 9 shuffles, plus 5 for the ninth), after which 8 lanes issue one
+// 32-byte vector of float reductions and lane 0 a ninth: one global atomic transaction
+// per (warp, splat) instead of nine CAS loops per pixel (the reference's addF, :148-157).
 //
 // In the persistent mode a fixed grid pulls (view, tile) work items from a global
 // counter, in an order that puts the longest tile lists first.
@@ -38,18 +46,50 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Thread -> pixels.  With PPT pixels per thread the CTA has 256 / PPT threads; warp w
-// covers an 8 x (4 PPT) block of the 16 x 16 tile (a squarer footprint than full rows,
-// so fewer splats reach each warp); lane l owns x = l & 7, y = l >> 3 (+ 4 p for its
-// p-th pixel).
+// 2^e by the PTX ex2.approx instruction (relative error about 2^-22; e here lies in
+// [log2(1/255), 0], far from the subnormal range the .ftz qualifier flushes).
+__device__ __forceinline__ float ex2_approx(float e) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
+    return r;
+}
+
+// 1/x by the PTX rcp.approx instruction (x = 1 - alpha in [0.01, 1], or a positive
+// conic coefficient).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Groups of a warp: x half and y quarter of its p-th group.
+template <int PPT>
+__device__ __forceinline__ int group_xh(int w, int p) {
+    return PPT == 8 ? (p >> 2) : (w & 1);
+}
+template <int PPT>
+__device__ __forceinline__ int group_yq(int w, int p) {
+    return PPT == 8 ? (p & 3) : ((w >> 1) * PPT + p);
+}
+template <int PPT>
+constexpr uint32_t all_groups() {
+    return (1u << PPT) - 1u;
+}
+
 template <int PPT>
 struct TileInfo {
-    int g;                     // global tile id
-    int x, y[PPT];             // this thread's pixels
+    int g;                       // global tile id
+    int x[PPT], y[PPT];          // this thread's pixels
+    bool inside[PPT];
     int width, height;
     int pixel_offset;
-    bool inside[PPT];
-    float wx0, wx1, wy0, wy1;  // pixel-centre rectangle of this thread's warp
+    float cx0, cy0;              // centre of the tile's first pixel
 };
 
 template <int PPT>
@@ -64,20 +104,18 @@ __device__ __forceinline__ TileInfo<PPT> tile_info(const RasterArgs& a, int item
     const int lt = ti.g - vw.tile_offset;
     const int tx = lt % vw.tiles_x, ty = lt / vw.tiles_x;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bx = tx * GS_TILE + (w & 1) * 8, by = ty * GS_TILE + (w >> 1) * 4 * PPT;
-    ti.x = bx + (lane & 7);
+    const int x0 = tx * GS_TILE, y0 = ty * GS_TILE;
 #pragma unroll
     for (int p = 0; p < PPT; p++) {
-        ti.y[p] = by + (lane >> 3) + 4 * p;
-        ti.inside[p] = ti.x < vw.width && ti.y[p] < vw.height;
+        ti.x[p] = x0 + 8 * group_xh<PPT>(w, p) + (lane & 7);
+        ti.y[p] = y0 + 4 * group_yq<PPT>(w, p) + (lane >> 3);
+        ti.inside[p] = ti.x[p] < vw.width && ti.y[p] < vw.height;
     }
     ti.width = vw.width;
     ti.height = vw.height;
     ti.pixel_offset = vw.pixel_offset;
-    ti.wx0 = (float)bx + 0.5f;
-    ti.wx1 = (float)bx + 7.5f;
-    ti.wy0 = (float)by + 0.5f;
-    ti.wy1 = (float)(by + 4 * PPT) - 0.5f;
+    ti.cx0 = (float)x0 + 0.5f;
+    ti.cy0 = (float)y0 + 0.5f;
     return ti;
 }
 
@@ -104,21 +142,6 @@ __device__ __forceinline__ void stage_batch(const RasterArgs& a, uint32_t first,
 }
 
 constexpr float LOG2E = 1.4426950408889634f;
-
-// 2^e by the PTX ex2.approx instruction (relative error about 2^-22; e here lies in
-// [log2(1/255), 0], far from the subnormal range the .ftz qualifier flushes).
-__device__ __forceinline__ float ex2_approx(float e) {
-    float r;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
-    return r;
-}
-
-// 1/x by the PTX rcp.approx instruction, for x = 1 - alpha in [0.01, 1].
-__device__ __forceinline__ float rcp_approx(float x) {
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
 constexpr float ALPHA_Q_BAND = 1e-4f;  // |q - log2(alpha_min)| below this: reference formula
 
 // After the batch's copies landed, each staging thread derives for its splats:
@@ -137,13 +160,56 @@ __device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g
     }
 }
 
-// alpha of splat (g0, g1, q) at offset (dx, dy), or 0 when the pixel skips it:
-// alphaAt (trainer/gpu.js:91-103).  2^q by the fast exp2; within ALPHA_Q_BAND of the
-// alpha_min threshold the reference expression min(0.99, op exp(power)) decides (a rare
-// branch), so skip decisions match the reference's.  Otherwise branch-free.  Explicit
-// rounding intrinsics keep forward and backward bit-identical.
+// The warp's groups (bit p = its p-th group) where splat (g0, g1) can give a pixel
+// centre alpha >= alpha_min.  Per x band of 8 pixel centres (the warp's half, or both):
+// the y-range of the ellipse A dx^2 + 2B dx dy + C dy^2 <= thr (thr = g1.w) over the
+// band, clipped to the splat's bounding square |dx|, |dy| <= radius, against each
+// group's 4 pixel rows.  Over a band the ellipse's upper edge is concave and its lower
+// edge convex in dx, so the range's ends sit at the stationary points
+// dx = -/+ B sqrt(thr / (A det)) clamped to the band.  Conservative: the slack covers the
+// approximate instructions; the pixels' own tests decide.
+template <int PPT>
+__device__ __forceinline__ uint32_t group_mask(const float4& g0, const float4& g1, float cx0, float cy0, int w) {
+    const float thr = g1.w;
+    if (!(thr > 0.f)) return 0u;
+    const float u = g0.x, v = g0.y, A = g0.z, B = g0.w, C = g1.x, r = g1.z;
+    const float det = fmaxf(A * C - B * B, 1e-30f);
+    const float idet = rcp_approx(det);
+    const float iC = rcp_approx(C);
+    const float xr = sqrt_approx(thr * C * idet);                  // the ellipse's x half-extent
+    const float sx = B * sqrt_approx(thr * idet * rcp_approx(A));  // stationary point of the lower edge
+    const float slack = 1e-3f * (1.0f + r);
+    uint32_t m = 0u;
+    constexpr int NH = PPT == 8 ? 2 : 1;
+    constexpr int NQ = PPT == 8 ? 4 : PPT;
+#pragma unroll
+    for (int hh = 0; hh < NH; hh++) {
+        const int xhalf = PPT == 8 ? hh : (w & 1);
+        const float bx = cx0 + 8.0f * (float)xhalf - u;  // first pixel centre of the band, from u
+        const float xl = fmaxf(fmaxf(bx, -r), -xr - slack);
+        const float xh = fminf(fminf(bx + 7.0f, r), xr + slack);
+        if (xl > xh) continue;
+        const float du = fminf(fmaxf(-sx, xl), xh);  // maximiser of the upper edge
+        const float dl = fminf(fmaxf(sx, xl), xh);   // minimiser of the lower edge
+        const float hi = fminf((-B * du + sqrt_approx(fmaxf(C * thr - det * du * du, 0.f))) * iC + slack, r);
+        const float lo = fmaxf((-B * dl - sqrt_approx(fmaxf(C * thr - det * dl * dl, 0.f))) * iC - slack, -r);
+#pragma unroll
+        for (int i = 0; i < NQ; i++) {
+            const int q = PPT == 8 ? i : ((w >> 1) * PPT + i);
+            const float y0 = cy0 + 4.0f * (float)q - v;  // first pixel-centre row of the group, from v
+            if (y0 <= hi && y0 + 3.0f >= lo) m |= 1u << (PPT == 8 ? hh * 4 + i : i);
+        }
+    }
+    return m;
+}
+
+// alpha of splat (g0, g1) at offset (dx, dy), or 0 when the pixel skips it:
+// alphaAt (trainer/gpu.js:91-103), in the reference's own arithmetic.  Used where the
+// log2-domain exponent lies within ALPHA_Q_BAND of the alpha_min threshold (a rare
+// branch), so skip decisions match the reference's.  Explicit rounding intrinsics keep
+// forward and backward bit-identical.
 __device__ __forceinline__ float alpha_band(const float4& g0, const float4& g1, float dx, float dy, float amax,
-                                         float amin) {
+                                            float amin) {
     const float power = __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(__fmul_rn(__fmul_rn(g0.z, dx), dx),
                                                              __fmul_rn(__fmul_rn(g1.x, dy), dy))),
                                   __fmul_rn(__fmul_rn(g0.w, dx), dy));
@@ -154,29 +220,39 @@ __device__ __forceinline__ float alpha_band(const float4& g0, const float4& g1, 
     return alpha < amin ? 0.f : fminf(amax, alpha);
 }
 
-__device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, float dx, float dy,
-                                          float amax, float amin, float qlo, float qhi) {
-    const float t = __fmaf_rn(q.y, dy, __fmul_rn(q.x, dx));
-    float e = __fmaf_rn(dx, t, q.w);
-    e = __fmaf_rn(__fmul_rn(q.z, dy), dy, e);
-    const bool inb = fabsf(dx) <= g1.z && fabsf(dy) <= g1.z;
+// The pieces of the alpha exponent that depend on one splat and one pixel column:
+// log2(alpha) = a0 + dy (b0 + qc dy) with a0 = log2(op) + qa dx^2, b0 = qb dx; and
+// whether |dx| <= radius.
+struct XTerm {
+    float dx, a0, b0;
+    bool inb;
+};
+
+__device__ __forceinline__ XTerm xterm(const float4& q, float dx, float radius) {
+    XTerm t;
+    t.dx = dx;
+    t.a0 = __fmaf_rn(dx, __fmul_rn(q.x, dx), q.w);
+    t.b0 = __fmul_rn(q.y, dx);
+    t.inb = fabsf(dx) <= radius;
+    return t;
+}
+
+// alpha at the pixel (column term xt, row offset dy), or 0 when the pixel skips the
+// splat: 2^q by the fast exp2; within ALPHA_Q_BAND of the alpha_min threshold the
+// reference expression decides.  Otherwise branch-free.
+__device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, const XTerm& xt,
+                                          float dy, float amax, float amin, float qlo, float qhi) {
+    const float e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, xt.b0), xt.a0);
+    const bool inb = xt.inb && fabsf(dy) <= g1.z;
     float alpha = (inb && e >= qhi) ? fminf(amax, ex2_approx(e)) : 0.f;
-    if (inb && e >= qlo && e < qhi) alpha = alpha_band(g0, g1, dx, dy, amax, amin);
+    if (inb && e >= qlo && e < qhi) alpha = alpha_band(g0, g1, xt.dx, dy, amax, amin);
     return alpha;
 }
 
-// Can splat (g0, g1) give any pixel centre of the warp's rectangle alpha >= alpha_min?
-// Conservative: the pixels' own tests (bounding box, then alpha) decide; this only
-// skips splats that cannot pass them anywhere in the rectangle.
-template <int PPT>
-__device__ __forceinline__ bool warp_reaches(const float4& g0, const float4& g1, const TileInfo<PPT>& ti) {
-    return splat_reaches_box(g0.x, g0.y, g0.z, g0.w, g1.x, g1.z, g1.w, ti.wx0, ti.wx1, ti.wy0, ti.wy1);
-}
-
-// Resident CTAs per SM the register allocation is sized for (64 threads with 4 pixels
-// each get more registers per thread than 16 CTAs would leave them).
-constexpr int fwd_min_ctas(int ppt) { return ppt == 4 ? 12 : 4 * ppt; }
-constexpr int bwd_min_ctas(int ppt) { return ppt == 4 ? 10 : (ppt == 2 ? 7 : 4); }
+// Resident CTAs per SM the register allocation is sized for (fewer threads with more
+// pixels each get more registers per thread).
+constexpr int fwd_min_ctas(int ppt) { return ppt == 8 ? 20 : (ppt == 4 ? 12 : 4 * ppt); }
+constexpr int bwd_min_ctas(int ppt) { return ppt == 8 ? 16 : (ppt == 4 ? 10 : (ppt == 2 ? 7 : 4)); }
 
 template <int BATCH, int PPT>
 __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kernel(RasterArgs a) {
@@ -185,7 +261,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
     __shared__ __align__(16) float4 s_c[2][BATCH];
     __shared__ __align__(16) float4 s_q[2][BATCH];
     __shared__ int s_item;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const float log_amin = __logf(a.alpha_min);
     const float qthr = __log2f(a.alpha_min);
     const float qlo = qthr - ALPHA_Q_BAND, qhi = qthr + ALPHA_Q_BAND;
@@ -194,10 +270,12 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
         const TileInfo<PPT> ti = tile_info<PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x, end = rg.y;
-        const float pxf = (float)ti.x + 0.5f;
-        float pyf[PPT], T[PPT], cr[PPT], cg[PPT], cb[PPT];
+        float pxf[PPT == 8 ? 2 : 1], pyf[PPT], T[PPT], cr[PPT], cg[PPT], cb[PPT];
         uint32_t last[PPT];
         bool done[PPT];
+        pxf[0] = (float)ti.x[0] + 0.5f;
+        if (PPT == 8) pxf[PPT == 8 ? 1 : 0] = (float)ti.x[PPT - 1] + 0.5f;
+        uint32_t gdone = 0u;  // warp-uniform: groups whose pixels have all stopped
 #pragma unroll
         for (int p = 0; p < PPT; p++) {
             pyf[p] = (float)ti.y[p] + 0.5f;
@@ -205,6 +283,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
             cr[p] = cg[p] = cb[p] = 0.f;
             last[p] = start;
             done[p] = !ti.inside[p];
+            if (__all_sync(FULL_MASK, done[p])) gdone |= 1u << p;
         }
         int buf = 0;
         if (start < end) stage_batch(a, start, min((uint32_t)BATCH, end - start), false, s_g0[0], s_g1[0], s_c[0], nullptr);
@@ -224,46 +303,46 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
             const float4* g1s = s_g1[buf];
             const float4* cs = s_c[buf];
             const float4* qs = s_q[buf];
-            bool all_done = true;
-#pragma unroll
-            for (int p = 0; p < PPT; p++) all_done = all_done && done[p];
-            bool warp_done = __all_sync(FULL_MASK, all_done);
-            for (int gb = 0; gb < cnt && !warp_done; gb += 32) {
+            for (int gb = 0; gb < cnt && gdone != all_groups<PPT>(); gb += 32) {
                 const int jl = gb + lane;
-                const bool rel = jl < cnt && warp_reaches<PPT>(g0s[jl], g1s[jl], ti);
-                uint32_t mask = __ballot_sync(FULL_MASK, rel);
-                while (mask) {
-                    const int j = gb + __ffs(mask) - 1;
-                    mask &= mask - 1;
+                const uint32_t gm = jl < cnt ? group_mask<PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) : 0u;
+                uint32_t live = __ballot_sync(FULL_MASK, (gm & ~gdone) != 0u);
+                while (live) {
+                    const int jj = __ffs(live) - 1;
+                    live &= live - 1;
+                    const int j = gb + jj;
+                    const uint32_t m = __shfl_sync(FULL_MASK, gm, jj) & ~gdone;  // warp-uniform
                     const float4 g0 = g0s[j];
                     const float4 g1 = g1s[j];
                     const float4 q = qs[j];
-                    const float dx = pxf - g0.x;
+                    const float4 c = cs[j];
+                    const uint32_t pos = b0 + (uint32_t)j + 1u;
+                    XTerm xt[PPT == 8 ? 2 : 1];
+                    xt[0] = xterm(q, pxf[0] - g0.x, g1.z);
+                    if (PPT == 8) xt[PPT == 8 ? 1 : 0] = xterm(q, pxf[PPT == 8 ? 1 : 0] - g0.x, g1.z);
 #pragma unroll
                     for (int p = 0; p < PPT; p++) {
-                        // Branch-free per lane (alpha = 0 leaves colour, T and last as
-                        // they are); the warp skips the pixel row when no lane blends.
-                        float alpha = alpha_at(g0, g1, q, dx, pyf[p] - g0.y, a.alpha_max, a.alpha_min, qlo, qhi);
+                        if (!(m & (1u << p))) continue;
+                        // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
+                        float alpha = alpha_at(g0, g1, q, xt[PPT == 8 ? (p >> 2) : 0], pyf[p] - g0.y, a.alpha_max,
+                                               a.alpha_min, qlo, qhi);
                         alpha = done[p] ? 0.f : alpha;
-                        if (!__any_sync(FULL_MASK, alpha != 0.f)) continue;
-                        const float4 c = cs[j];
-                        const float w = alpha * T[p];
-                        cr[p] += c.x * w;
-                        cg[p] += c.y * w;
-                        cb[p] += c.z * w;
+                        const float wgt = alpha * T[p];
+                        cr[p] += c.x * wgt;
+                        cg[p] += c.y * wgt;
+                        cb[p] += c.z * wgt;
                         T[p] *= 1.0f - alpha;
-                        last[p] = alpha != 0.f ? b0 + (uint32_t)j + 1u : last[p];
+                        last[p] = alpha != 0.f ? pos : last[p];
                         done[p] = done[p] || T[p] <= a.t_min;
                     }
                 }
-                all_done = true;
 #pragma unroll
-                for (int p = 0; p < PPT; p++) all_done = all_done && done[p];
-                warp_done = __all_sync(FULL_MASK, all_done);
+                for (int p = 0; p < PPT; p++)
+                    if (__all_sync(FULL_MASK, done[p])) gdone |= 1u << p;
             }
             buf ^= 1;
             // All pixels done: the rest of the list cannot change the tile.
-            if (__syncthreads_count(all_done) == (int)blockDim.x) {
+            if (__syncthreads_count(gdone == all_groups<PPT>()) == (int)blockDim.x) {
                 cp_async_wait<0>();
                 break;
             }
@@ -271,7 +350,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
 #pragma unroll
         for (int p = 0; p < PPT; p++) {
             if (!ti.inside[p]) continue;
-            const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x;
+            const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x[p];
             a.image[pix * 3 + 0] = cr[p];
             a.image[pix * 3 + 1] = cg[p];
             a.image[pix * 3 + 2] = cb[p];
@@ -321,7 +400,7 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
     __shared__ uint32_t s_pair[2][BATCH];
     __shared__ int s_item;
     __shared__ unsigned int s_end;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const float log_amin = __logf(a.alpha_min);
     const float qthr = __log2f(a.alpha_min);
     const float qlo = qthr - ALPHA_Q_BAND, qhi = qthr + ALPHA_Q_BAND;
@@ -341,10 +420,11 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
         const TileInfo<PPT> ti = tile_info<PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
-        const float pxf = (float)ti.x + 0.5f;
-        float pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
-        uint32_t mylast[PPT];
-        unsigned int tmax = start;
+        float pxf[PPT == 8 ? 2 : 1], pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
+        uint32_t mylast[PPT], gmax[PPT];
+        pxf[0] = (float)ti.x[0] + 0.5f;
+        if (PPT == 8) pxf[PPT == 8 ? 1 : 0] = (float)ti.x[PPT - 1] + 0.5f;
+        unsigned int wmax = start;
 #pragma unroll
         for (int p = 0; p < PPT; p++) {
             pyf[p] = (float)ti.y[p] + 0.5f;
@@ -353,22 +433,23 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
             bd[p] = 0.f;  // dL . (colour of the splats behind), "behind"
             mylast[p] = start;
             if (ti.inside[p]) {
-                const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x;
+                const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x[p];
                 T[p] = a.t_final[pix];
                 mylast[p] = a.last[pix];
                 dlr[p] = a.dl[pix * 3 + 0];
                 dlg[p] = a.dl[pix * 3 + 1];
                 dlb[p] = a.dl[pix * 3 + 2];
             }
-            tmax = max(tmax, mylast[p]);
+            // Each group walks from the largest last of its pixels.
+            unsigned int gm = mylast[p];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) gm = max(gm, __shfl_xor_sync(FULL_MASK, gm, o));
+            gmax[p] = gm;
+            wmax = max(wmax, gm);
         }
         if (threadIdx.x == 0) s_end = start;
         __syncthreads();
-        // Tile end = largest last of its pixels (BACKWARD_SG, trainer/gpu.js:247-253);
-        // each warp also stops at its own largest last.
-        unsigned int wmax = tmax;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) wmax = max(wmax, __shfl_xor_sync(FULL_MASK, wmax, o));
+        // Tile end = largest last of its pixels (BACKWARD_SG, trainer/gpu.js:247-253).
         if (lane == 0) atomicMax(&s_end, wmax);
         __syncthreads();
         const uint32_t end = s_end;
@@ -397,33 +478,43 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
             if (bstart < wmax) {
                 for (int gb = 0; gb < cnt; gb += 32) {
                     const int jl = gb + lane;
-                    const bool rel = jl < cnt && (bend - 1 - (uint32_t)jl) < wmax && warp_reaches<PPT>(g0s[jl], g1s[jl], ti);
-                    uint32_t mask = __ballot_sync(FULL_MASK, rel);
-                    while (mask) {
-                        const int j = gb + __ffs(mask) - 1;
-                        mask &= mask - 1;
+                    uint32_t gm = 0u;
+                    if (jl < cnt) {
+                        const uint32_t kl = bend - 1 - (uint32_t)jl;
+                        uint32_t act = 0u;  // groups with a pixel whose last is past this entry
+#pragma unroll
+                        for (int p = 0; p < PPT; p++) act |= kl < gmax[p] ? (1u << p) : 0u;
+                        if (act) gm = group_mask<PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) & act;
+                    }
+                    uint32_t live = __ballot_sync(FULL_MASK, gm != 0u);
+                    while (live) {
+                        const int jj = __ffs(live) - 1;
+                        live &= live - 1;
+                        const int j = gb + jj;
+                        const uint32_t m = __shfl_sync(FULL_MASK, gm, jj);  // warp-uniform
                         const uint32_t k = bend - 1 - (uint32_t)j;
                         const float4 g0 = g0s[j];
                         const float4 g1 = g1s[j];
                         const float4 q = qs[j];
-                        const float dx = pxf - g0.x;
+                        const float4 c = cs[j];
+                        XTerm xt[PPT == 8 ? 2 : 1];
+                        xt[0] = xterm(q, pxf[0] - g0.x, g1.z);
+                        if (PPT == 8) xt[PPT == 8 ? 1 : 0] = xterm(q, pxf[PPT == 8 ? 1 : 0] - g0.x, g1.z);
                         // Per pixel: colour terms and the moments of dP = dL/dpower over the
                         // offsets (sum dP, dP dx, dP dy, dP dx^2, dP dx dy, dP dy^2); the
                         // splat's conic and opacity turn the warp sums into the gradients of
                         // (opacity logit, u, v, A, B, C) after the reduction.
                         float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                         float v8 = 0.f;
-                        bool contrib = false;  // warp-uniform
 #pragma unroll
                         for (int p = 0; p < PPT; p++) {
+                            if (!(m & (1u << p))) continue;
                             // Branch-free per lane: alpha = 0 adds zeros and leaves T
                             // (T / 1) and dL.behind as they are.
-                            const float dy = pyf[p] - g0.y;
-                            float alpha = alpha_at(g0, g1, q, dx, dy, a.alpha_max, a.alpha_min, qlo, qhi);
+                            const XTerm& x = xt[PPT == 8 ? (p >> 2) : 0];
+                            const float dx = x.dx, dy = pyf[p] - g0.y;
+                            float alpha = alpha_at(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi);
                             alpha = k < mylast[p] ? alpha : 0.f;
-                            if (!__any_sync(FULL_MASK, alpha != 0.f)) continue;
-                            contrib = true;
-                            const float4 c = cs[j];
                             const float ioma = rcp_approx(1.0f - alpha);
                             const float Tk = T[p] * ioma;
                             const float at = alpha * Tk;
@@ -446,23 +537,21 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
                             v[7] += dPx * dy;
                             v8 += dPy * dy;
                         }
-                        if (contrib) {
-                            float s = warp_sum8_transposed(v);
-                            float s8 = v8;
+                        float s = warp_sum8_transposed(v);
+                        float s8 = v8;
 #pragma unroll
-                            for (int o = 16; o > 0; o >>= 1) s8 += __shfl_xor_sync(FULL_MASK, s8, o);
-                            // lane 4g holds sum g: 3 -> opacity logit (x (1 - op)), 4/5 -> u/v
-                            // (A Sx + B Sy, C Sy + B Sx), 6/7 -> A/B (-Sxx/2, -Sxy), C = -Syy/2.
-                            // Branch-free: s = s (k0 + kop op + kA A + kC C) + other kB B with the
-                            // lane's selector constants.
-                            const float other = __shfl_xor_sync(FULL_MASK, s, 4);
-                            const float m0 = fmaf(sel.w, g1.x, fmaf(sel.z, g0.z, fmaf(sel.y, g1.y, sel.x)));
-                            s = fmaf(s, m0, other * (sel_b * g0.w));
-                            s8 *= -0.5f;
-                            const uint32_t pair = ps[j];
-                            if ((lane & 3) == 0 && s != 0.0f) atomicAdd(sg8f + (size_t)pair * 8 + (lane >> 2), s);
-                            if (lane == 0 && s8 != 0.0f) atomicAdd(a.sg1 + pair, s8);
-                        }
+                        for (int o = 16; o > 0; o >>= 1) s8 += __shfl_xor_sync(FULL_MASK, s8, o);
+                        // lane 4g holds sum g: 3 -> opacity logit (x (1 - op)), 4/5 -> u/v
+                        // (A Sx + B Sy, C Sy + B Sx), 6/7 -> A/B (-Sxx/2, -Sxy), C = -Syy/2.
+                        // Branch-free: s = s (k0 + kop op + kA A + kC C) + other kB B with the
+                        // lane's selector constants.
+                        const float other = __shfl_xor_sync(FULL_MASK, s, 4);
+                        const float m0 = fmaf(sel.w, g1.x, fmaf(sel.z, g0.z, fmaf(sel.y, g1.y, sel.x)));
+                        s = fmaf(s, m0, other * (sel_b * g0.w));
+                        s8 *= -0.5f;
+                        const uint32_t pair = ps[j];
+                        if ((lane & 3) == 0 && s != 0.0f) atomicAdd(sg8f + (size_t)pair * 8 + (lane >> 2), s);
+                        if (lane == 0 && s8 != 0.0f) atomicAdd(a.sg1 + pair, s8);
                     }
                 }
             }
@@ -476,8 +565,6 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
 }
 
 // Variant = (shared-memory batch, pixels per thread); the autotuner picks one.
-static const int kBatches[3] = {64, 128, 256};
-
 template <int BATCH, int PPT>
 static void fwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
     raster_fwd_kernel<BATCH, PPT><<<ctas, 256 / PPT, 0, s>>>(a);
@@ -487,27 +574,21 @@ static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
     raster_bwd_kernel<BATCH, PPT><<<ctas, 256 / PPT, 0, s>>>(a);
 }
 
-#define RASTER_SWITCH(FN, batch, ppt, ...)                   \
+#define RASTER_BATCHES(FN, batch, P, ...)                    \
     do {                                                     \
-        if ((ppt) == 4) {                                    \
-            switch (batch) {                                 \
-                case 64: FN<64, 4>(__VA_ARGS__); break;      \
-                case 128: FN<128, 4>(__VA_ARGS__); break;    \
-                default: FN<256, 4>(__VA_ARGS__); break;     \
-            }                                                \
-        } else if ((ppt) == 2) {                             \
-            switch (batch) {                                 \
-                case 64: FN<64, 2>(__VA_ARGS__); break;      \
-                case 128: FN<128, 2>(__VA_ARGS__); break;    \
-                default: FN<256, 2>(__VA_ARGS__); break;     \
-            }                                                \
-        } else {                                             \
-            switch (batch) {                                 \
-                case 64: FN<64, 1>(__VA_ARGS__); break;      \
-                case 128: FN<128, 1>(__VA_ARGS__); break;    \
-                default: FN<256, 1>(__VA_ARGS__); break;     \
-            }                                                \
+        switch (batch) {                                     \
+            case 64: FN<64, P>(__VA_ARGS__); break;          \
+            case 128: FN<128, P>(__VA_ARGS__); break;        \
+            default: FN<256, P>(__VA_ARGS__); break;         \
         }                                                    \
+    } while (0)
+
+#define RASTER_SWITCH(FN, batch, ppt, ...)                                      \
+    do {                                                                        \
+        if ((ppt) == 8) RASTER_BATCHES(FN, batch, 8, __VA_ARGS__);             \
+        else if ((ppt) == 4) RASTER_BATCHES(FN, batch, 4, __VA_ARGS__);        \
+        else if ((ppt) == 2) RASTER_BATCHES(FN, batch, 2, __VA_ARGS__);        \
+        else RASTER_BATCHES(FN, batch, 1, __VA_ARGS__);                         \
     } while (0)
 
 void launch_raster_fwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s) {

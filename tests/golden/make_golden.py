@@ -22,7 +22,7 @@ sample_ply_quarter.npz -- every 4th splat of the reference's tour/sample.ply (th
     colour = clamp(f_dc * SH0 + 0.5, 0, 1), opacity logit, log-scales, rotation w,x,y,z),
     in the host record layout (mean3, logScale3, rotation4, opacityLogit, colour3).
 
-    python tests/golden/make_golden.py [path/to/reference]
+    python tests/golden/make_golden.py path/to/reference
 """
 import os
 import sys
@@ -30,7 +30,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py path/to/reference")
+REF = sys.argv[1]
 
 
 def lcg(seed=7):

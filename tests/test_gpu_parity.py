@@ -163,7 +163,7 @@ def test_batched_equals_plain(hmp):
     assert np.array_equal(out[True], out[False])
 
 
-@pytest.mark.parametrize("ppt", [1, 2, 4])
+@pytest.mark.parametrize("ppt", [1, 2, 4, 8])
 def test_raster_variants_agree(hmp, ppt):
     """Every (shared-memory batch, pixels per thread) variant the autotuner may pick,
     persistent over four uneven views: the same images bit for bit (each pixel blends the
