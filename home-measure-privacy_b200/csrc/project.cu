@@ -78,14 +78,18 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
             p.ok = false;
         uint32_t count = (p.ok && x1 > x0 && y1 > y0) ? (uint32_t)((x1 - x0) * (y1 - y0)) : 0u;
         uint32_t sp[4] = {0u, 0u, 0u, 0u};
+        // Conic elongation kappa = A C / (A C - B^2): above 256 the ellipse arithmetic below
+        // is not trusted (its rounding grows with kappa) and the whole rectangle is kept.
+        const float kap_ac = p.a * p.c;
+        const float kappa = p.ok ? kap_ac / fmaxf(kap_ac - p.b * p.b, kap_ac * 1e-12f + 1e-30f) : 0.f;
         if (count && a.tile_cull) {
-            if (y1 - y0 <= GS_SPAN_ROWS && x1 - x0 < 256) {
+            if (y1 - y0 <= GS_SPAN_ROWS && x1 - x0 < 256 && kappa <= 256.f) {
                 // Per rectangle row, the tiles the ellipse A dx^2 + 2B dx dy + C dy^2 <= thr
                 // reaches inside the row's pixel band (and the |d| <= r square, and the
                 // image): the band's x-extent of the ellipse is contiguous, its right edge
                 // concave and its left edge convex in dy, so each extreme sits at its
                 // stationary point dy* = -/+ B sqrt(thr / (det C)) clamped to the band.
-                const float thr = thr_g;
+                const float thr = thr_g * (1.0f + kappa * 1.52587890625e-05f);  // rounding of the form grows with kappa
                 const float A = p.a, B = p.b, C = p.c;
                 const float det = fmaxf(A * C - B * B, 1e-30f);
                 const float idet = rcp_approx(det);

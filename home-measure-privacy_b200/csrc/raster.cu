@@ -143,20 +143,41 @@ __device__ __forceinline__ void stage_batch(const RasterArgs& a, uint32_t first,
 
 constexpr float LOG2E = 1.4426950408889634f;
 constexpr float ALPHA_Q_BAND = 1e-4f;  // |q - log2(alpha_min)| below this: reference formula
+constexpr float KAPPA_CULL_MAX = 256.f; // elongation above which culling uses the bounding square only
+constexpr float KAPPA_EXACT = 32.f;     // elongation above which every pixel uses the reference expression
+
+// Elongation of a splat's conic, kappa = A C / (A C - B^2) >= 1: the quadratic form's
+// terms reach kappa times its value, so rounding errors in the exponent (and in the
+// ellipse arithmetic) grow with it.
+__device__ __forceinline__ float conic_kappa(float A, float B, float C) {
+    const float ac = A * C;
+    return ac / fmaxf(ac - B * B, ac * 1e-12f + 1e-30f);
+}
 
 // After the batch's copies landed, each staging thread derives for its splats:
 // s_g1.w = the culling bound 2 ln(opacity / alpha_min) + slack (a pixel can reach
-// alpha >= alpha_min only where the conic's quadratic form is below it), and
+// alpha >= alpha_min only where the conic's quadratic form is below it);
 // s_q = (-A/2, -B, -C/2) log2(e) and log2(opacity), so that alpha = 2^q with
-// q = log2(op) + qa dx^2 + qb dx dy + qc dy^2.
-__device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g1, float4* s_q, float log_amin) {
+// q = log2(op) + qa dx^2 + qb dx dy + qc dy^2; and s_c.w = the half-width of the band
+// around log2(alpha_min) in which the reference expression decides: 1e-4 plus a bound
+// on the rounding of q and of the reference's own exponent, which grows with the
+// conic's elongation (for near-degenerate splats seen from close by, the terms of q are
+// thousands of times q itself).  Above KAPPA_EXACT the rounding of the reference's own
+// exponent shows in alpha's value, so such splats take their exponent from the
+// reference's power, rounded as the reference rounds it (alpha_at's exact form, marked by
+// a negative s_c.w), with the plain 1e-4 band.
+__device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g1, float4* s_q, float4* s_c,
+                                              float log_amin, float qthr) {
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
         const float4 g0 = s_g0[t];
         const float4 g1 = s_g1[t];
         const float op = g1.y;
-        s_g1[t].w = op > 0.f ? 2.0f * (__logf(op) - log_amin) + 1e-3f : -1.0f;
-        s_q[t] = make_float4(-0.5f * LOG2E * g0.z, -LOG2E * g0.w, -0.5f * LOG2E * g1.x,
-                             op > 0.f ? __log2f(op) : -1e30f);
+        const float kappa = conic_kappa(g0.z, g0.w, g1.x);
+        const float lop = op > 0.f ? __log2f(op) : -1e30f;
+        s_g1[t].w = op > 0.f ? 2.0f * (__logf(op) - log_amin) * (1.0f + kappa * 1.52587890625e-05f) + 1e-3f : -1.0f;
+        s_q[t] = make_float4(-0.5f * LOG2E * g0.z, -LOG2E * g0.w, -0.5f * LOG2E * g1.x, lop);
+        s_c[t].w = kappa > KAPPA_EXACT ? -ALPHA_Q_BAND
+                                       : ALPHA_Q_BAND + 7.62939453125e-06f * kappa * fmaxf(lop - qthr, 1.0f);  // 2^-17
     }
 }
 
@@ -173,6 +194,26 @@ __device__ __forceinline__ uint32_t group_mask(const float4& g0, const float4& g
     const float thr = g1.w;
     if (!(thr > 0.f)) return 0u;
     const float u = g0.x, v = g0.y, A = g0.z, B = g0.w, C = g1.x, r = g1.z;
+    constexpr int NH = PPT == 8 ? 2 : 1;
+    constexpr int NQ = PPT == 8 ? 4 : PPT;
+    if (conic_kappa(A, B, C) > KAPPA_CULL_MAX) {
+        // Near-degenerate conic: its ellipse arithmetic is not trusted, cull by the
+        // bounding square |dx|, |dy| <= radius alone.
+        uint32_t m = 0u;
+#pragma unroll
+        for (int hh = 0; hh < NH; hh++) {
+            const int xhalf = PPT == 8 ? hh : (w & 1);
+            const float bx = cx0 + 8.0f * (float)xhalf - u;
+            if (bx > r || bx + 7.0f < -r) continue;
+#pragma unroll
+            for (int i = 0; i < NQ; i++) {
+                const int q = PPT == 8 ? i : ((w >> 1) * PPT + i);
+                const float y0 = cy0 + 4.0f * (float)q - v;
+                if (y0 <= r && y0 + 3.0f >= -r) m |= 1u << (PPT == 8 ? hh * 4 + i : i);
+            }
+        }
+        return m;
+    }
     const float det = fmaxf(A * C - B * B, 1e-30f);
     const float idet = rcp_approx(det);
     const float iC = rcp_approx(C);
@@ -180,8 +221,6 @@ __device__ __forceinline__ uint32_t group_mask(const float4& g0, const float4& g
     const float sx = B * sqrt_approx(thr * idet * rcp_approx(A));  // stationary point of the lower edge
     const float slack = 1e-3f * (1.0f + r);
     uint32_t m = 0u;
-    constexpr int NH = PPT == 8 ? 2 : 1;
-    constexpr int NQ = PPT == 8 ? 4 : PPT;
 #pragma unroll
     for (int hh = 0; hh < NH; hh++) {
         const int xhalf = PPT == 8 ? hh : (w & 1);
@@ -238,11 +277,22 @@ __device__ __forceinline__ XTerm xterm(const float4& q, float dx, float radius) 
 }
 
 // alpha at the pixel (column term xt, row offset dy), or 0 when the pixel skips the
-// splat: 2^q by the fast exp2; within ALPHA_Q_BAND of the alpha_min threshold the
-// reference expression decides.  Otherwise branch-free.
+// splat: 2^q by the fast exp2; within [qlo, qhi) around the alpha_min threshold the
+// reference expression decides.  Otherwise branch-free.  `exact` (warp-uniform: a splat
+// property) takes q from the reference's power, rounded as the reference rounds it,
+// instead of the expanded quadratic, for elongated conics whose expanded terms are far
+// larger than q.
 __device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, const XTerm& xt,
-                                          float dy, float amax, float amin, float qlo, float qhi) {
-    const float e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, xt.b0), xt.a0);
+                                          float dy, float amax, float amin, float qlo, float qhi, bool exact) {
+    float e;
+    if (exact) {
+        const float power = __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(__fmul_rn(__fmul_rn(g0.z, xt.dx), xt.dx),
+                                                                 __fmul_rn(__fmul_rn(g1.x, dy), dy))),
+                                      __fmul_rn(__fmul_rn(g0.w, xt.dx), dy));
+        e = power > 0.f ? -1e30f : __fmaf_rn(power, LOG2E, q.w);  // the reference skips power > 0
+    } else {
+        e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, xt.b0), xt.a0);
+    }
     const bool inb = xt.inb && fabsf(dy) <= g1.z;
     float alpha = (inb && e >= qhi) ? fminf(amax, ex2_approx(e)) : 0.f;
     if (inb && e >= qlo && e < qhi) alpha = alpha_band(g0, g1, xt.dx, dy, amax, amin);
@@ -264,7 +314,6 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const float log_amin = __logf(a.alpha_min);
     const float qthr = __log2f(a.alpha_min);
-    const float qlo = qthr - ALPHA_Q_BAND, qhi = qthr + ALPHA_Q_BAND;
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
         const TileInfo<PPT> ti = tile_info<PPT>(a, item);
@@ -297,7 +346,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
             } else {
                 cp_async_wait<0>();
             }
-            prepare_batch(cnt, s_g0[buf], s_g1[buf], s_q[buf], log_amin);
+            prepare_batch(cnt, s_g0[buf], s_g1[buf], s_q[buf], s_c[buf], log_amin, qthr);
             __syncthreads();
             const float4* g0s = s_g0[buf];
             const float4* g1s = s_g1[buf];
@@ -316,6 +365,8 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
                     const float4 g1 = g1s[j];
                     const float4 q = qs[j];
                     const float4 c = cs[j];
+                    const bool exact = c.w < 0.f;  // warp-uniform
+                    const float qlo = qthr - fabsf(c.w), qhi = qthr + fabsf(c.w);
                     const uint32_t pos = b0 + (uint32_t)j + 1u;
                     XTerm xt[PPT == 8 ? 2 : 1];
                     xt[0] = xterm(q, pxf[0] - g0.x, g1.z);
@@ -325,7 +376,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
                         if (!(m & (1u << p))) continue;
                         // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
                         float alpha = alpha_at(g0, g1, q, xt[PPT == 8 ? (p >> 2) : 0], pyf[p] - g0.y, a.alpha_max,
-                                               a.alpha_min, qlo, qhi);
+                                               a.alpha_min, qlo, qhi, exact);
                         alpha = done[p] ? 0.f : alpha;
                         const float wgt = alpha * T[p];
                         cr[p] += c.x * wgt;
@@ -403,7 +454,6 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const float log_amin = __logf(a.alpha_min);
     const float qthr = __log2f(a.alpha_min);
-    const float qlo = qthr - ALPHA_Q_BAND, qhi = qthr + ALPHA_Q_BAND;
     float* sg8f = reinterpret_cast<float*>(a.sg8);
     // Selector constants of this lane's reduced value g = lane / 4 (see the reduction):
     // (k0, kop, kA, kC) and kB.
@@ -466,7 +516,7 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
             } else {
                 cp_async_wait<0>();
             }
-            prepare_batch(cnt, s_g0[buf], s_g1[buf], s_q[buf], log_amin);
+            prepare_batch(cnt, s_g0[buf], s_g1[buf], s_q[buf], s_c[buf], log_amin, qthr);
             __syncthreads();
             const float4* g0s = s_g0[buf];
             const float4* g1s = s_g1[buf];
@@ -497,6 +547,8 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
                         const float4 g1 = g1s[j];
                         const float4 q = qs[j];
                         const float4 c = cs[j];
+                        const bool exact = c.w < 0.f;  // warp-uniform
+                    const float qlo = qthr - fabsf(c.w), qhi = qthr + fabsf(c.w);
                         XTerm xt[PPT == 8 ? 2 : 1];
                         xt[0] = xterm(q, pxf[0] - g0.x, g1.z);
                         if (PPT == 8) xt[PPT == 8 ? 1 : 0] = xterm(q, pxf[PPT == 8 ? 1 : 0] - g0.x, g1.z);
@@ -513,7 +565,7 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
                             // (T / 1) and dL.behind as they are.
                             const XTerm& x = xt[PPT == 8 ? (p >> 2) : 0];
                             const float dx = x.dx, dy = pyf[p] - g0.y;
-                            float alpha = alpha_at(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi);
+                            float alpha = alpha_at(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi, exact);
                             alpha = k < mylast[p] ? alpha : 0.f;
                             const float ioma = rcp_approx(1.0f - alpha);
                             const float Tk = T[p] * ioma;
