@@ -150,7 +150,8 @@ def algorithmic_bytes(st, n, planes, views, pixels, tiles):
     pairs = n * views
     inst = st["instances"]
     vis = st["visible_pairs"]
-    passes_pairs, passes_inst = 4, 2
+    bits = max(1, math.ceil(math.log2(max(tiles, 2))))
+    passes_pairs, passes_inst = 4, 2 * math.ceil(math.ceil(bits / 8) / 2)  # 8-bit digits, an even count
     return {
         "project": n * P + pairs * (48 + 8 + 4),
         # one digit-count read of the keys, then per pass keys + values read and written
@@ -688,7 +689,8 @@ def main():
             warmup=args.warmup, ms_per_step=round(ms, 4), higher_is_better=True, scaling="weak",
             vs_baseline=None, dtype="f32", data="synthetic",
             config=config_dict(hmp, res["c"], res["cams"], args.config, world),
-            raster_variant=dict(fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1]),
+            raster_variant=dict(tile=res["tuned"]["tile"],
+                                fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1]),
                                 bwd=dict(batch=res["tuned"]["bwd"][0], pixels_per_thread=res["tuned"]["bwd"][1])),
             skipped_steps=res["counts"]["skipped_steps"],
             overflow=res["counts"]["overflow"],

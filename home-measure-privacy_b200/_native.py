@@ -32,7 +32,7 @@ class GsConfig(ctypes.Structure):
                 ("alpha_min", c_float), ("t_min", c_float), ("sh_degree", c_int32), ("rect_mode", c_int32),
                 ("batched", c_int32), ("use_graph", c_int32), ("device", c_int32), ("autotune", c_int32),
                 ("raster_batch", c_int32), ("lpt_order", c_int32), ("instance_capacity", c_int32),
-                ("raster_ppt", c_int32), ("tile_cull", c_int32), ("reserved", c_int32 * 1)]
+                ("raster_ppt", c_int32), ("tile_cull", c_int32), ("tile_size", c_int32)]
 
 
 class GsAdamConfig(ctypes.Structure):
@@ -49,7 +49,7 @@ class GsStats(ctypes.Structure):
     _fields_ = [("instances", c_int64), ("instance_capacity", c_int64), ("visible_pairs", c_int64),
                 ("tiles", c_int64), ("pixels", c_int64), ("kernel_launches_per_step", c_int64),
                 ("raster_batch", c_int32), ("raster_threads", c_int32), ("overflow", c_int32),
-                ("raster_variant", c_int32)]
+                ("raster_variant", c_int32), ("tile_size", c_int32)]
 
 
 class GsError(RuntimeError):

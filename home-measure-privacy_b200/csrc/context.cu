@@ -151,10 +151,12 @@ struct GsContext {
     bool status_pending = false;
     int64_t skipped_steps = 0;
     unsigned int debug_wait_host = 0;   // source of gs_debug_lookback_wait's copy
+    bool tuned = false;                 // cfg.autotune has run
     // last forward
     int last_first = -1, last_count = 0, last_batched = 1;
     bool have_loss = false;
     // raster tuning: shared-memory batch and pixels per thread of each kernel
+    int tile = GS_TILE;                 // tile edge of binning and raster (8, 16 or 32)
     int batch_fwd = 256, batch_bwd = 256, ppt_fwd = 1, ppt_bwd = 1;
     int ctas_fwd = 0, ctas_bwd = 0;
     // graphs
@@ -284,7 +286,7 @@ static int end_record(GsContext* c) {
 // ---------------------------------------------------------------------------------
 // Views and layout.
 // ---------------------------------------------------------------------------------
-static ViewDesc make_desc(const GsCamera& cam) {
+static ViewDesc make_desc(const GsCamera& cam, int tile) {
     ViewDesc d;
     memset(&d, 0, sizeof d);
     const float* m = cam.view;
@@ -297,8 +299,9 @@ static ViewDesc make_desc(const GsCamera& cam) {
     for (int j = 0; j < 3; j++) d.campos[j] = -(d.R[0 * 3 + j] * d.t[0] + d.R[1 * 3 + j] * d.t[1] + d.R[2 * 3 + j] * d.t[2]);
     d.width = cam.width;
     d.height = cam.height;
-    d.tiles_x = (cam.width + GS_TILE - 1) / GS_TILE;
-    d.tiles_y = (cam.height + GS_TILE - 1) / GS_TILE;
+    d.tile = tile;
+    d.tiles_x = (cam.width + tile - 1) / tile;
+    d.tiles_y = (cam.height + tile - 1) / tile;
     d.loss_blocks_x = (cam.width + loss_block_w() - 1) / loss_block_w();
     d.loss_blocks_y = (cam.height + loss_block_h() - 1) / loss_block_h();
     return d;
@@ -316,7 +319,7 @@ static int layout(GsContext* c) {
     c->vdesc.resize(c->cams.size());
     int64_t pix = 0, tiles = 0, lb = 0;
     for (size_t v = 0; v < c->cams.size(); v++) {
-        ViewDesc d = make_desc(c->cams[v]);
+        ViewDesc d = make_desc(c->cams[v], c->tile);
         d.tile_offset = (int)tiles;
         d.pixel_offset = (int)pix;
         d.loss_block_offset = (int)lb;
@@ -419,8 +422,8 @@ static int size_instances(GsContext* c, int64_t cap) {
 static SegInfo* seg_ptr(GsContext* c, int idx) { return c->segs.as<SegInfo>() + idx; }
 
 static int persistent_ctas(GsContext* c, bool backward) {
-    const int per_sm = backward ? raster_max_ctas_per_sm(c->batch_bwd, c->ppt_bwd, true)
-                                : raster_max_ctas_per_sm(c->batch_fwd, c->ppt_fwd, false);
+    const int per_sm = backward ? raster_max_ctas_per_sm(c->tile, c->batch_bwd, c->ppt_bwd, true)
+                                : raster_max_ctas_per_sm(c->tile, c->batch_fwd, c->ppt_fwd, false);
     return c->num_sms * per_sm;
 }
 
@@ -571,7 +574,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
         r.work_counter = &st->work_counter;
     }
     CKI(mark(c, ST_RASTER_FWD));
-    launch_raster_fwd(r, c->batch_fwd, c->ppt_fwd, batched ? c->ctas_fwd : 0, c->stream);
+    launch_raster_fwd(r, c->tile, c->batch_fwd, c->ppt_fwd, batched ? c->ctas_fwd : 0, c->stream);
     count_launches(c, ST_RASTER_FWD, 1);
     CK(cudaGetLastError());
     return GS_OK;
@@ -618,7 +621,7 @@ static int enqueue_backward_view(GsContext* c, int first, int step_first, int co
         r.work_counter = &st->work_counter_bwd;
         if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
     }
-    launch_raster_bwd(r, c->batch_bwd, c->ppt_bwd, batched ? c->ctas_bwd : 0, c->stream);
+    launch_raster_bwd(r, c->tile, c->batch_bwd, c->ppt_bwd, batched ? c->ctas_bwd : 0, c->stream);
     count_launches(c, ST_RASTER_BWD, 1);
     CKI(mark(c, ST_PROJECT_BWD));
     ProjectBwdArgs pb;
@@ -889,6 +892,7 @@ void gs_config_default(GsConfig* cfg) {
     cfg->raster_batch = 256;
     cfg->raster_ppt = 1;
     cfg->tile_cull = 1;
+    cfg->tile_size = GS_TILE;
     cfg->lpt_order = 1;
 }
 
@@ -941,8 +945,12 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if (cfg.raster_batch != 64 && cfg.raster_batch != 128 && cfg.raster_batch != 256)
         return fail(GS_ERR_INVALID_ARG, "raster_batch must be 64, 128 or 256");
     if (cfg.raster_ppt == 0) cfg.raster_ppt = 1;
-    if (cfg.raster_ppt != 1 && cfg.raster_ppt != 2 && cfg.raster_ppt != 4 && cfg.raster_ppt != 8)
-        return fail(GS_ERR_INVALID_ARG, "raster_ppt must be 1, 2, 4 or 8");
+    if (cfg.tile_size == 0) cfg.tile_size = GS_TILE;
+    if (cfg.tile_size != 8 && cfg.tile_size != 16 && cfg.tile_size != 32)
+        return fail(GS_ERR_INVALID_ARG, "tile_size must be 8, 16 or 32");
+    if (!raster_variant_ok(cfg.tile_size, cfg.raster_ppt))
+        return fail(GS_ERR_INVALID_ARG, "raster_ppt %d does not exist for %d-pixel tiles (8: 1, 2; 16: 1, 2, 4, 8; 32: 2, 4, 8)",
+                    cfg.raster_ppt, cfg.tile_size);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) {
@@ -961,6 +969,7 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     c->device_name = prop.name;
     c->degree = cfg.sh_degree;
     c->planes = num_planes(cfg.sh_degree);
+    c->tile = cfg.tile_size;
     c->batch_fwd = c->batch_bwd = cfg.raster_batch;
     c->ppt_fwd = c->ppt_bwd = cfg.raster_ppt;
     int rc = GS_OK;
@@ -1407,7 +1416,7 @@ int gs_render(GsContext* c, const GsCamera* cam, float* rgb_out, float* state_ou
         for (int y = 0; y < d.height; y++)
             for (int x = 0; x < d.width; x++) {
                 const size_t p = (size_t)y * d.width + x;
-                const uint2 r = rg[(size_t)(y / GS_TILE) * d.tiles_x + x / GS_TILE];
+                const uint2 r = rg[(size_t)(y / d.tile) * d.tiles_x + x / d.tile];
                 state_out[p * 2] = T[p];
                 state_out[p * 2 + 1] = (float)(L[p] - r.x);
             }
@@ -1540,6 +1549,11 @@ static int train_step_impl(GsContext* c, const GsAdamConfig* ad, const GsLossCon
     }
     int kind;
     CKI(targets_kind(c, first, count, &kind));
+    if (c->cfg.autotune && !c->tuned && first == 0 && count == c->V) {
+        c->tuned = true;  // timing only: the photos need not be on the device yet
+        CKI(poll_status(c, true));
+        CKI(gs_autotune(c, nullptr));
+    }
     CKI(size_pairs(c, count));
     CKI(poll_status(c, false));
     CKI(ensure_capacity(c, first, count));
@@ -1843,9 +1857,10 @@ int gs_get_stats(GsContext* c, GsStats* out) {
     }
     out->kernel_launches_per_step = c->last_step_launches;
     out->raster_batch = c->batch_bwd;
-    out->raster_threads = 256 / c->ppt_bwd;
+    out->raster_threads = c->tile * c->tile / c->ppt_bwd;
     out->raster_variant = (int32_t)((uint32_t)c->batch_fwd | ((uint32_t)c->ppt_fwd << 12) |
                                     ((uint32_t)c->batch_bwd << 16) | ((uint32_t)c->ppt_bwd << 28));
+    out->tile_size = c->tile;
     out->overflow = (int32_t)c->skipped_steps;
     return GS_OK;
 }
@@ -2227,10 +2242,28 @@ int gs_scene_extent(const GsCamera* cams, int32_t count, float* extent_out) {
     return GS_OK;
 }
 
-// Raster tuning: times the persistent forward and backward raster kernels, each for every
-// (shared-memory batch, pixels per thread) variant, on all training views after one
-// forward and loss, and keeps the fastest of each.  The choice is cached per device and
-// workload in `cache_path` (lines "key|fwd_batch fwd_ppt bwd_batch bwd_ppt").
+// Switches the context to tiles of `tile` pixels: views re-laid out, the instance
+// capacity measured again by the next forward, graphs re-captured.
+static int set_tile(GsContext* c, int tile) {
+    if (c->tile == tile) return GS_OK;
+    c->tile = tile;
+    CKI(layout(c));
+    c->inst_cap_valid = false;
+    c->have_loss = false;
+    c->last_first = -1;
+    c->ctas_fwd = persistent_ctas(c, false);
+    c->ctas_bwd = persistent_ctas(c, true);
+    drop_graphs(c);
+    return GS_OK;
+}
+
+// Tuning: for each tile size (16, 8, 32) the persistent forward and backward raster
+// kernels are timed for every (shared-memory batch, pixels per thread) variant that
+// exists for it, on all training views after one forward and loss, keeping the fastest
+// of each; then the tile size's whole forward + loss + backward (projection, binning,
+// blending, loss, their backward; no update) is timed with those variants, and the tile
+// size with the fastest is kept.  The choice is cached per device and workload in
+// `cache_path` (lines "key|tile fwd_batch fwd_ppt bwd_batch bwd_ppt").
 int gs_autotune(GsContext* c, const char* cache_path) {
     CTX_CHECK(c);
     if (c->V < 1 || c->n <= 0) return fail(GS_ERR_STATE, "autotune needs Gaussians and views");
@@ -2239,7 +2272,8 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     char key[256];
     snprintf(key, sizeof key, "%s n=%d views=%d px=%lld deg=%d", c->device_name.c_str(), c->n, c->V,
              (long long)c->total_pixels, c->degree);
-    auto apply = [&](int bf, int pf, int bb, int pb) {
+    auto apply = [&](int tile, int bf, int pf, int bb, int pb) -> int {
+        CKI(set_tile(c, tile));
         c->batch_fwd = bf;
         c->ppt_fwd = pf;
         c->batch_bwd = bb;
@@ -2247,83 +2281,119 @@ int gs_autotune(GsContext* c, const char* cache_path) {
         c->ctas_fwd = persistent_ctas(c, false);
         c->ctas_bwd = persistent_ctas(c, true);
         drop_graphs(c);
+        return GS_OK;
     };
+    auto ok_batch = [](int b) { return b == 64 || b == 128 || b == 256; };
     if (cache_path) {
         FILE* f = fopen(cache_path, "r");
         if (f) {
             char line[512];
             while (fgets(line, sizeof line, f)) {
-                int bf, pf, bb, pb;
+                int t, bf, pf, bb, pb;
                 char* bar = strrchr(line, '|');
                 if (!bar) continue;
                 *bar = 0;
-                if (strcmp(line, key) == 0 && sscanf(bar + 1, "%d %d %d %d", &bf, &pf, &bb, &pb) == 4 &&
-                    (bf == 64 || bf == 128 || bf == 256) && (bb == 64 || bb == 128 || bb == 256) &&
-                    (pf == 1 || pf == 2 || pf == 4 || pf == 8) && (pb == 1 || pb == 2 || pb == 4 || pb == 8)) {
+                if (strcmp(line, key) == 0 && sscanf(bar + 1, "%d %d %d %d %d", &t, &bf, &pf, &bb, &pb) == 5 &&
+                    ok_batch(bf) && ok_batch(bb) && raster_variant_ok(t, pf) && raster_variant_ok(t, pb)) {
                     fclose(f);
-                    apply(bf, pf, bb, pb);
-                    return GS_OK;
+                    return apply(t, bf, pf, bb, pb);
                 }
             }
             fclose(f);
         }
     }
     const int saved_batched = c->cfg.batched;
-    c->cfg.batched = 1;
-    int rc = run_forward(c, 0, c->V);
-    c->cfg.batched = saved_batched;
-    CKI(rc);
-    GsLossConfig lc{0.2f, 1};
-    CKI(gs_loss(c, &lc, nullptr));
     DevStatus* st = c->status.as<DevStatus>();
     const int batches[3] = {64, 128, 256};
-    float best_f = 1e30f, best_b = 1e30f;
-    int bf = c->batch_fwd, pf = c->ppt_fwd, bb = c->batch_bwd, pb = c->ppt_bwd;
-    RasterArgs r = raster_args(c, 0, c->V);
-    if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
-    for (int bi = 0; bi < 3; bi++)
-        for (int ppt = 1; ppt <= 8; ppt *= 2)
-            for (int backward = 0; backward < 2; backward++) {
-                const int ctas = c->num_sms * raster_max_ctas_per_sm(batches[bi], ppt, backward != 0);
-                float total = 0.f;
-                for (int rep = 0; rep < 3; rep++) {
-                    CK(cudaMemsetAsync(&st->work_counter, 0, 8, c->stream));
-                    if (backward) {
-                        CK(cudaMemsetAsync(c->sg8.p, 0, (size_t)c->V * c->n_pad * 32, c->stream));
-                        CK(cudaMemsetAsync(c->sg1.p, 0, (size_t)c->V * c->n_pad * 4, c->stream));
+    const int tiles[3] = {16, 8, 32};
+    const GsLossConfig lc{0.2f, 1};
+    cudaEvent_t e0 = c->user_events[62], e1 = c->user_events[63];
+    float best_total = 1e30f;
+    int best[5] = {c->tile, c->batch_fwd, c->ppt_fwd, c->batch_bwd, c->ppt_bwd};
+    for (int ti = 0; ti < 3; ti++) {
+        const int tile = tiles[ti];
+        CKI(set_tile(c, tile));
+        c->cfg.batched = 1;
+        int rc = run_forward(c, 0, c->V);
+        c->cfg.batched = saved_batched;
+        CKI(rc);
+        CKI(gs_loss(c, &lc, nullptr));
+        float best_f = 1e30f, best_b = 1e30f;
+        int bf = 0, pf = 0, bb = 0, pb = 0;
+        RasterArgs r = raster_args(c, 0, c->V);
+        if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
+        for (int bi = 0; bi < 3; bi++)
+            for (int ppt = 1; ppt <= 8; ppt *= 2) {
+                if (!raster_variant_ok(tile, ppt)) continue;
+                for (int backward = 0; backward < 2; backward++) {
+                    const int ctas = c->num_sms * raster_max_ctas_per_sm(tile, batches[bi], ppt, backward != 0);
+                    float total = 0.f;
+                    for (int rep = 0; rep < 3; rep++) {
+                        CK(cudaMemsetAsync(&st->work_counter, 0, 8, c->stream));
+                        if (backward) {
+                            CK(cudaMemsetAsync(c->sg8.p, 0, (size_t)c->V * c->n_pad * 32, c->stream));
+                            CK(cudaMemsetAsync(c->sg1.p, 0, (size_t)c->V * c->n_pad * 4, c->stream));
+                        }
+                        CK(cudaEventRecord(e0, c->stream));
+                        if (backward) {
+                            r.work_counter = &st->work_counter_bwd;
+                            launch_raster_bwd(r, tile, batches[bi], ppt, ctas, c->stream);
+                        } else {
+                            r.work_counter = &st->work_counter;
+                            launch_raster_fwd(r, tile, batches[bi], ppt, ctas, c->stream);
+                        }
+                        CK(cudaEventRecord(e1, c->stream));
+                        CK(cudaGetLastError());
+                        CK(cudaEventSynchronize(e1));
+                        float ms = 0.f;
+                        CK(cudaEventElapsedTime(&ms, e0, e1));
+                        if (rep > 0) total += ms;
                     }
-                    CK(cudaEventRecord(c->user_events[62], c->stream));
-                    if (backward) {
-                        r.work_counter = &st->work_counter_bwd;
-                        launch_raster_bwd(r, batches[bi], ppt, ctas, c->stream);
-                    } else {
-                        r.work_counter = &st->work_counter;
-                        launch_raster_fwd(r, batches[bi], ppt, ctas, c->stream);
+                    if (backward && total < best_b) {
+                        best_b = total;
+                        bb = batches[bi];
+                        pb = ppt;
                     }
-                    CK(cudaEventRecord(c->user_events[63], c->stream));
-                    CK(cudaGetLastError());
-                    CK(cudaEventSynchronize(c->user_events[63]));
-                    float ms = 0.f;
-                    CK(cudaEventElapsedTime(&ms, c->user_events[62], c->user_events[63]));
-                    if (rep > 0) total += ms;
-                }
-                if (backward && total < best_b) {
-                    best_b = total;
-                    bb = batches[bi];
-                    pb = ppt;
-                }
-                if (!backward && total < best_f) {
-                    best_f = total;
-                    bf = batches[bi];
-                    pf = ppt;
+                    if (!backward && total < best_f) {
+                        best_f = total;
+                        bf = batches[bi];
+                        pf = ppt;
+                    }
                 }
             }
-    apply(bf, pf, bb, pb);
+        CKI(apply(tile, bf, pf, bb, pb));
+        // The tile size's whole forward, loss and backward with its best variants.
+        float total = 0.f;
+        for (int rep = 0; rep < 3; rep++) {
+            CK(cudaMemsetAsync(c->acc.p, 0, sizeof(double) * 2 * (GS_MAX_VIEWS + 1), c->stream));
+            CK(cudaEventRecord(e0, c->stream));
+            CKI(enqueue_forward(c, 0, c->V, true));
+            CKI(enqueue_loss_view(c, 0, c->V, lc, kind));
+            CKI(enqueue_backward_view(c, 0, 0, c->V, true, false));
+            CK(cudaEventRecord(e1, c->stream));
+            CK(cudaEventSynchronize(e1));
+            CKI(read_status(c));
+            if (c->status_host->overflow) return fail(GS_ERR_CAPACITY, "key instances overflowed while tuning");
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0) total += ms;
+        }
+        if (total < best_total) {
+            best_total = total;
+            best[0] = tile;
+            best[1] = bf;
+            best[2] = pf;
+            best[3] = bb;
+            best[4] = pb;
+        }
+    }
+    CKI(apply(best[0], best[1], best[2], best[3], best[4]));
     c->have_loss = false;
+    c->last_first = -1;
     if (cache_path) {
         FILE* f = fopen(cache_path, "a");
         if (f) {
-            fprintf(f, "%s|%d %d %d %d\n", key, bf, pf, bb, pb);
+            fprintf(f, "%s|%d %d %d %d %d\n", key, best[0], best[1], best[2], best[3], best[4]);
             fclose(f);
         }
     }

@@ -16,8 +16,7 @@
 #include <string.h>
 #include <math.h>
 
-#define GS_TILE 16
-#define GS_TILE_PIXELS (GS_TILE * GS_TILE)
+#define GS_TILE 16                    // default tile edge (the reference's); contexts may use 8 or 32
 #define GS_MAX_VIEWS 64
 #define GS_MAX_PLANES 59
 #define GS_KEY_SENTINEL 0x7FFFFFFFu   // above +inf's bits: culled pairs sort last
@@ -35,7 +34,7 @@ struct ViewDesc {
     int tile_offset;     // first global tile id of this view
     int pixel_offset;    // first pixel of this view in the per-pixel buffers
     int loss_blocks_x, loss_blocks_y, loss_block_offset;
-    int pad;
+    int tile;            // tile edge in pixels (8, 16 or 32; the same for every view)
 };
 
 // Step status kept on the device; mirrored to pinned host memory.  The first 24 bytes
@@ -227,24 +226,26 @@ __host__ __device__ __forceinline__ Projected project_exact(const ViewDesc& vw, 
     return o;
 }
 
-// Tile rectangle [x0, x1) x [y0, y1) of a splat.  mode 0: the reference's GPU BIN
-// (trainer/gpu.js:632-635, f32, clamps so off-screen-right/bottom splats still land in
-// the last tile column/row); mode 1: tileLists (trainer/gpu.js:456-461, f64 like JS,
+// Tile rectangle [x0, x1) x [y0, y1) of a splat for tiles of `tile` pixels.  mode 0:
+// the reference's GPU BIN (trainer/gpu.js:632-635, f32, clamps so off-screen-right/bottom
+// splats still land in the last tile column/row; its 1/16 is 1/tile here, exact for the
+// powers of two allowed); mode 1: tileLists (trainer/gpu.js:456-461, f64 like JS,
 // inclusive bounds made half-open).
 __host__ __device__ __forceinline__ void tile_rect(float u, float v, float r, int tiles_x, int tiles_y,
-                                                  int mode, int& x0, int& x1, int& y0, int& y1) {
+                                                  int mode, int tile, int& x0, int& x1, int& y0, int& y1) {
     if (mode == 0) {
         const float tx = (float)(tiles_x - 1), ty = (float)(tiles_y - 1);
-        const float fx0 = fminf(fmaxf(floorf(xmul(xsub(xsub(u, r), 0.5f), 0.0625f)), 0.0f), tx);
-        const float fx1 = fminf(fmaxf(floorf(xmul(xsub(xadd(u, r), 0.5f), 0.0625f)), -1.0f), tx);
-        const float fy0 = fminf(fmaxf(floorf(xmul(xsub(xsub(v, r), 0.5f), 0.0625f)), 0.0f), ty);
-        const float fy1 = fminf(fmaxf(floorf(xmul(xsub(xadd(v, r), 0.5f), 0.0625f)), -1.0f), ty);
+        const float it = 1.0f / (float)tile;
+        const float fx0 = fminf(fmaxf(floorf(xmul(xsub(xsub(u, r), 0.5f), it)), 0.0f), tx);
+        const float fx1 = fminf(fmaxf(floorf(xmul(xsub(xadd(u, r), 0.5f), it)), -1.0f), tx);
+        const float fy0 = fminf(fmaxf(floorf(xmul(xsub(xsub(v, r), 0.5f), it)), 0.0f), ty);
+        const float fy1 = fminf(fmaxf(floorf(xmul(xsub(xadd(v, r), 0.5f), it)), -1.0f), ty);
         x0 = (int)fx0; x1 = (int)xadd(fx1, 1.0f);
         y0 = (int)fy0; y1 = (int)xadd(fy1, 1.0f);
     } else {
-        const double du = (double)u, dv = (double)v, dr = (double)r;
-        const double fx0 = floor((du - dr - 0.5) / 16.0), fx1 = floor((du + dr - 0.5) / 16.0);
-        const double fy0 = floor((dv - dr - 0.5) / 16.0), fy1 = floor((dv + dr - 0.5) / 16.0);
+        const double du = (double)u, dv = (double)v, dr = (double)r, dt = (double)tile;
+        const double fx0 = floor((du - dr - 0.5) / dt), fx1 = floor((du + dr - 0.5) / dt);
+        const double fy0 = floor((dv - dr - 0.5) / dt), fy1 = floor((dv + dr - 0.5) / dt);
         x0 = (int)fmax(0.0, fx0); x1 = (int)fmin((double)(tiles_x - 1), fx1) + 1;
         y0 = (int)fmax(0.0, fy0); y1 = (int)fmin((double)(tiles_y - 1), fy1) + 1;
     }

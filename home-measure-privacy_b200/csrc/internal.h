@@ -153,9 +153,12 @@ struct RasterArgs {
     unsigned int* work_counter;     // persistent queue head (nullptr = one CTA per tile)
     const uint32_t* tile_order;     // optional permutation of the tiles (heavy first)
 };
-void launch_raster_fwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s);
-void launch_raster_bwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s);
-int raster_max_ctas_per_sm(int batch, int ppt, bool backward);
+// Raster variants: tile edge (8, 16 or 32 pixels), shared-memory batch (64, 128 or 256
+// splats), pixels per thread (raster_variant_ok lists the pairs that exist).
+bool raster_variant_ok(int tile, int ppt);
+void launch_raster_fwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s);
+void launch_raster_bwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s);
+int raster_max_ctas_per_sm(int tile, int batch, int ppt, bool backward);
 
 // Blends (pixel, splat evaluations) of the last forward, added to *out.
 void launch_blend_count(const ViewDesc* views, int view_first, int num_views, int max_pixels, const uint2* ranges,

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
         if (finite) p = project_exact(vw, mean, Sig, a.near_plane, a.dilation);
         int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
         if (p.ok && isfinite(p.u) && isfinite(p.v) && isfinite(p.radius))
-            tile_rect(p.u, p.v, p.radius, vw.tiles_x, vw.tiles_y, a.rect_mode, x0, x1, y0, y1);
+            tile_rect(p.u, p.v, p.radius, vw.tiles_x, vw.tiles_y, a.rect_mode, vw.tile, x0, x1, y0, y1);
         else
             p.ok = false;
         uint32_t count = (p.ok && x1 > x0 && y1 > y0) ? (uint32_t)((x1 - x0) * (y1 - y0)) : 0u;
@@ -100,13 +100,15 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
                 const float H1 = (float)vw.height - 0.5f, W1 = (float)vw.width - 0.5f;
                 const float xlo_lim = fmaxf(p.u - p.radius, 0.5f), xhi_lim = fminf(p.u + p.radius, W1);
                 const float slack = 1e-3f * (1.0f + p.radius);
+                const int T = vw.tile;
+                const float Tm = (float)T - 0.5f, iT = 1.0f / (float)T;
                 count = 0;
 #pragma unroll
                 for (int r = 0; r < GS_SPAN_ROWS; r++) {
                     const int ty = y0 + r;
                     if (ty >= y1) break;
-                    float yl = fmaxf(fmaxf((float)(ty * GS_TILE) + 0.5f, p.v - p.radius), p.v - ymax) - p.v;
-                    float yh = fminf(fminf(fminf((float)(ty * GS_TILE) + 15.5f, H1), p.v + p.radius), p.v + ymax) - p.v;
+                    float yl = fmaxf(fmaxf((float)(ty * T) + 0.5f, p.v - p.radius), p.v - ymax) - p.v;
+                    float yh = fminf(fminf(fminf((float)(ty * T) + Tm, H1), p.v + p.radius), p.v + ymax) - p.v;
                     int xs = 0, xe = 0;
                     if (thr > 0.f && yl <= yh) {
                         const float dr = fminf(fmaxf(-ystat, yl), yh);   // right edge maximiser
@@ -116,9 +118,9 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
                         const float xhi = fminf(p.u + (-B * dr + sr) * iA + slack, xhi_lim);
                         const float xlo = fmaxf(p.u + (-B * dl - sl) * iA - slack, xlo_lim);
                         if (xlo <= xhi) {
-                            // Tile tx holds pixel centres [16 tx + 0.5, 16 tx + 15.5].
-                            xs = max(x0, __float2int_ru((xlo - 15.5f) * 0.0625f));
-                            xe = min(x1, __float2int_rd((xhi - 0.5f) * 0.0625f) + 1);
+                            // Tile tx holds pixel centres [T tx + 0.5, T tx + T - 0.5].
+                            xs = max(x0, __float2int_ru((xlo - Tm) * iT));
+                            xe = min(x1, __float2int_rd((xhi - 0.5f) * iT) + 1);
                             if (xe < xs) xe = xs;
                         }
                     }

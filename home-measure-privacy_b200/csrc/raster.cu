@@ -1,18 +1,18 @@
 // Tiled alpha blending, forward and backward.
 //
-// A 16 x 16 pixel tile is 8 groups of 8 x 4 pixels (group g = 4 xh + yq: x half xh, y
-// quarter yq); lane l of a warp holds pixel (l & 7, l >> 3) of each group the warp owns.
-// With PPT pixels per thread a CTA of 256 / PPT threads owns one tile and warp w owns PPT
-// groups: all eight (PPT 8, one warp per tile), or x half w & 1 and quarters
-// (w >> 1) PPT ... (w >> 1) PPT + PPT - 1.  The tile's depth-ordered list is walked in
-// batches: the CTA stages a batch of splat records (32-byte geometry + 16-byte colour,
-// gathered by pair index) in shared memory with cp.async, double-buffered so the next
-// batch's gather overlaps the current batch's blending.  Each warp then takes the staged
-// splats 32 at a time, a lane per splat, and finds for each the warp's groups that its
-// alpha >= alpha_min ellipse (clipped to its bounding square) can reach and whose pixels
-// are still live; the splats with any such group are blended in order, group by group,
-// and only those groups are evaluated.  Skipped groups have alpha = 0 at every pixel, so
-// results are those of evaluating every pixel against every splat.
+// A tile of TILE x TILE pixels (8, 16 or 32; 16 is the reference's) is cut into groups of
+// 8 x 4 pixels; lane l of a warp holds pixel (l & 7, l >> 3) of each group the warp owns.
+// With PPT pixels per thread a CTA of TILE^2 / PPT threads owns one tile and each warp a
+// block of PPT groups (1 x PPT groups, or 2 x 4 with 8 pixels per thread; Lay below).
+// The tile's depth-ordered list is walked in batches: the CTA stages a batch of splat
+// records (32-byte geometry + 16-byte colour, gathered by pair index) in shared memory
+// with cp.async, double-buffered so the next batch's gather overlaps the current
+// batch's blending.  Each warp then takes the staged splats 32 at a time, a lane per
+// splat, and finds for each the warp's groups that its alpha >= alpha_min ellipse
+// (clipped to its bounding square) can reach and whose pixels are still live; the splats
+// with any such group are blended in order, group by group, and only those groups are
+// evaluated.  Skipped groups have alpha = 0 at every pixel, so results are those of
+// evaluating every pixel against every splat, whatever the tile size.
 //
 // Forward = FORWARD (trainer/gpu.js:105-137) with alphaAt (:91-103): square bounding-box
 // test, Gaussian power, alpha = min(0.99, opacity * exp(power)), skip below 1/255, stop
@@ -68,15 +68,22 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return r;
 }
 
-// Groups of a warp: x half and y quarter of its p-th group.
-template <int PPT>
-__device__ __forceinline__ int group_xh(int w, int p) {
-    return PPT == 8 ? (p >> 2) : (w & 1);
-}
-template <int PPT>
-__device__ __forceinline__ int group_yq(int w, int p) {
-    return PPT == 8 ? (p & 3) : ((w >> 1) * PPT + p);
-}
+// Layout of a CTA over one TILE x TILE tile with PPT pixels per thread: the tile is
+// GX x GY groups of 8 x 4 pixels; each warp owns a block of WX x WY groups (WX = 2 when
+// a thread has 8 pixels, else 1) and its p-th group is column p / WY, row p % WY of that
+// block.
+template <int TILE, int PPT>
+struct Lay {
+    static constexpr int NT = TILE * TILE / PPT;  // threads per CTA
+    static constexpr int GX = TILE / 8, GY = TILE / 4;
+    static constexpr int WX = PPT == 8 ? 2 : 1;
+    static constexpr int WY = PPT / WX;
+    static constexpr int NWX = GX / WX;           // warps across the tile
+    static_assert(WX <= GX && WY <= GY && NT >= 32 && NT <= 1024, "no such raster layout");
+    __device__ static int xg(int w, int p) { return (w % NWX) * WX + p / WY; }
+    __device__ static int yg(int w, int p) { return (w / NWX) * WY + p % WY; }
+};
+
 template <int PPT>
 constexpr uint32_t all_groups() {
     return (1u << PPT) - 1u;
@@ -92,8 +99,9 @@ struct TileInfo {
     float cx0, cy0;              // centre of the tile's first pixel
 };
 
-template <int PPT>
+template <int TILE, int PPT>
 __device__ __forceinline__ TileInfo<PPT> tile_info(const RasterArgs& a, int item) {
+    using L = Lay<TILE, PPT>;
     TileInfo<PPT> ti;
     const int local = a.tile_order ? (int)a.tile_order[item] : item;
     ti.g = a.tile_first + local;
@@ -104,11 +112,11 @@ __device__ __forceinline__ TileInfo<PPT> tile_info(const RasterArgs& a, int item
     const int lt = ti.g - vw.tile_offset;
     const int tx = lt % vw.tiles_x, ty = lt / vw.tiles_x;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x0 = tx * GS_TILE, y0 = ty * GS_TILE;
+    const int x0 = tx * TILE, y0 = ty * TILE;
 #pragma unroll
     for (int p = 0; p < PPT; p++) {
-        ti.x[p] = x0 + 8 * group_xh<PPT>(w, p) + (lane & 7);
-        ti.y[p] = y0 + 4 * group_yq<PPT>(w, p) + (lane >> 3);
+        ti.x[p] = x0 + 8 * L::xg(w, p) + (lane & 7);
+        ti.y[p] = y0 + 4 * L::yg(w, p) + (lane >> 3);
         ti.inside[p] = ti.x[p] < vw.width && ti.y[p] < vw.height;
     }
     ti.width = vw.width;
@@ -182,34 +190,33 @@ __device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g
 }
 
 // The warp's groups (bit p = its p-th group) where splat (g0, g1) can give a pixel
-// centre alpha >= alpha_min.  Per x band of 8 pixel centres (the warp's half, or both):
-// the y-range of the ellipse A dx^2 + 2B dx dy + C dy^2 <= thr (thr = g1.w) over the
-// band, clipped to the splat's bounding square |dx|, |dy| <= radius, against each
-// group's 4 pixel rows.  Over a band the ellipse's upper edge is concave and its lower
-// edge convex in dx, so the range's ends sit at the stationary points
-// dx = -/+ B sqrt(thr / (A det)) clamped to the band.  Conservative: the slack covers the
-// approximate instructions; the pixels' own tests decide.
-template <int PPT>
+// centre alpha >= alpha_min.  Per x band of 8 pixel centres the warp covers: the y-range
+// of the ellipse A dx^2 + 2B dx dy + C dy^2 <= thr (thr = g1.w) over the band, clipped to
+// the splat's bounding square |dx|, |dy| <= radius, against each of its groups' 4 pixel
+// rows.  Over a band the ellipse's upper edge is concave and its lower edge convex in
+// dx, so the range's ends sit at the stationary points dx = -/+ B sqrt(thr / (A det))
+// clamped to the band.  Conservative: the slack covers the approximate instructions; the
+// pixels' own tests decide.
+template <int TILE, int PPT>
 __device__ __forceinline__ uint32_t group_mask(const float4& g0, const float4& g1, float cx0, float cy0, int w) {
+    using L = Lay<TILE, PPT>;
     const float thr = g1.w;
     if (!(thr > 0.f)) return 0u;
     const float u = g0.x, v = g0.y, A = g0.z, B = g0.w, C = g1.x, r = g1.z;
-    constexpr int NH = PPT == 8 ? 2 : 1;
-    constexpr int NQ = PPT == 8 ? 4 : PPT;
+    const float bx0 = cx0 + 8.0f * (float)L::xg(w, 0) - u;  // first pixel centre of the warp's first band, from u
+    const float by0 = cy0 + 4.0f * (float)L::yg(w, 0) - v;  // first pixel-centre row of its first group row, from v
     if (conic_kappa(A, B, C) > KAPPA_CULL_MAX) {
         // Near-degenerate conic: its ellipse arithmetic is not trusted, cull by the
         // bounding square |dx|, |dy| <= radius alone.
         uint32_t m = 0u;
 #pragma unroll
-        for (int hh = 0; hh < NH; hh++) {
-            const int xhalf = PPT == 8 ? hh : (w & 1);
-            const float bx = cx0 + 8.0f * (float)xhalf - u;
+        for (int hh = 0; hh < L::WX; hh++) {
+            const float bx = bx0 + 8.0f * (float)hh;
             if (bx > r || bx + 7.0f < -r) continue;
 #pragma unroll
-            for (int i = 0; i < NQ; i++) {
-                const int q = PPT == 8 ? i : ((w >> 1) * PPT + i);
-                const float y0 = cy0 + 4.0f * (float)q - v;
-                if (y0 <= r && y0 + 3.0f >= -r) m |= 1u << (PPT == 8 ? hh * 4 + i : i);
+            for (int i = 0; i < L::WY; i++) {
+                const float y0 = by0 + 4.0f * (float)i;
+                if (y0 <= r && y0 + 3.0f >= -r) m |= 1u << (hh * L::WY + i);
             }
         }
         return m;
@@ -222,9 +229,8 @@ __device__ __forceinline__ uint32_t group_mask(const float4& g0, const float4& g
     const float slack = 1e-3f * (1.0f + r);
     uint32_t m = 0u;
 #pragma unroll
-    for (int hh = 0; hh < NH; hh++) {
-        const int xhalf = PPT == 8 ? hh : (w & 1);
-        const float bx = cx0 + 8.0f * (float)xhalf - u;  // first pixel centre of the band, from u
+    for (int hh = 0; hh < L::WX; hh++) {
+        const float bx = bx0 + 8.0f * (float)hh;  // first pixel centre of the band, from u
         const float xl = fmaxf(fmaxf(bx, -r), -xr - slack);
         const float xh = fminf(fminf(bx + 7.0f, r), xr + slack);
         if (xl > xh) continue;
@@ -233,10 +239,9 @@ __device__ __forceinline__ uint32_t group_mask(const float4& g0, const float4& g
         const float hi = fminf((-B * du + sqrt_approx(fmaxf(C * thr - det * du * du, 0.f))) * iC + slack, r);
         const float lo = fmaxf((-B * dl - sqrt_approx(fmaxf(C * thr - det * dl * dl, 0.f))) * iC - slack, -r);
 #pragma unroll
-        for (int i = 0; i < NQ; i++) {
-            const int q = PPT == 8 ? i : ((w >> 1) * PPT + i);
-            const float y0 = cy0 + 4.0f * (float)q - v;  // first pixel-centre row of the group, from v
-            if (y0 <= hi && y0 + 3.0f >= lo) m |= 1u << (PPT == 8 ? hh * 4 + i : i);
+        for (int i = 0; i < L::WY; i++) {
+            const float y0 = by0 + 4.0f * (float)i;  // first pixel-centre row of the group, from v
+            if (y0 <= hi && y0 + 3.0f >= lo) m |= 1u << (hh * L::WY + i);
         }
     }
     return m;
@@ -301,11 +306,18 @@ __device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, co
 
 // Resident CTAs per SM the register allocation is sized for (fewer threads with more
 // pixels each get more registers per thread).
-constexpr int fwd_min_ctas(int ppt) { return ppt == 8 ? 20 : (ppt == 4 ? 12 : 4 * ppt); }
-constexpr int bwd_min_ctas(int ppt) { return ppt == 8 ? 16 : (ppt == 4 ? 10 : (ppt == 2 ? 7 : 4)); }
+// For 16 x 16 tiles; other tiles scale the count by the threads per CTA.
+constexpr int fwd_min_ctas16(int ppt) { return ppt == 8 ? 20 : (ppt == 4 ? 12 : 4 * ppt); }
+constexpr int bwd_min_ctas16(int ppt) { return ppt == 8 ? 16 : (ppt == 4 ? 10 : (ppt == 2 ? 7 : 4)); }
+constexpr int scale_ctas(int c16, int tile) {
+    return c16 * 256 / (tile * tile) < 1 ? 1 : (c16 * 256 / (tile * tile) > 32 ? 32 : c16 * 256 / (tile * tile));
+}
+constexpr int fwd_min_ctas(int tile, int ppt) { return scale_ctas(fwd_min_ctas16(ppt), tile); }
+constexpr int bwd_min_ctas(int tile, int ppt) { return scale_ctas(bwd_min_ctas16(ppt), tile); }
 
-template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kernel(RasterArgs a) {
+template <int TILE, int BATCH, int PPT>
+__global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) raster_fwd_kernel(RasterArgs a) {
+    using L = Lay<TILE, PPT>;
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -316,14 +328,14 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
     const float qthr = __log2f(a.alpha_min);
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
-        const TileInfo<PPT> ti = tile_info<PPT>(a, item);
+        const TileInfo<PPT> ti = tile_info<TILE, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x, end = rg.y;
-        float pxf[PPT == 8 ? 2 : 1], pyf[PPT], T[PPT], cr[PPT], cg[PPT], cb[PPT];
+        float pxf[L::WX], pyf[PPT], T[PPT], cr[PPT], cg[PPT], cb[PPT];
         uint32_t last[PPT];
         bool done[PPT];
-        pxf[0] = (float)ti.x[0] + 0.5f;
-        if (PPT == 8) pxf[PPT == 8 ? 1 : 0] = (float)ti.x[PPT - 1] + 0.5f;
+#pragma unroll
+        for (int b = 0; b < L::WX; b++) pxf[b] = (float)ti.x[b * L::WY] + 0.5f;  // the warp's x bands
         uint32_t gdone = 0u;  // warp-uniform: groups whose pixels have all stopped
 #pragma unroll
         for (int p = 0; p < PPT; p++) {
@@ -354,7 +366,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
             const float4* qs = s_q[buf];
             for (int gb = 0; gb < cnt && gdone != all_groups<PPT>(); gb += 32) {
                 const int jl = gb + lane;
-                const uint32_t gm = jl < cnt ? group_mask<PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) : 0u;
+                const uint32_t gm = jl < cnt ? group_mask<TILE, PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) : 0u;
                 uint32_t live = __ballot_sync(FULL_MASK, (gm & ~gdone) != 0u);
                 while (live) {
                     const int jj = __ffs(live) - 1;
@@ -368,14 +380,14 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas(PPT)) raster_fwd_kerne
                     const bool exact = c.w < 0.f;  // warp-uniform
                     const float qlo = qthr - fabsf(c.w), qhi = qthr + fabsf(c.w);
                     const uint32_t pos = b0 + (uint32_t)j + 1u;
-                    XTerm xt[PPT == 8 ? 2 : 1];
-                    xt[0] = xterm(q, pxf[0] - g0.x, g1.z);
-                    if (PPT == 8) xt[PPT == 8 ? 1 : 0] = xterm(q, pxf[PPT == 8 ? 1 : 0] - g0.x, g1.z);
+                    XTerm xt[L::WX];
+#pragma unroll
+                    for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
 #pragma unroll
                     for (int p = 0; p < PPT; p++) {
                         if (!(m & (1u << p))) continue;
                         // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
-                        float alpha = alpha_at(g0, g1, q, xt[PPT == 8 ? (p >> 2) : 0], pyf[p] - g0.y, a.alpha_max,
+                        float alpha = alpha_at(g0, g1, q, xt[p / L::WY], pyf[p] - g0.y, a.alpha_max,
                                                a.alpha_min, qlo, qhi, exact);
                         alpha = done[p] ? 0.f : alpha;
                         const float wgt = alpha * T[p];
@@ -442,8 +454,9 @@ __device__ __forceinline__ float warp_sum8_transposed(float v[8]) {
     return v[0];
 }
 
-template <int BATCH, int PPT>
-__global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kernel(RasterArgs a) {
+template <int TILE, int BATCH, int PPT>
+__global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) raster_bwd_kernel(RasterArgs a) {
+    using L = Lay<TILE, PPT>;
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -467,13 +480,13 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
     }
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
     while (item < a.num_tiles) {
-        const TileInfo<PPT> ti = tile_info<PPT>(a, item);
+        const TileInfo<PPT> ti = tile_info<TILE, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
-        float pxf[PPT == 8 ? 2 : 1], pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
+        float pxf[L::WX], pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
         uint32_t mylast[PPT], gmax[PPT];
-        pxf[0] = (float)ti.x[0] + 0.5f;
-        if (PPT == 8) pxf[PPT == 8 ? 1 : 0] = (float)ti.x[PPT - 1] + 0.5f;
+#pragma unroll
+        for (int b = 0; b < L::WX; b++) pxf[b] = (float)ti.x[b * L::WY] + 0.5f;  // the warp's x bands
         unsigned int wmax = start;
 #pragma unroll
         for (int p = 0; p < PPT; p++) {
@@ -534,7 +547,7 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
                         uint32_t act = 0u;  // groups with a pixel whose last is past this entry
 #pragma unroll
                         for (int p = 0; p < PPT; p++) act |= kl < gmax[p] ? (1u << p) : 0u;
-                        if (act) gm = group_mask<PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) & act;
+                        if (act) gm = group_mask<TILE, PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) & act;
                     }
                     uint32_t live = __ballot_sync(FULL_MASK, gm != 0u);
                     while (live) {
@@ -549,9 +562,9 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
                         const float4 c = cs[j];
                         const bool exact = c.w < 0.f;  // warp-uniform
                     const float qlo = qthr - fabsf(c.w), qhi = qthr + fabsf(c.w);
-                        XTerm xt[PPT == 8 ? 2 : 1];
-                        xt[0] = xterm(q, pxf[0] - g0.x, g1.z);
-                        if (PPT == 8) xt[PPT == 8 ? 1 : 0] = xterm(q, pxf[PPT == 8 ? 1 : 0] - g0.x, g1.z);
+                        XTerm xt[L::WX];
+#pragma unroll
+                        for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
                         // Per pixel: colour terms and the moments of dP = dL/dpower over the
                         // offsets (sum dP, dP dx, dP dy, dP dx^2, dP dx dy, dP dy^2); the
                         // splat's conic and opacity turn the warp sums into the gradients of
@@ -563,7 +576,7 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
                             if (!(m & (1u << p))) continue;
                             // Branch-free per lane: alpha = 0 adds zeros and leaves T
                             // (T / 1) and dL.behind as they are.
-                            const XTerm& x = xt[PPT == 8 ? (p >> 2) : 0];
+                            const XTerm& x = xt[p / L::WY];
                             const float dx = x.dx, dy = pyf[p] - g0.y;
                             float alpha = alpha_at(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi, exact);
                             alpha = k < mylast[p] ? alpha : 0.f;
@@ -616,54 +629,74 @@ __global__ void __launch_bounds__(256 / PPT, bwd_min_ctas(PPT)) raster_bwd_kerne
     }
 }
 
-// Variant = (shared-memory batch, pixels per thread); the autotuner picks one.
-template <int BATCH, int PPT>
+// Variant = (tile edge, shared-memory batch, pixels per thread); the autotuner picks one.
+template <int TILE, int BATCH, int PPT>
 static void fwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
-    raster_fwd_kernel<BATCH, PPT><<<ctas, 256 / PPT, 0, s>>>(a);
+    raster_fwd_kernel<TILE, BATCH, PPT><<<ctas, Lay<TILE, PPT>::NT, 0, s>>>(a);
 }
-template <int BATCH, int PPT>
+template <int TILE, int BATCH, int PPT>
 static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
-    raster_bwd_kernel<BATCH, PPT><<<ctas, 256 / PPT, 0, s>>>(a);
+    raster_bwd_kernel<TILE, BATCH, PPT><<<ctas, Lay<TILE, PPT>::NT, 0, s>>>(a);
 }
 
-#define RASTER_BATCHES(FN, batch, P, ...)                    \
+#define RASTER_BATCHES(FN, T, batch, P, ...)                 \
     do {                                                     \
         switch (batch) {                                     \
-            case 64: FN<64, P>(__VA_ARGS__); break;          \
-            case 128: FN<128, P>(__VA_ARGS__); break;        \
-            default: FN<256, P>(__VA_ARGS__); break;         \
+            case 64: FN<T, 64, P>(__VA_ARGS__); break;       \
+            case 128: FN<T, 128, P>(__VA_ARGS__); break;     \
+            default: FN<T, 256, P>(__VA_ARGS__); break;      \
         }                                                    \
     } while (0)
 
-#define RASTER_SWITCH(FN, batch, ppt, ...)                                      \
-    do {                                                                        \
-        if ((ppt) == 8) RASTER_BATCHES(FN, batch, 8, __VA_ARGS__);             \
-        else if ((ppt) == 4) RASTER_BATCHES(FN, batch, 4, __VA_ARGS__);        \
-        else if ((ppt) == 2) RASTER_BATCHES(FN, batch, 2, __VA_ARGS__);        \
-        else RASTER_BATCHES(FN, batch, 1, __VA_ARGS__);                         \
+// The (tile, pixels per thread) pairs that exist: 8 x 8 tiles with 1 or 2 pixels per
+// thread, 16 x 16 with 1, 2, 4 or 8, 32 x 32 with 2, 4 or 8 (raster_variant_ok).
+#define RASTER_SWITCH(FN, tile, batch, ppt, ...)                                           \
+    do {                                                                                   \
+        if ((tile) == 8) {                                                                 \
+            if ((ppt) == 2) RASTER_BATCHES(FN, 8, batch, 2, __VA_ARGS__);                  \
+            else RASTER_BATCHES(FN, 8, batch, 1, __VA_ARGS__);                             \
+        } else if ((tile) == 32) {                                                         \
+            if ((ppt) == 8) RASTER_BATCHES(FN, 32, batch, 8, __VA_ARGS__);                 \
+            else if ((ppt) == 4) RASTER_BATCHES(FN, 32, batch, 4, __VA_ARGS__);            \
+            else RASTER_BATCHES(FN, 32, batch, 2, __VA_ARGS__);                            \
+        } else {                                                                           \
+            if ((ppt) == 8) RASTER_BATCHES(FN, 16, batch, 8, __VA_ARGS__);                 \
+            else if ((ppt) == 4) RASTER_BATCHES(FN, 16, batch, 4, __VA_ARGS__);            \
+            else if ((ppt) == 2) RASTER_BATCHES(FN, 16, batch, 2, __VA_ARGS__);            \
+            else RASTER_BATCHES(FN, 16, batch, 1, __VA_ARGS__);                            \
+        }                                                                                  \
     } while (0)
 
-void launch_raster_fwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
-    const int ctas = a.work_counter ? persistent_ctas : a.num_tiles;
-    if (ctas <= 0 || a.num_tiles <= 0) return;
-    RASTER_SWITCH(fwd_launch, batch, ppt, a, ctas, s);
+bool raster_variant_ok(int tile, int ppt) {
+    if (tile == 8) return ppt == 1 || ppt == 2;
+    if (tile == 16) return ppt == 1 || ppt == 2 || ppt == 4 || ppt == 8;
+    if (tile == 32) return ppt == 2 || ppt == 4 || ppt == 8;
+    return false;
 }
 
-void launch_raster_bwd(const RasterArgs& a, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
+void launch_raster_fwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
     const int ctas = a.work_counter ? persistent_ctas : a.num_tiles;
     if (ctas <= 0 || a.num_tiles <= 0) return;
-    RASTER_SWITCH(bwd_launch, batch, ppt, a, ctas, s);
+    RASTER_SWITCH(fwd_launch, tile, batch, ppt, a, ctas, s);
 }
 
-template <int BATCH, int PPT>
+void launch_raster_bwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
+    const int ctas = a.work_counter ? persistent_ctas : a.num_tiles;
+    if (ctas <= 0 || a.num_tiles <= 0) return;
+    RASTER_SWITCH(bwd_launch, tile, batch, ppt, a, ctas, s);
+}
+
+template <int TILE, int BATCH, int PPT>
 static void occ(int* n, bool backward) {
-    if (backward) cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_bwd_kernel<BATCH, PPT>, 256 / PPT, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_fwd_kernel<BATCH, PPT>, 256 / PPT, 0);
+    if (backward)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_bwd_kernel<TILE, BATCH, PPT>, Lay<TILE, PPT>::NT, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_fwd_kernel<TILE, BATCH, PPT>, Lay<TILE, PPT>::NT, 0);
 }
 
-int raster_max_ctas_per_sm(int batch, int ppt, bool backward) {
+int raster_max_ctas_per_sm(int tile, int batch, int ppt, bool backward) {
     int n = 0;
-    RASTER_SWITCH(occ, batch, ppt, &n, backward);
+    RASTER_SWITCH(occ, tile, batch, ppt, &n, backward);
     cudaGetLastError();
     return n < 1 ? 1 : n;
 }
@@ -718,7 +751,7 @@ __global__ void blend_count_kernel(const ViewDesc* views, int view_first, const 
     unsigned long long n = 0;
     if (px < vw.width * vw.height) {
         const int x = px % vw.width, y = px / vw.width;
-        const int tile = vw.tile_offset + (y / GS_TILE) * vw.tiles_x + x / GS_TILE;
+        const int tile = vw.tile_offset + (y / vw.tile) * vw.tiles_x + x / vw.tile;
         const uint32_t start = ranges[tile].x, l = last[(size_t)vw.pixel_offset + px];
         n = l > start ? (unsigned long long)(l - start) : 0ull;
     }

@@ -64,8 +64,8 @@ class Renderer:
     """createRenderer() result.  One CUDA context (device, stream, buffers)."""
 
     def __init__(self, gpuTiles=True, sh_degree=0, near=0.2, batched=True, use_graph=True, device=0,
-                 raster_batch=256, lpt_order=True, rect_mode=None, instance_capacity=0, raster_ppt=1,
-                 tile_cull=True):
+                 raster_batch=256, lpt_order=True, rect_mode=None, instance_capacity=0, raster_ppt=None,
+                 tile_cull=True, tile_size=16):
         self.lib = N.load()
         cfg = N.GsConfig()
         self.lib.gs_config_default(ctypes.byref(cfg))
@@ -77,8 +77,10 @@ class Renderer:
         cfg.raster_batch = int(raster_batch)
         cfg.lpt_order = 1 if lpt_order else 0
         cfg.instance_capacity = int(instance_capacity)
-        cfg.raster_ppt = int(raster_ppt)
+        # pixels per raster thread: 1 (16- and 8-pixel tiles) or 4 (32-pixel tiles) unless given
+        cfg.raster_ppt = int(raster_ppt) if raster_ppt is not None else (4 if int(tile_size) == 32 else 1)
         cfg.tile_cull = 1 if tile_cull else 0
+        cfg.tile_size = int(tile_size)
         # gpuTiles=False is the reference's CPU tileLists path (trainer/gpu.js:703, :799-806):
         # here the binning always runs on the GPU, with tileLists' tile rectangle.
         cfg.rect_mode = int(rect_mode) if rect_mode is not None else (0 if gpuTiles else 1)
@@ -470,10 +472,13 @@ class Renderer:
         N.check(self.lib.gs_debug_lookback_wait(self.ctx, int(polls)))
 
     def autotune(self, cache_path=None):
-        """Picks the raster variants; returns {fwd: (batch, ppt), bwd: (batch, ppt)}."""
+        """Picks the tile size and raster variants; returns {tile, fwd: (batch, ppt),
+        bwd: (batch, ppt)}."""
         N.check(self.lib.gs_autotune(self.ctx, cache_path.encode() if cache_path else None))
-        v = self.stats()["raster_variant"]
-        return dict(fwd=(v & 0xfff, (v >> 12) & 0xf), bwd=((v >> 16) & 0xfff, (v >> 28) & 0xf))
+        st = self.stats()
+        v = st["raster_variant"]
+        return dict(tile=int(st["tile_size"]), fwd=(v & 0xfff, (v >> 12) & 0xf),
+                    bwd=((v >> 16) & 0xfff, (v >> 28) & 0xf))
 
     def stage_times(self):
         ms = np.zeros(N.GS_NUM_STAGES, np.float64)

@@ -67,7 +67,8 @@ typedef struct GsConfig {
                               0 = the plain path: one launch per view per stage        */
     int32_t use_graph;     /* 1 = capture each training step in a CUDA graph           */
     int32_t device;        /* CUDA device ordinal                                     */
-    int32_t autotune;      /* 1 = pick raster batch/threads by timing on first step   */
+    int32_t autotune;      /* 1 = run gs_autotune before the first training step over
+                              all views                                                 */
     int32_t raster_batch;  /* Gaussians per shared-memory batch: 64, 128 or 256        */
     int32_t lpt_order;     /* 1 = persistent raster takes heavy tiles first           */
     int32_t instance_capacity; /* initial key-instance capacity; 0 = measured by a first
@@ -80,7 +81,9 @@ typedef struct GsConfig {
                               alpha >= alpha_min ellipse reaches the tile: same images
                               and gradients, fewer entries; 0 = the reference's
                               rectangle lists (rect_mode), whose keys match BIN + SORT  */
-    int32_t reserved[1];
+    int32_t tile_size;     /* tile edge in pixels: 16 (default, the reference's,
+                              trainer/gpu.js:118), 8 or 32; 0 = 16.  Images are the same
+                              for every size; gs_autotune may change it                 */
 } GsConfig;
 
 /* Adam settings.  The per-group learning rates are the reference's (trainer/gpu.js:846,
@@ -412,6 +415,7 @@ typedef struct GsStats {
     int32_t raster_threads;
     int32_t overflow;
     int32_t raster_variant;  /* fwd batch | fwd ppt << 12 | bwd batch << 16 | bwd ppt << 28 */
+    int32_t tile_size;       /* tile edge in pixels in use (gs_autotune may have changed it) */
 } GsStats;
 GS_API int gs_get_stats(GsContext* ctx, GsStats* out);
 
@@ -435,10 +439,13 @@ GS_API int gs_get_tile_lists(GsContext* ctx, int32_t view, uint32_t* list_out,
  * depth, r, g, b, valid. */
 GS_API int gs_get_splats(GsContext* ctx, int32_t view, float* splats12_out);
 
-/* Raster tuning: measures the raster kernels' candidate variants (splats per shared-
- * memory batch, pixels per thread) on the current views and keeps the fastest forward
- * and backward.  cache_path (optional): a text file that records the choice per device
- * and workload. */
+/* Tuning (no counterpart in the reference, whose tile size, workgroup size and batch are
+ * fixed): for each tile size (16, 8 and 32 pixels) times the raster kernels' candidate
+ * variants (splats per shared-memory batch, pixels per thread) on the current views and
+ * keeps the fastest forward and backward, then times that tile size's whole forward,
+ * loss and backward (no update) and keeps the tile size with the fastest.  Images do not
+ * depend on the choice.  The views need targets.  cache_path (optional): a text file
+ * that records the choice per device and workload. */
 GS_API int gs_autotune(GsContext* ctx, const char* cache_path);
 
 /* ---- loss gradient without allocation ------------------------------------------------

@@ -450,3 +450,61 @@ def test_pipelined_host_step_matches_synchronous(hmp):
     lr_max = max(a for a in (hmp.adam_config().lr_color, hmp.adam_config().lr_opacity))
     assert np.mean(diff < 1e-5) > 0.995
     assert diff.max() < 4 * 2 * lr_max
+
+
+# ------------------------------------------------------------------------------ tile sizes
+def test_tile_sizes_agree(hmp):
+    """8-, 16- and 32-pixel tiles with every (batch, pixels per thread) variant that exists
+    for them: the same images bit for bit (each pixel blends the same splats in the same
+    order, whatever the tiles) and the same gradients up to atomic order."""
+    rec = hmp.synthetic_scene(40_000, 3, 17, "normal", (-4.5, 0.7), (0.0, 1.5))
+    tg = hmp.scene.jitter_means(rec, 18)
+    cams = hmp.ring_cameras([(333, 250), (512, 384), (200, 411)], 4.0)
+
+    def run(tile, ppt, batch):
+        with make(hmp, 3, tile_size=tile, raster_ppt=ppt, raster_batch=batch) as r:
+            r.set_gaussians(tg)
+            r.set_views(cams)
+            timgs = r.forward(0, 3)
+            off = 0
+            for v, c in enumerate(cams):
+                px = c["width"] * c["height"] * 3
+                r.set_target(v, timgs[off:off + px])
+                off += px
+            r.set_gaussians(rec)
+            img = r.forward(0, 3)
+            assert r.stats()["tile_size"] == tile
+            r.loss(ssim=0.2, window=1)
+            return img, r.backward()
+
+    ref_img, ref_g = run(16, 1, 256)
+    for tile, ppts in ((8, (1, 2)), (16, (8,)), (32, (2, 4, 8))):
+        for ppt in ppts:
+            for batch in (64, 256):
+                img, g = run(tile, ppt, batch)
+                assert np.array_equal(img, ref_img), (tile, ppt, batch)
+                assert rel_err(g, ref_g) < 1e-5, (tile, ppt, batch)
+
+
+def test_autotune_picks_a_tile_size_and_trains_the_same(hmp):
+    """gs_autotune (tile size, batch, pixels per thread) leaves the results unchanged."""
+    rec = hmp.synthetic_scene(30_000, 1, 19, "normal", (-4.0, 0.6), (0.0, 1.5))
+    cams = hmp.ring_cameras([(320, 240), (400, 300)], 4.0)
+    out = {}
+    for tuned in (False, True):
+        with make(hmp, 1) as r:
+            r.set_gaussians(hmp.scene.jitter_means(rec, 20))
+            r.set_views(cams)
+            imgs = r.forward(0, 2)
+            off = 0
+            for v, c in enumerate(cams):
+                px = c["width"] * c["height"] * 3
+                r.set_target(v, imgs[off:off + px])
+                off += px
+            r.set_gaussians(rec)
+            if tuned:
+                t = r.autotune()
+                assert t["tile"] in (8, 16, 32)
+            out[tuned] = (r.forward(0, 2), r.train_step(ssim=0.2, window=1))
+    assert np.array_equal(out[True][0], out[False][0])
+    assert abs(out[True][1] - out[False][1]) < 1e-6
