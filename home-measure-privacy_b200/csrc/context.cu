@@ -2248,6 +2248,10 @@ static int set_tile(GsContext* c, int tile) {
     if (c->tile == tile) return GS_OK;
     c->tile = tile;
     CKI(layout(c));
+    // The instance buffers are sized again for this tile size: the sort and emission
+    // grids follow their capacity, which another tile size may have grown.
+    for (DevBuf* b : {&c->ikeys, &c->ivals, &c->ikeys_alt, &c->ivals_alt, &c->block_first_pair}) release(*b);
+    c->inst_cap = 0;
     c->inst_cap_valid = false;
     c->have_loss = false;
     c->last_first = -1;

@@ -34,7 +34,6 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
     const bool real = i < a.n;
     const int np = a.n_pad;
     float mean[3], ls[3], q[4], ol = 0.f, dc[3];
-    float sh[3][NK > 0 ? NK : 1];
     if (real) {
 #pragma unroll
         for (int k = 0; k < 3; k++) {
@@ -45,10 +44,6 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
 #pragma unroll
         for (int k = 0; k < 4; k++) q[k] = __ldg(a.params + (6 + k) * np + i);
         ol = __ldg(a.params + 10 * np + i);
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-            for (int k = 0; k < NK; k++) sh[c][k] = __ldg(a.params + (14 + c * NK + k) * np + i);
     }
     float Sig[9];
     bool finite = false;
@@ -65,6 +60,7 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
     // the approximate arithmetic below and the raster's own rounding.
     const float thr_g = opacity > 0.f ? 2.0f * (__logf(opacity) - __logf(a.alpha_min)) + 1e-3f : -1.0f;
     unsigned int my_visible = 0, ok_views = 0;
+    unsigned long long ok_mask = 0ull;  // views the Gaussian projects into (SH colour below)
     for (int s = 0; s < a.num_views; s++) {
         const ViewDesc& vw = a.views[a.view_first + s];
         const size_t pair = (size_t)(a.pair_slot_first + s) * np + i;
@@ -136,27 +132,11 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
             count |= GS_PCOUNT_RECT;
         }
         const bool covers = (count & ~GS_PCOUNT_RECT) != 0u;
-        float r = 0.f, g = 0.f, b = 0.f;
-        if (p.ok) {
-            r = dc[0]; g = dc[1]; b = dc[2];
-            if (DEG > 0) {
-                float dx = mean[0] - vw.campos[0], dy = mean[1] - vw.campos[1], dz = mean[2] - vw.campos[2];
-                const float inv = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
-                dx *= inv; dy *= inv; dz *= inv;
-                float Y[NK > 0 ? NK : 1];
-                sh_basis(DEG, dx, dy, dz, Y);
-#pragma unroll
-                for (int k = 0; k < NK; k++) {
-                    r += Y[k] * sh[0][k];
-                    g += Y[k] * sh[1][k];
-                    b += Y[k] * sh[2][k];
-                }
-            }
-        }
+        if (DEG == 0) a.rgb[pair] = p.ok ? make_float4(dc[0], dc[1], dc[2], 1.0f) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (p.ok) ok_mask |= 1ull << s;
         a.geo0[pair] = make_float4(p.ok ? p.u : 0.f, p.ok ? p.v : 0.f, p.ok ? p.a : 0.f, p.ok ? p.b : 0.f);
         a.geo1[pair] = make_float4(p.ok ? p.c : 0.f, p.ok ? opacity : 0.f, p.ok ? p.radius : 0.f,
                                    p.ok ? p.depth : 0.f);
-        a.rgb[pair] = make_float4(r, g, b, p.ok ? 1.0f : 0.0f);
         a.keys[pair] = covers ? __float_as_uint(p.depth) : GS_KEY_SENTINEL;
         a.pcount[pair] = covers ? count : 0u;
         if (covers) {
@@ -168,6 +148,38 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
         }
         my_visible += covers ? 1u : 0u;
         ok_views += p.ok ? 1u : 0u;
+    }
+    if (DEG > 0) {
+        // SH colour per view, after the geometry: the 3 (K - 1) band coefficients are
+        // loaded only now, so they do not hold registers through the projection.
+        float sh[3][NK > 0 ? NK : 1];
+        if (ok_mask) {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int k = 0; k < NK; k++) sh[c][k] = __ldg(a.params + (14 + c * NK + k) * np + i);
+        }
+        for (int s = 0; s < a.num_views; s++) {
+            const size_t pair = (size_t)(a.pair_slot_first + s) * np + i;
+            float4 col = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ok_mask >> s & 1ull) {
+                const ViewDesc& vw = a.views[a.view_first + s];
+                float r = dc[0], g = dc[1], b = dc[2];
+                float dx = mean[0] - vw.campos[0], dy = mean[1] - vw.campos[1], dz = mean[2] - vw.campos[2];
+                const float inv = rsqrtf(fmaxf(dx * dx + dy * dy + dz * dz, 1e-30f));
+                dx *= inv; dy *= inv; dz *= inv;
+                float Y[NK > 0 ? NK : 1];
+                sh_basis(DEG, dx, dy, dz, Y);
+#pragma unroll
+                for (int k = 0; k < NK; k++) {
+                    r += Y[k] * sh[0][k];
+                    g += Y[k] * sh[1][k];
+                    b += Y[k] * sh[2][k];
+                }
+                col = make_float4(r, g, b, 1.0f);
+            }
+            a.rgb[pair] = col;
+        }
     }
     if (a.stats_cnt && ok_views) a.stats_cnt[i] += (float)ok_views;  // STATS count (trainer/gpu.js:494-496)
     if (a.visible) {

@@ -30,6 +30,8 @@
 //
 // In the persistent mode a fixed grid pulls (view, tile) work items from a global
 // counter, in an order that puts the longest tile lists first.
+#include <type_traits>
+
 #include "internal.h"
 
 namespace gs {
@@ -283,14 +285,15 @@ __device__ __forceinline__ XTerm xterm(const float4& q, float dx, float radius) 
 
 // alpha at the pixel (column term xt, row offset dy), or 0 when the pixel skips the
 // splat: 2^q by the fast exp2; within [qlo, qhi) around the alpha_min threshold the
-// reference expression decides.  Otherwise branch-free.  `exact` (warp-uniform: a splat
-// property) takes q from the reference's power, rounded as the reference rounds it,
-// instead of the expanded quadratic, for elongated conics whose expanded terms are far
-// larger than q.
+// reference expression decides.  Otherwise branch-free.  EXACT (a splat property; the
+// kernels instantiate the group loop for each) takes q from the reference's power,
+// rounded as the reference rounds it, instead of the expanded quadratic, for elongated
+// conics whose expanded terms are far larger than q.
+template <bool EXACT>
 __device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, const XTerm& xt,
-                                          float dy, float amax, float amin, float qlo, float qhi, bool exact) {
+                                          float dy, float amax, float amin, float qlo, float qhi) {
     float e;
-    if (exact) {
+    if (EXACT) {
         const float power = __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(__fmul_rn(__fmul_rn(g0.z, xt.dx), xt.dx),
                                                                  __fmul_rn(__fmul_rn(g1.x, dy), dy))),
                                       __fmul_rn(__fmul_rn(g0.w, xt.dx), dy));
@@ -383,21 +386,27 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) r
                     XTerm xt[L::WX];
 #pragma unroll
                     for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
+                    // The group loop, instantiated for both exponent forms (a uniform branch).
+                    auto groups = [&](auto ex) {
+                        constexpr bool EXACT = decltype(ex)::value;
 #pragma unroll
-                    for (int p = 0; p < PPT; p++) {
-                        if (!(m & (1u << p))) continue;
-                        // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
-                        float alpha = alpha_at(g0, g1, q, xt[p / L::WY], pyf[p] - g0.y, a.alpha_max,
-                                               a.alpha_min, qlo, qhi, exact);
-                        alpha = done[p] ? 0.f : alpha;
-                        const float wgt = alpha * T[p];
-                        cr[p] += c.x * wgt;
-                        cg[p] += c.y * wgt;
-                        cb[p] += c.z * wgt;
-                        T[p] *= 1.0f - alpha;
-                        last[p] = alpha != 0.f ? pos : last[p];
-                        done[p] = done[p] || T[p] <= a.t_min;
-                    }
+                        for (int p = 0; p < PPT; p++) {
+                            if (!(m & (1u << p))) continue;
+                            // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
+                            float alpha = alpha_at<EXACT>(g0, g1, q, xt[p / L::WY], pyf[p] - g0.y, a.alpha_max,
+                                                          a.alpha_min, qlo, qhi);
+                            alpha = done[p] ? 0.f : alpha;
+                            const float wgt = alpha * T[p];
+                            cr[p] += c.x * wgt;
+                            cg[p] += c.y * wgt;
+                            cb[p] += c.z * wgt;
+                            T[p] *= 1.0f - alpha;
+                            last[p] = alpha != 0.f ? pos : last[p];
+                            done[p] = done[p] || T[p] <= a.t_min;
+                        }
+                    };
+                    if (exact) groups(std::true_type{});
+                    else groups(std::false_type{});
                 }
 #pragma unroll
                 for (int p = 0; p < PPT; p++)
@@ -571,6 +580,9 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                         // (opacity logit, u, v, A, B, C) after the reduction.
                         float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                         float v8 = 0.f;
+                        // The group loop, instantiated for both exponent forms (a uniform branch).
+                        auto groups = [&](auto ex) {
+                            constexpr bool EXACT = decltype(ex)::value;
 #pragma unroll
                         for (int p = 0; p < PPT; p++) {
                             if (!(m & (1u << p))) continue;
@@ -578,7 +590,7 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                             // (T / 1) and dL.behind as they are.
                             const XTerm& x = xt[p / L::WY];
                             const float dx = x.dx, dy = pyf[p] - g0.y;
-                            float alpha = alpha_at(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi, exact);
+                            float alpha = alpha_at<EXACT>(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi);
                             alpha = k < mylast[p] ? alpha : 0.f;
                             const float ioma = rcp_approx(1.0f - alpha);
                             const float Tk = T[p] * ioma;
@@ -602,6 +614,9 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                             v[7] += dPx * dy;
                             v8 += dPy * dy;
                         }
+                        };
+                        if (exact) groups(std::true_type{});
+                        else groups(std::false_type{});
                         float s = warp_sum8_transposed(v);
                         float s8 = v8;
 #pragma unroll

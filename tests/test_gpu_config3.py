@@ -101,8 +101,9 @@ def test_config3_parameter_gradients_fp64(hmp, oracle, cfg3, n, view):
 def test_adam_several_steps_matches_oracle(hmp, oracle):
     """Six training steps (t = 1..6, moments carried): each step's update equals the
     restated ADAM applied to the gradients that step computed (read back from the
-    context), element by element within 1e-6 of the update plus the rounding of the
-    parameter itself (two units in its last place)."""
+    context), element by element within 1e-6 of the update (1e-7 of the learning rate at
+    least) plus four units in the last place of the parameter (the roundings of
+    p + update and of the quaternion's renormalisation)."""
     rec = hmp.synthetic_scene(20_000, 3, 41, "normal", (-4.0, 0.6), (0.0, 1.5))
     cams = hmp.ring_cameras([(320, 240), (400, 300)], 4.0)
     tg = hmp.scene.jitter_means(rec, 42)
@@ -132,10 +133,18 @@ def test_adam_several_steps_matches_oracle(hmp, oracle):
             p = before.copy()
             oracle.adam(p, g, m, v, 3, t, lr6)
             upd = (p - before).astype(np.float64)
-            tol = 1e-6 * np.abs(upd) + 2.0 * np.spacing(np.abs(p)).astype(np.float64)
+            # 1e-6 of the update, or 1e-7 of the plane's learning rate where the update is
+            # small (a first moment that cancelled amplifies rounding relative to it), plus
+            # the rounding of p + update on either side and of the quaternion's
+            # renormalisation
+            lr_plane = np.array([lr6[2]] * 3 + [lr6[3]] * 3 + [lr6[4]] * 4 + [lr6[1]] + [lr6[0]] * 3 +
+                                [lr6[5]] * (p.shape[1] - 14), np.float64)
+            tol = 1e-6 * np.maximum(np.abs(upd), 0.1 * lr_plane) + 4.0 * np.spacing(np.abs(p)).astype(np.float64)
             err = np.abs(after.astype(np.float64) - p)
-            worst = float((err / tol).max())
-            assert worst <= 1.0, (t, worst, float(err.max()))
+            ratio = err / tol
+            worst = float(ratio.max())
+            at = np.unravel_index(int(ratio.argmax()), ratio.shape)
+            assert worst <= 1.0, (t, worst, int(at[1]), float(p[at]), float(after[at]), float(upd[at]))
             moved = np.abs(after - before).max(axis=0)
             assert np.all(moved[:14] > 0), t  # every parameter group was updated
         assert n == r.lib.gs_num_gaussians(r.ctx)
