@@ -398,7 +398,10 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
 constexpr int EM_THREADS = 256;
 constexpr int EM_ITEMS = 8;
 constexpr int EM_CHUNK = EM_THREADS * EM_ITEMS;
-constexpr int EM_OUT = 1024;
+#ifndef GS_EM_OUT
+#define GS_EM_OUT 1024
+#endif
+constexpr int EM_OUT = GS_EM_OUT;  // instances per expansion block
 
 int emit_chunk_items() { return EM_CHUNK; }
 int emit_out_items() { return EM_OUT; }
