@@ -30,8 +30,6 @@
 //
 // In the persistent mode a fixed grid pulls (view, tile) work items from a global
 // counter, in an order that puts the longest tile lists first.
-#include <type_traits>
-
 #include "internal.h"
 
 namespace gs {
@@ -173,9 +171,9 @@ __device__ __forceinline__ float conic_kappa(float A, float B, float C) {
 // on the rounding of q and of the reference's own exponent, which grows with the
 // conic's elongation (for near-degenerate splats seen from close by, the terms of q are
 // thousands of times q itself).  Above KAPPA_EXACT the rounding of the reference's own
-// exponent shows in alpha's value, so such splats take their exponent from the
-// reference's power, rounded as the reference rounds it (alpha_at's exact form, marked by
-// a negative s_c.w), with the plain 1e-4 band.
+// exponent shows in alpha's value, so such splats (about 1 % of the benchmark's list
+// entries) get an unbounded band: every pixel takes alpha from the reference expression.
+// s_c.w holds the band's lower end qlo; its upper end is 2 log2(alpha_min) - qlo.
 __device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g1, float4* s_q, float4* s_c,
                                               float log_amin, float qthr) {
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
@@ -186,8 +184,9 @@ __device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g
         const float lop = op > 0.f ? __log2f(op) : -1e30f;
         s_g1[t].w = op > 0.f ? 2.0f * (__logf(op) - log_amin) * (1.0f + kappa * 1.52587890625e-05f) + 1e-3f : -1.0f;
         s_q[t] = make_float4(-0.5f * LOG2E * g0.z, -LOG2E * g0.w, -0.5f * LOG2E * g1.x, lop);
-        s_c[t].w = kappa > KAPPA_EXACT ? -ALPHA_Q_BAND
-                                       : ALPHA_Q_BAND + 7.62939453125e-06f * kappa * fmaxf(lop - qthr, 1.0f);  // 2^-17
+        s_c[t].w = kappa > KAPPA_EXACT
+                       ? -1e30f
+                       : qthr - (ALPHA_Q_BAND + 7.62939453125e-06f * kappa * fmaxf(lop - qthr, 1.0f));  // 2^-17
     }
 }
 
@@ -284,23 +283,11 @@ __device__ __forceinline__ XTerm xterm(const float4& q, float dx, float radius) 
 }
 
 // alpha at the pixel (column term xt, row offset dy), or 0 when the pixel skips the
-// splat: 2^q by the fast exp2; within [qlo, qhi) around the alpha_min threshold the
-// reference expression decides.  Otherwise branch-free.  EXACT (a splat property; the
-// kernels instantiate the group loop for each) takes q from the reference's power,
-// rounded as the reference rounds it, instead of the expanded quadratic, for elongated
-// conics whose expanded terms are far larger than q.
-template <bool EXACT>
+// splat: 2^q by the fast exp2; within [qlo, qhi) around the alpha_min threshold (the
+// splat's band) the reference expression decides.  Otherwise branch-free.
 __device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, const XTerm& xt,
                                           float dy, float amax, float amin, float qlo, float qhi) {
-    float e;
-    if (EXACT) {
-        const float power = __fsub_rn(__fmul_rn(-0.5f, __fadd_rn(__fmul_rn(__fmul_rn(g0.z, xt.dx), xt.dx),
-                                                                 __fmul_rn(__fmul_rn(g1.x, dy), dy))),
-                                      __fmul_rn(__fmul_rn(g0.w, xt.dx), dy));
-        e = power > 0.f ? -1e30f : __fmaf_rn(power, LOG2E, q.w);  // the reference skips power > 0
-    } else {
-        e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, xt.b0), xt.a0);
-    }
+    const float e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, xt.b0), xt.a0);
     const bool inb = xt.inb && fabsf(dy) <= g1.z;
     float alpha = (inb && e >= qhi) ? fminf(amax, ex2_approx(e)) : 0.f;
     if (inb && e >= qlo && e < qhi) alpha = alpha_band(g0, g1, xt.dx, dy, amax, amin);
@@ -380,33 +367,26 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) r
                     const float4 g1 = g1s[j];
                     const float4 q = qs[j];
                     const float4 c = cs[j];
-                    const bool exact = c.w < 0.f;  // warp-uniform
-                    const float qlo = qthr - fabsf(c.w), qhi = qthr + fabsf(c.w);
+                    const float qlo = c.w, qhi = 2.0f * qthr - c.w;  // the splat's band
                     const uint32_t pos = b0 + (uint32_t)j + 1u;
                     XTerm xt[L::WX];
 #pragma unroll
                     for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
-                    // The group loop, instantiated for both exponent forms (a uniform branch).
-                    auto groups = [&](auto ex) {
-                        constexpr bool EXACT = decltype(ex)::value;
 #pragma unroll
-                        for (int p = 0; p < PPT; p++) {
-                            if (!(m & (1u << p))) continue;
-                            // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
-                            float alpha = alpha_at<EXACT>(g0, g1, q, xt[p / L::WY], pyf[p] - g0.y, a.alpha_max,
-                                                          a.alpha_min, qlo, qhi);
-                            alpha = done[p] ? 0.f : alpha;
-                            const float wgt = alpha * T[p];
-                            cr[p] += c.x * wgt;
-                            cg[p] += c.y * wgt;
-                            cb[p] += c.z * wgt;
-                            T[p] *= 1.0f - alpha;
-                            last[p] = alpha != 0.f ? pos : last[p];
-                            done[p] = done[p] || T[p] <= a.t_min;
-                        }
-                    };
-                    if (exact) groups(std::true_type{});
-                    else groups(std::false_type{});
+                    for (int p = 0; p < PPT; p++) {
+                        if (!(m & (1u << p))) continue;
+                        // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
+                        float alpha = alpha_at(g0, g1, q, xt[p / L::WY], pyf[p] - g0.y, a.alpha_max, a.alpha_min,
+                                               qlo, qhi);
+                        alpha = done[p] ? 0.f : alpha;
+                        const float wgt = alpha * T[p];
+                        cr[p] += c.x * wgt;
+                        cg[p] += c.y * wgt;
+                        cb[p] += c.z * wgt;
+                        T[p] *= 1.0f - alpha;
+                        last[p] = alpha != 0.f ? pos : last[p];
+                        done[p] = done[p] || T[p] <= a.t_min;
+                    }
                 }
 #pragma unroll
                 for (int p = 0; p < PPT; p++)
@@ -569,8 +549,7 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                         const float4 g1 = g1s[j];
                         const float4 q = qs[j];
                         const float4 c = cs[j];
-                        const bool exact = c.w < 0.f;  // warp-uniform
-                    const float qlo = qthr - fabsf(c.w), qhi = qthr + fabsf(c.w);
+                        const float qlo = c.w, qhi = 2.0f * qthr - c.w;  // the splat's band
                         XTerm xt[L::WX];
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
@@ -580,9 +559,6 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                         // (opacity logit, u, v, A, B, C) after the reduction.
                         float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
                         float v8 = 0.f;
-                        // The group loop, instantiated for both exponent forms (a uniform branch).
-                        auto groups = [&](auto ex) {
-                            constexpr bool EXACT = decltype(ex)::value;
 #pragma unroll
                         for (int p = 0; p < PPT; p++) {
                             if (!(m & (1u << p))) continue;
@@ -590,7 +566,7 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                             // (T / 1) and dL.behind as they are.
                             const XTerm& x = xt[p / L::WY];
                             const float dx = x.dx, dy = pyf[p] - g0.y;
-                            float alpha = alpha_at<EXACT>(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi);
+                            float alpha = alpha_at(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi);
                             alpha = k < mylast[p] ? alpha : 0.f;
                             const float ioma = rcp_approx(1.0f - alpha);
                             const float Tk = T[p] * ioma;
@@ -614,9 +590,6 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                             v[7] += dPx * dy;
                             v8 += dPy * dy;
                         }
-                        };
-                        if (exact) groups(std::true_type{});
-                        else groups(std::false_type{});
                         float s = warp_sum8_transposed(v);
                         float s8 = v8;
 #pragma unroll
