@@ -636,7 +636,7 @@ def main():
                     help="use the data-parallel step (gradients, NCCL all-reduce, update) even on one GPU")
     ap.add_argument("--autotune-cache", default=None,
                     help="file caching the raster variant choice (a profiled run then uses the unprofiled choice)")
-    ap.add_argument("--profile-ppt", type=int, default=4, choices=(1, 2, 4, 8),
+    ap.add_argument("--profile-ppt", type=int, default=4, choices=(2, 4, 8),
                     help="pixels per raster thread in --profile-case")
     ap.add_argument("--profile-case", action="store_true",
                     help="run the small ncu capture case instead of the benchmark")

@@ -16,8 +16,20 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/gsb200.h"
 #include "internal.h"
+
+// NVTX range over a C-ABI call, named after it: host-side structure for a timeline
+// profiler (NVTX v3 is header-only; with no tool attached a range costs a pointer test).
+struct NvtxScope {
+    explicit NvtxScope(const char* name) { nvtxRangePushA(name); }
+    ~NvtxScope() { nvtxRangePop(); }
+    NvtxScope(const NvtxScope&) = delete;
+    NvtxScope& operator=(const NvtxScope&) = delete;
+};
+#define GS_TRACE(name) NvtxScope gs_nvtx_scope_(name)
 
 using namespace gs;
 
@@ -890,7 +902,7 @@ void gs_config_default(GsConfig* cfg) {
     cfg->device = 0;
     cfg->autotune = 0;
     cfg->raster_batch = 256;
-    cfg->raster_ppt = 1;
+    cfg->raster_ppt = 0;
     cfg->tile_cull = 1;
     cfg->tile_size = GS_TILE;
     cfg->lpt_order = 1;
@@ -935,6 +947,7 @@ const char* gs_stage_name(int32_t stage) {
 }
 
 int gs_create(const GsConfig* cfg_in, GsContext** out) {
+    GS_TRACE("gs_create");
     if (!out) return fail(GS_ERR_INVALID_ARG, "out is null");
     *out = nullptr;
     GsConfig cfg;
@@ -944,12 +957,12 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if (cfg.rect_mode < 0 || cfg.rect_mode > 1) return fail(GS_ERR_INVALID_ARG, "rect_mode must be 0 or 1");
     if (cfg.raster_batch != 64 && cfg.raster_batch != 128 && cfg.raster_batch != 256)
         return fail(GS_ERR_INVALID_ARG, "raster_batch must be 64, 128 or 256");
-    if (cfg.raster_ppt == 0) cfg.raster_ppt = 1;
     if (cfg.tile_size == 0) cfg.tile_size = GS_TILE;
+    if (cfg.raster_ppt == 0) cfg.raster_ppt = cfg.tile_size == 8 ? 2 : 4;
     if (cfg.tile_size != 8 && cfg.tile_size != 16 && cfg.tile_size != 32)
         return fail(GS_ERR_INVALID_ARG, "tile_size must be 8, 16 or 32");
     if (!raster_variant_ok(cfg.tile_size, cfg.raster_ppt))
-        return fail(GS_ERR_INVALID_ARG, "raster_ppt %d does not exist for %d-pixel tiles (8: 1, 2; 16: 1, 2, 4, 8; 32: 2, 4, 8)",
+        return fail(GS_ERR_INVALID_ARG, "raster_ppt %d does not exist for %d-pixel tiles (8: 2; 16 and 32: 2, 4, 8)",
                     cfg.raster_ppt, cfg.tile_size);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
@@ -1001,6 +1014,7 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
 }
 
 int gs_destroy(GsContext* c) {
+    GS_TRACE("gs_destroy");
     if (!c) return GS_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
@@ -1074,6 +1088,7 @@ static int upload_planes(GsContext* c, int n, const std::vector<float>& planes_h
 }
 
 int gs_set_gaussians(GsContext* c, int32_t n, const float* params) {
+    GS_TRACE("gs_set_gaussians");
     CTX_CHECK(c);
     if (n < 0 || n > (1 << 28) || (n > 0 && !params)) return fail(GS_ERR_INVALID_ARG, "bad Gaussian count or pointer");
     const int P = c->planes;
@@ -1087,6 +1102,7 @@ int gs_set_gaussians(GsContext* c, int32_t n, const float* params) {
 }
 
 int gs_set_gaussians_packed(GsContext* c, int32_t n, const float* packed) {
+    GS_TRACE("gs_set_gaussians_packed");
     CTX_CHECK(c);
     if (n < 0 || n > (1 << 28) || (n > 0 && !packed)) return fail(GS_ERR_INVALID_ARG, "bad Gaussian count or pointer");
     const int P = c->planes;
@@ -1138,6 +1154,7 @@ int32_t gs_num_gaussians(const GsContext* c) { return c ? c->n : 0; }
 
 // ---- views ------------------------------------------------------------------------
 int gs_set_views(GsContext* c, int32_t num_views, const GsCamera* cams) {
+    GS_TRACE("gs_set_views");
     CTX_CHECK(c);
     if (num_views < 0 || num_views > GS_MAX_VIEWS || (num_views > 0 && !cams))
         return fail(GS_ERR_INVALID_ARG, "num_views must be 0..%d", GS_MAX_VIEWS);
@@ -1215,6 +1232,7 @@ static int run_forward(GsContext* c, int first, int count) {
 }
 
 int gs_forward(GsContext* c, int32_t first, int32_t count, float* images_out) {
+    GS_TRACE("gs_forward");
     CTX_CHECK(c);
     CKI(check_range(c, first, count, false));
     CKI(run_forward(c, first, count));
@@ -1246,6 +1264,7 @@ static int check_loss(const GsLossConfig* lc) {
 }
 
 int gs_loss(GsContext* c, const GsLossConfig* lc, float* loss_out) {
+    GS_TRACE("gs_loss");
     CTX_CHECK(c);
     CKI(check_loss(lc));
     if (c->last_first < 0) return fail(GS_ERR_STATE, "gs_loss needs a forward first");
@@ -1269,6 +1288,7 @@ int gs_loss(GsContext* c, const GsLossConfig* lc, float* loss_out) {
 }
 
 int gs_backward(GsContext* c, const float* dl_dimages) {
+    GS_TRACE("gs_backward");
     CTX_CHECK(c);
     if (c->last_first < 0) return fail(GS_ERR_STATE, "gs_backward needs a forward first");
     const int first = c->last_first, count = c->last_count;
@@ -1394,6 +1414,7 @@ int gs_get_tile_lists(GsContext* c, int32_t view, uint32_t* list_out, uint32_t* 
 
 // ---- one-camera helpers (render, gradients, loss gradient) ------------------------------
 int gs_render(GsContext* c, const GsCamera* cam, float* rgb_out, float* state_out) {
+    GS_TRACE("gs_render");
     CTX_CHECK(c);
     if (!cam || !rgb_out) return fail(GS_ERR_INVALID_ARG, "null argument");
     if (c->n <= 0) return fail(GS_ERR_STATE, "no Gaussians set");
@@ -1427,6 +1448,7 @@ int gs_render(GsContext* c, const GsCamera* cam, float* rgb_out, float* state_ou
 
 int gs_gradients(GsContext* c, const GsCamera* cam, const float* target, float ssim_lambda, float* image_out,
                  float* grads16_out, float* shape10_out) {
+    GS_TRACE("gs_gradients");
     CTX_CHECK(c);
     if (!cam || !target) return fail(GS_ERR_INVALID_ARG, "null argument");
     if (c->n <= 0) return fail(GS_ERR_STATE, "no Gaussians set");
@@ -1458,6 +1480,7 @@ int gs_gradients(GsContext* c, const GsCamera* cam, const float* target, float s
 
 int gs_loss_gradient(GsContext* c, const float* image, const float* target, int32_t width, int32_t height,
                      float ssim_lambda, int32_t window, float* grad_out, float* loss_out) {
+    GS_TRACE("gs_loss_gradient");
     CTX_CHECK(c);
     if (!image || !target || !grad_out) return fail(GS_ERR_INVALID_ARG, "null argument");
     GsLossConfig lc{ssim_lambda, window};
@@ -1587,17 +1610,20 @@ static int train_step_impl(GsContext* c, const GsAdamConfig* ad, const GsLossCon
 
 int gs_train_step(GsContext* c, const GsAdamConfig* adam, const GsLossConfig* loss, int32_t first, int32_t count,
                   float* loss_out) {
+    GS_TRACE("gs_train_step");
     return train_step_impl(c, adam, loss, first, count, nullptr, loss_out);
 }
 
 int gs_train_step_host(GsContext* c, const GsAdamConfig* adam, const GsLossConfig* loss, int32_t first, int32_t count,
                        const uint8_t* targets_u8, float* loss_out) {
+    GS_TRACE("gs_train_step_host");
     if (!targets_u8) return fail(GS_ERR_INVALID_ARG, "targets_u8 is null");
     return train_step_impl(c, adam, loss, first, count, targets_u8, loss_out);
 }
 
 int gs_step_gradients(GsContext* c, const GsLossConfig* lc, int32_t first, int32_t count, float** grads_device,
                       int64_t* num_floats) {
+    GS_TRACE("gs_step_gradients");
     CTX_CHECK(c);
     CKI(check_loss(lc));
     CKI(check_range(c, first, count, false));
@@ -1638,6 +1664,7 @@ int gs_step_gradients(GsContext* c, const GsLossConfig* lc, int32_t first, int32
 }
 
 int gs_step_apply(GsContext* c, const GsAdamConfig* ad, float* loss_out, int32_t* skipped_out) {
+    GS_TRACE("gs_step_apply");
     CTX_CHECK(c);
     CKI(check_adam(ad));
     if (!c->grads_pending) return fail(GS_ERR_STATE, "gs_step_apply without gs_step_gradients");
@@ -1674,6 +1701,7 @@ int gs_get_stream(GsContext* c, void** stream_out) {
 
 int gs_train_step_host_async(GsContext* c, const GsAdamConfig* ad, const GsLossConfig* lc, int32_t first,
                              int32_t count, const uint8_t* targets_u8, float* loss_out) {
+    GS_TRACE("gs_train_step_host_async");
     CTX_CHECK(c);
     CKI(check_adam(ad));
     CKI(check_loss(lc));
@@ -1733,6 +1761,7 @@ int gs_train_step_host_async(GsContext* c, const GsAdamConfig* ad, const GsLossC
 }
 
 int gs_train(GsContext* c, int32_t steps, const GsAdamConfig* adam, float* losses_out) {
+    GS_TRACE("gs_train");
     CTX_CHECK(c);
     if (steps < 0) return fail(GS_ERR_INVALID_ARG, "steps < 0");
     if (c->V < 1) return fail(GS_ERR_STATE, "no views");
@@ -1935,6 +1964,7 @@ static int neighbour_sizes_device(GsContext* c, const float* xyz, int count, dou
 
 int gs_neighbour_sizes(GsContext* c, const float* xyz, int32_t count, double min_size, double max_size,
                        double fallback, float* sizes_out) {
+    GS_TRACE("gs_neighbour_sizes");
     CTX_CHECK(c);
     if (count < 0 || count > (1 << 28) || (count > 0 && (!xyz || !sizes_out)))
         return fail(GS_ERR_INVALID_ARG, "bad point count or pointer");
@@ -1947,6 +1977,7 @@ int gs_neighbour_sizes(GsContext* c, const float* xyz, int32_t count, double min
 }
 
 int gs_init_from_points(GsContext* c, const float* xyz, const float* rgb, int32_t count, float size) {
+    GS_TRACE("gs_init_from_points");
     CTX_CHECK(c);
     if (count < 0 || count > (1 << 28) || (count > 0 && (!xyz || !rgb)))
         return fail(GS_ERR_INVALID_ARG, "bad point count or pointer");
@@ -1978,6 +2009,7 @@ int gs_init_from_points(GsContext* c, const float* xyz, const float* rgb, int32_
 // ---- photo selection -------------------------------------------------------------------
 int gs_sharpness(GsContext* c, const uint8_t* images, int32_t count, int32_t width, int32_t height,
                  int32_t channels, double* scores) {
+    GS_TRACE("gs_sharpness");
     CTX_CHECK(c);
     if (count < 0 || width < 1 || height < 1 || (channels != 1 && channels != 3) || (count > 0 && (!images || !scores)))
         return fail(GS_ERR_INVALID_ARG, "bad images");
@@ -2045,6 +2077,7 @@ int gs_choose_sharp(const double* scores, int32_t count, int32_t max_views, int3
 
 // ---- scene I/O ------------------------------------------------------------------------
 int gs_load_ply(GsContext* c, const void* data, int64_t bytes, int32_t* count_out) {
+    GS_TRACE("gs_load_ply");
     CTX_CHECK(c);
     if (!data || bytes <= 0) return fail(GS_ERR_INVALID_ARG, "no data");
     PlyHeaderInfo h;
@@ -2068,6 +2101,7 @@ int gs_load_ply(GsContext* c, const void* data, int64_t bytes, int32_t* count_ou
 }
 
 int gs_save_ply(GsContext* c, int32_t with_sh, void* out, int64_t capacity, int64_t* bytes_out) {
+    GS_TRACE("gs_save_ply");
     CTX_CHECK(c);
     if (!bytes_out) return fail(GS_ERR_INVALID_ARG, "bytes_out is null");
     const int nk_out = with_sh ? (c->planes - 14) / 3 : 0;
@@ -2093,6 +2127,7 @@ int gs_save_ply(GsContext* c, int32_t with_sh, void* out, int64_t capacity, int6
 }
 
 int gs_save_splat(GsContext* c, void* out, int64_t capacity, int64_t* bytes_out) {
+    GS_TRACE("gs_save_splat");
     CTX_CHECK(c);
     if (!bytes_out) return fail(GS_ERR_INVALID_ARG, "bytes_out is null");
     const int n = c->n;
@@ -2161,6 +2196,7 @@ void gs_densify_config_default(GsDensifyConfig* d) {
 }
 
 int gs_densify(GsContext* c, const GsDensifyConfig* d, int32_t* new_count) {
+    GS_TRACE("gs_densify");
     CTX_CHECK(c);
     if (!d) return fail(GS_ERR_INVALID_ARG, "config is null");
     if (std::isnan(d->grad_threshold) || std::isnan(d->size_threshold) || std::isnan(d->min_opacity) ||
@@ -2269,6 +2305,7 @@ static int set_tile(GsContext* c, int tile) {
 // size with the fastest is kept.  The choice is cached per device and workload in
 // `cache_path` (lines "key|tile fwd_batch fwd_ppt bwd_batch bwd_ppt").
 int gs_autotune(GsContext* c, const char* cache_path) {
+    GS_TRACE("gs_autotune");
     CTX_CHECK(c);
     if (c->V < 1 || c->n <= 0) return fail(GS_ERR_STATE, "autotune needs Gaussians and views");
     int kind;

@@ -18,7 +18,10 @@
 // a window of inputs.  Windows are the reference's: centres whose whole window lies
 // inside the image (7x7 box, R = 3), or the 11-tap Gaussian (sigma 1.5, R = 5) with the
 // same rule.  The kernel also sums |x - y| and the SSIM of the windows centred in its
-// block for the loss value.
+// block for the loss value.  The filters carry their values in pairs (x and y, the two
+// moments of squares and products, coefficients a and b) through the packed FP32
+// instructions of sm_100 (FFMA2), which round each half as the scalar FFMA does: the
+// same sums with half the instructions.
 #include "internal.h"
 
 namespace gs {
@@ -29,7 +32,10 @@ constexpr int LB_THREADS = 256;
 
 struct LossWeights {
     float w[11];
+    float2 w2[11];  // each tap twice, a packed-FMA operand
 };
+
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
 template <int R>
 struct LossDims {
@@ -50,12 +56,14 @@ struct LossDims {
     static constexpr int NS3 = (LB_W + S3 - 1) / S3;
     static constexpr int S4 = 4;
     static constexpr int NS4 = LB_H / S4;
-    // Region A: image and target with halo, later the coefficients (X, Y are dead once
-    // the horizontal moments exist; the gradient pass reads its own pixels from HBM).
+    // Region A: image and target with halo as (x, y) pairs, later the coefficients as
+    // (a, b) pairs and d (the pixels are dead once the horizontal moments exist; the
+    // gradient pass reads its own pixels from HBM).
     static constexpr int XY = 2 * RH * RW;
     static constexpr int CF = 3 * CH * CFP;
-    static constexpr int A = XY > CF ? XY : CF;
-    // Region B: horizontal moments, later the horizontally filtered coefficients.
+    static constexpr int A = ((XY > CF ? XY : CF) + 1) & ~1;  // even: region B holds float2
+    // Region B: horizontal moments as (x, y) and (x^2 + y^2, xy) pairs, later the
+    // horizontally filtered coefficients as (a, b) pairs and d.
     static constexpr int HM = 4 * RH * HMP;
     static constexpr int HC = 3 * CH * LB_W;
     static constexpr int B = HM > HC ? HM : HC;
@@ -90,7 +98,7 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
                                                           LossWeights wts) {
     using D = LossDims<R>;
     constexpr int K = D::K;
-    extern __shared__ float sm[];
+    extern __shared__ __align__(16) float sm[];
     __shared__ float s_red[2][LB_THREADS / 32];
     __shared__ float s_lut[256];
     if (sizeof(TT) == 1) s_lut[threadIdx.x] = (float)threadIdx.x / 255.0f;
@@ -112,11 +120,13 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
     const bool use_ssim = a.lambda > 0.0f && windows > 0.0f;
     // Filter taps stay in the kernel-parameter constant bank (FFMA operands).
     const float* w = wts.w;
-    float* X = sm;
-    float* Y = sm + D::RH * D::RW;
-    float* CF = sm;
-    float* HM = sm + D::A;
-    float* HC = sm + D::A;
+    float2* XY = reinterpret_cast<float2*>(sm);                       // [RH][RW] (x, y)
+    float2* CFAB = reinterpret_cast<float2*>(sm);                     // [CH][CFP] (a, b)
+    float* CFD = sm + 2 * D::CH * D::CFP;                             // [CH][CFP] d
+    float2* HMA = reinterpret_cast<float2*>(sm + D::A);               // [RH][HMP] (x, y)
+    float2* HMB = HMA + D::RH * D::HMP;                               // [RH][HMP] (x^2 + y^2, xy)
+    float2* HCAB = reinterpret_cast<float2*>(sm + D::A);              // [CH][LB_W] (a, b)
+    float* HCD = sm + D::A + 2 * D::CH * LB_W;                        // [CH][LB_W] d
     float l1 = 0.f, ssim_sum = 0.f;
     const float C1 = 1e-4f, C2 = 9e-4f;
     const int tid = threadIdx.x;
@@ -141,69 +151,58 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
 #pragma unroll
         for (int i = 0; i < NL; i++) {
             const int idx = tid + i * LB_THREADS;
-            if (idx < D::RH * D::RW) {
-                X[idx] = xl[i];
-                Y[idx] = yl[i];
-            }
+            if (idx < D::RH * D::RW) XY[idx] = make_float2(xl[i], yl[i]);
         }
         __syncthreads();
         // P1: horizontal moments (x, y, x^2 + y^2, xy) at the centre columns of a strip.
         if (tid < D::RH * D::NS1) {
             const int r = tid / D::NS1, c0 = (tid % D::NS1) * D::S1;
-            float acc[D::S1][4];
+            float2 acc[D::S1][2];  // (x, y), (x^2 + y^2, xy)
 #pragma unroll
-            for (int k = 0; k < D::S1; k++)
-#pragma unroll
-                for (int m = 0; m < 4; m++) acc[k][m] = 0.f;
+            for (int k = 0; k < D::S1; k++) acc[k][0] = acc[k][1] = make_float2(0.f, 0.f);
 #pragma unroll
             for (int j = 0; j < D::S1 + 2 * R; j++) {
                 const int col = c0 + j;
-                const float xv = col < D::RW ? X[r * D::RW + col] : 0.f;
-                const float yv = col < D::RW ? Y[r * D::RW + col] : 0.f;
-                const float ss = fmaf(xv, xv, yv * yv), xy = xv * yv;
+                const float2 v = col < D::RW ? XY[r * D::RW + col] : make_float2(0.f, 0.f);
+                const float2 sq = make_float2(fmaf(v.x, v.x, v.y * v.y), v.x * v.y);
 #pragma unroll
                 for (int k = 0; k < D::S1; k++) {
                     if (j - k < 0 || j - k >= K) continue;
-                    const float wt = w[j - k];
-                    acc[k][0] = fmaf(wt, xv, acc[k][0]);
-                    acc[k][1] = fmaf(wt, yv, acc[k][1]);
-                    acc[k][2] = fmaf(wt, ss, acc[k][2]);
-                    acc[k][3] = fmaf(wt, xy, acc[k][3]);
+                    const float2 wt = wts.w2[j - k];
+                    acc[k][0] = fma2(wt, v, acc[k][0]);
+                    acc[k][1] = fma2(wt, sq, acc[k][1]);
                 }
             }
 #pragma unroll
             for (int k = 0; k < D::S1; k++) {
                 if (c0 + k >= D::HW) break;
-#pragma unroll
-                for (int m = 0; m < 4; m++) HM[m * D::RH * D::HMP + r * D::HMP + c0 + k] = acc[k][m];
+                HMA[r * D::HMP + c0 + k] = acc[k][0];
+                HMB[r * D::HMP + c0 + k] = acc[k][1];
             }
         }
         __syncthreads();
         // P2: vertical moments at a strip of window centres -> SSIM coefficients.
         const bool p2 = tid < D::HW * D::NS2;
         const int hc = tid % D::HW, h0 = (tid / D::HW) * D::S2;
-        float acc2[D::S2][4];
+        float2 acc2[D::S2][2];
 #pragma unroll
-        for (int k = 0; k < D::S2; k++)
-#pragma unroll
-            for (int m = 0; m < 4; m++) acc2[k][m] = 0.f;
+        for (int k = 0; k < D::S2; k++) acc2[k][0] = acc2[k][1] = make_float2(0.f, 0.f);
         if (p2) {
 #pragma unroll
             for (int j = 0; j < D::S2 + 2 * R; j++) {
                 const int row = h0 + j;
-                float v[4];
-#pragma unroll
-                for (int m = 0; m < 4; m++) v[m] = row < D::RH ? HM[m * D::RH * D::HMP + row * D::HMP + hc] : 0.f;
+                const float2 va = row < D::RH ? HMA[row * D::HMP + hc] : make_float2(0.f, 0.f);
+                const float2 vb = row < D::RH ? HMB[row * D::HMP + hc] : make_float2(0.f, 0.f);
 #pragma unroll
                 for (int k = 0; k < D::S2; k++) {
                     if (j - k < 0 || j - k >= K) continue;
-                    const float wt = w[j - k];
-#pragma unroll
-                    for (int m = 0; m < 4; m++) acc2[k][m] = fmaf(wt, v[m], acc2[k][m]);
+                    const float2 wt = wts.w2[j - k];
+                    acc2[k][0] = fma2(wt, va, acc2[k][0]);
+                    acc2[k][1] = fma2(wt, vb, acc2[k][1]);
                 }
             }
         }
-        // CF aliases X and Y, which only P1 read.
+        // The coefficients alias the pixels, which only P1 read.
         if (p2) {
             const int gx = bx0 - R + hc;
             const bool col_ok = gx >= R && gx < W - R;
@@ -215,7 +214,7 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
                 const int gy = by0 - R + hr;
                 float ca = 0.f, cb = 0.f, cd = 0.f;
                 if (col_ok && gy >= R && gy < H - R) {
-                    const float mx = acc2[k][0], my = acc2[k][1], s2 = acc2[k][2], sxy = acc2[k][3];
+                    const float mx = acc2[k][0].x, my = acc2[k][0].y, s2 = acc2[k][1].x, sxy = acc2[k][1].y;
                     const float a1 = 2.0f * mx * my + C1;
                     const float a2 = 2.0f * (sxy - mx * my) + C2;
                     const float b1 = mx * mx + my * my + C1;
@@ -232,39 +231,38 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
                     if (col_in && gy >= by0 && gy < by0 + LB_H) ssim_sum += ssim;
                 }
                 const int o = hr * D::CFP + hc;
-                CF[0 * D::CH * D::CFP + o] = ca;
-                CF[1 * D::CH * D::CFP + o] = cb;
-                CF[2 * D::CH * D::CFP + o] = cd;
+                CFAB[o] = make_float2(ca, cb);
+                CFD[o] = cd;
             }
         }
         __syncthreads();
         // P3: filter the coefficients back, horizontal ...
         if (tid < D::CH * D::NS3) {
             const int hr = tid / D::NS3, o0 = (tid % D::NS3) * D::S3;
-            float acc[D::S3][3];
+            float2 acc[D::S3];
+            float accd[D::S3];
 #pragma unroll
-            for (int k = 0; k < D::S3; k++)
-#pragma unroll
-                for (int q = 0; q < 3; q++) acc[k][q] = 0.f;
+            for (int k = 0; k < D::S3; k++) {
+                acc[k] = make_float2(0.f, 0.f);
+                accd[k] = 0.f;
+            }
 #pragma unroll
             for (int j = 0; j < D::S3 + 2 * R; j++) {
                 const int col = o0 + j;
-                float v[3];
-#pragma unroll
-                for (int q = 0; q < 3; q++) v[q] = col < D::HW ? CF[q * D::CH * D::CFP + hr * D::CFP + col] : 0.f;
+                const float2 vab = col < D::HW ? CFAB[hr * D::CFP + col] : make_float2(0.f, 0.f);
+                const float vd = col < D::HW ? CFD[hr * D::CFP + col] : 0.f;
 #pragma unroll
                 for (int k = 0; k < D::S3; k++) {
                     if (j - k < 0 || j - k >= K) continue;
-                    const float wt = w[j - k];
-#pragma unroll
-                    for (int q = 0; q < 3; q++) acc[k][q] = fmaf(wt, v[q], acc[k][q]);
+                    acc[k] = fma2(wts.w2[j - k], vab, acc[k]);
+                    accd[k] = fmaf(w[j - k], vd, accd[k]);
                 }
             }
 #pragma unroll
             for (int k = 0; k < D::S3; k++) {
                 if (o0 + k >= LB_W) break;
-#pragma unroll
-                for (int q = 0; q < 3; q++) HC[q * D::CH * LB_W + hr * LB_W + o0 + k] = acc[k][q];
+                HCAB[hr * LB_W + o0 + k] = acc[k];
+                HCD[hr * LB_W + o0 + k] = accd[k];
             }
         }
         __syncthreads();
@@ -273,23 +271,23 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
     if (tid < LB_W * D::NS4) {
         const int ox = tid % LB_W, oy0 = (tid / LB_W) * D::S4;
         const int gx = bx0 + ox;
-        float acc[D::S4][3];
+        float2 acc[D::S4];
+        float accd[D::S4];
 #pragma unroll
-        for (int k = 0; k < D::S4; k++)
-#pragma unroll
-            for (int q = 0; q < 3; q++) acc[k][q] = 0.f;
+        for (int k = 0; k < D::S4; k++) {
+            acc[k] = make_float2(0.f, 0.f);
+            accd[k] = 0.f;
+        }
         if (use_ssim) {
 #pragma unroll
             for (int j = 0; j < D::S4 + 2 * R; j++) {
-                float v[3];
-#pragma unroll
-                for (int q = 0; q < 3; q++) v[q] = HC[q * D::CH * LB_W + (oy0 + j) * LB_W + ox];
+                const float2 vab = HCAB[(oy0 + j) * LB_W + ox];
+                const float vd = HCD[(oy0 + j) * LB_W + ox];
 #pragma unroll
                 for (int k = 0; k < D::S4; k++) {
                     if (j - k < 0 || j - k >= K) continue;
-                    const float wt = w[j - k];
-#pragma unroll
-                    for (int q = 0; q < 3; q++) acc[k][q] = fmaf(wt, v[q], acc[k][q]);
+                    acc[k] = fma2(wts.w2[j - k], vab, acc[k]);
+                    accd[k] = fmaf(w[j - k], vd, accd[k]);
                 }
             }
         }
@@ -303,7 +301,7 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
             const float diff = xv - yv;
             float g = l1_scale * (float)((diff > 0.f) - (diff < 0.f));
             l1 += fabsf(diff);
-            if (use_ssim) g -= ssim_scale * (acc[k][0] + 2.0f * xv * acc[k][1] + yv * acc[k][2]);
+            if (use_ssim) g -= ssim_scale * (acc[k].x + 2.0f * xv * acc[k].y + yv * accd[k]);
             a.dl[q] = g;
         }
     }
@@ -343,6 +341,7 @@ static LossWeights make_weights(int window) {
         }
         for (int k = 0; k < 11; k++) w.w[k] = (float)(g[k] / s);
     }
+    for (int k = 0; k < 11; k++) w.w2[k] = make_float2(w.w[k], w.w[k]);
     return w;
 }
 

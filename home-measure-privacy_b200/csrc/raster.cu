@@ -68,6 +68,15 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return r;
 }
 
+// Two pixels of a thread that share an x band travel together as one float2 through
+// the packed FP32 instructions of sm_100 (FFMA2 / FADD2 / FMUL2): each half is rounded
+// as the scalar instruction would round it, so the blend is bit-identical to the scalar
+// arithmetic while issuing half the instructions.
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
 // Layout of a CTA over one TILE x TILE tile with PPT pixels per thread: the tile is
 // GX x GY groups of 8 x 4 pixels; each warp owns a block of WX x WY groups (WX = 2 when
 // a thread has 8 pixels, else 1) and its p-th group is column p / WY, row p % WY of that
@@ -266,31 +275,43 @@ __device__ __forceinline__ float alpha_band(const float4& g0, const float4& g1, 
 }
 
 // The pieces of the alpha exponent that depend on one splat and one pixel column:
-// log2(alpha) = a0 + dy (b0 + qc dy) with a0 = log2(op) + qa dx^2, b0 = qb dx; and
-// whether |dx| <= radius.
+// log2(alpha) = a0 + dy (b0 + qc dy) with a0 = log2(op) + qa dx^2, b0 = qb dx (both
+// duplicated for a pixel pair); and whether |dx| <= radius.
 struct XTerm {
-    float dx, a0, b0;
+    float dx;
+    float2 a0, b0;
     bool inb;
 };
 
 __device__ __forceinline__ XTerm xterm(const float4& q, float dx, float radius) {
     XTerm t;
     t.dx = dx;
-    t.a0 = __fmaf_rn(dx, __fmul_rn(q.x, dx), q.w);
-    t.b0 = __fmul_rn(q.y, dx);
+    t.a0 = f2(__fmaf_rn(dx, __fmul_rn(q.x, dx), q.w));
+    t.b0 = f2(__fmul_rn(q.y, dx));
     t.inb = fabsf(dx) <= radius;
     return t;
 }
 
-// alpha at the pixel (column term xt, row offset dy), or 0 when the pixel skips the
-// splat: 2^q by the fast exp2; within [qlo, qhi) around the alpha_min threshold (the
-// splat's band) the reference expression decides.  Otherwise branch-free.
-__device__ __forceinline__ float alpha_at(const float4& g0, const float4& g1, const float4& q, const XTerm& xt,
-                                          float dy, float amax, float amin, float qlo, float qhi) {
-    const float e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, xt.b0), xt.a0);
-    const bool inb = xt.inb && fabsf(dy) <= g1.z;
-    float alpha = (inb && e >= qhi) ? fminf(amax, ex2_approx(e)) : 0.f;
-    if (inb && e >= qlo && e < qhi) alpha = alpha_band(g0, g1, xt.dx, dy, amax, amin);
+// The exponents of a pixel pair of one column (row offsets dy).
+__device__ __forceinline__ float2 exponent2(const XTerm& xt, float2 qc, float2 dy) {
+    return fma2(dy, fma2(qc, dy, xt.b0), xt.a0);
+}
+
+// alpha at one pixel from its exponent e and row offset dy, or 0 when the pixel skips
+// the splat (live: the pixel still takes part and its column lies within the bounding
+// square): 2^e by the fast exp2; within [qlo, qhi) around the alpha_min threshold (the
+// splat's band) the reference expression decides.  hit = alpha != 0.  Branch-free but
+// for the band.
+__device__ __forceinline__ float alpha_pix(float e, float dx, float dy, bool live, const float4& g0,
+                                           const float4& g1, float amax, float amin, float qlo, float qhi,
+                                           bool& hit) {
+    const bool inb = live && fabsf(dy) <= g1.z;
+    hit = inb && e >= qhi;
+    float alpha = hit ? fminf(amax, ex2_approx(e)) : 0.f;
+    if (inb && e >= qlo && e < qhi) {
+        alpha = alpha_band(g0, g1, dx, dy, amax, amin);
+        hit = alpha != 0.f;
+    }
     return alpha;
 }
 
@@ -321,20 +342,23 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) r
         const TileInfo<PPT> ti = tile_info<TILE, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x, end = rg.y;
-        float pxf[L::WX], pyf[PPT], T[PPT], cr[PPT], cg[PPT], cb[PPT];
+        // Pixel pairs (2i, 2i + 1) share an x band.  A pixel blends while T > t_min (the
+        // reference stops once T <= 1e-4); pixels outside the view start at T = 0.
+        constexpr int NP = PPT / 2;
+        float pxf[L::WX];
+        float2 pyf[NP], T[NP], cr[NP], cg[NP], cb[NP];
         uint32_t last[PPT];
-        bool done[PPT];
 #pragma unroll
         for (int b = 0; b < L::WX; b++) pxf[b] = (float)ti.x[b * L::WY] + 0.5f;  // the warp's x bands
         uint32_t gdone = 0u;  // warp-uniform: groups whose pixels have all stopped
 #pragma unroll
-        for (int p = 0; p < PPT; p++) {
-            pyf[p] = (float)ti.y[p] + 0.5f;
-            T[p] = 1.0f;
-            cr[p] = cg[p] = cb[p] = 0.f;
-            last[p] = start;
-            done[p] = !ti.inside[p];
-            if (__all_sync(FULL_MASK, done[p])) gdone |= 1u << p;
+        for (int i = 0; i < NP; i++) {
+            pyf[i] = make_float2((float)ti.y[2 * i] + 0.5f, (float)ti.y[2 * i + 1] + 0.5f);
+            T[i] = make_float2(ti.inside[2 * i] ? 1.0f : 0.f, ti.inside[2 * i + 1] ? 1.0f : 0.f);
+            cr[i] = cg[i] = cb[i] = f2(0.f);
+            last[2 * i] = last[2 * i + 1] = start;
+            if (__all_sync(FULL_MASK, !ti.inside[2 * i])) gdone |= 1u << (2 * i);
+            if (__all_sync(FULL_MASK, !ti.inside[2 * i + 1])) gdone |= 2u << (2 * i);
         }
         int buf = 0;
         if (start < end) stage_batch(a, start, min((uint32_t)BATCH, end - start), false, s_g0[0], s_g1[0], s_c[0], nullptr);
@@ -369,28 +393,39 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) r
                     const float4 c = cs[j];
                     const float qlo = c.w, qhi = 2.0f * qthr - c.w;  // the splat's band
                     const uint32_t pos = b0 + (uint32_t)j + 1u;
+                    const float2 qc = f2(q.z), ngy = f2(-g0.y);
+                    const float2 cx = f2(c.x), cy = f2(c.y), cz = f2(c.z);
                     XTerm xt[L::WX];
 #pragma unroll
                     for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
 #pragma unroll
-                    for (int p = 0; p < PPT; p++) {
-                        if (!(m & (1u << p))) continue;
-                        // Branch-free per lane: alpha = 0 leaves colour, T and last as they are.
-                        float alpha = alpha_at(g0, g1, q, xt[p / L::WY], pyf[p] - g0.y, a.alpha_max, a.alpha_min,
-                                               qlo, qhi);
-                        alpha = done[p] ? 0.f : alpha;
-                        const float wgt = alpha * T[p];
-                        cr[p] += c.x * wgt;
-                        cg[p] += c.y * wgt;
-                        cb[p] += c.z * wgt;
-                        T[p] *= 1.0f - alpha;
-                        last[p] = alpha != 0.f ? pos : last[p];
-                        done[p] = done[p] || T[p] <= a.t_min;
+                    for (int i = 0; i < NP; i++) {
+                        if (!((m >> (2 * i)) & 3u)) continue;
+                        // Branch-free per lane: alpha = 0 leaves colour, T and last as they are
+                        // (also for a pair member whose group the mask left out).
+                        const XTerm& x = xt[(2 * i) / L::WY];
+                        const float2 dy = add2(pyf[i], ngy);
+                        const float2 e = exponent2(x, qc, dy);
+                        bool h0, h1;
+                        const float a0 = alpha_pix(e.x, x.dx, dy.x, x.inb && T[i].x > a.t_min, g0, g1, a.alpha_max,
+                                                   a.alpha_min, qlo, qhi, h0);
+                        const float a1 = alpha_pix(e.y, x.dx, dy.y, x.inb && T[i].y > a.t_min, g0, g1, a.alpha_max,
+                                                   a.alpha_min, qlo, qhi, h1);
+                        const float2 alpha = make_float2(a0, a1);
+                        const float2 wgt = mul2(alpha, T[i]);
+                        cr[i] = fma2(cx, wgt, cr[i]);
+                        cg[i] = fma2(cy, wgt, cg[i]);
+                        cb[i] = fma2(cz, wgt, cb[i]);
+                        T[i] = mul2(T[i], fma2(alpha, f2(-1.0f), f2(1.0f)));  // T (1 - alpha)
+                        last[2 * i] = h0 ? pos : last[2 * i];
+                        last[2 * i + 1] = h1 ? pos : last[2 * i + 1];
                     }
                 }
 #pragma unroll
-                for (int p = 0; p < PPT; p++)
-                    if (__all_sync(FULL_MASK, done[p])) gdone |= 1u << p;
+                for (int i = 0; i < NP; i++) {
+                    if (__all_sync(FULL_MASK, !(T[i].x > a.t_min))) gdone |= 1u << (2 * i);
+                    if (__all_sync(FULL_MASK, !(T[i].y > a.t_min))) gdone |= 2u << (2 * i);
+                }
             }
             buf ^= 1;
             // All pixels done: the rest of the list cannot change the tile.
@@ -403,10 +438,11 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) r
         for (int p = 0; p < PPT; p++) {
             if (!ti.inside[p]) continue;
             const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x[p];
-            a.image[pix * 3 + 0] = cr[p];
-            a.image[pix * 3 + 1] = cg[p];
-            a.image[pix * 3 + 2] = cb[p];
-            a.t_final[pix] = T[p];
+            const int i = p / 2;
+            a.image[pix * 3 + 0] = p & 1 ? cr[i].y : cr[i].x;
+            a.image[pix * 3 + 1] = p & 1 ? cg[i].y : cg[i].x;
+            a.image[pix * 3 + 2] = p & 1 ? cb[i].y : cb[i].x;
+            a.t_final[pix] = p & 1 ? T[i].y : T[i].x;
             a.last[pix] = last[p];
         }
         if (!a.work_counter) break;
@@ -472,25 +508,34 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
         const TileInfo<PPT> ti = tile_info<TILE, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
-        float pxf[L::WX], pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
+        // Pixel pairs (2i, 2i + 1) share an x band (see f2).
+        constexpr int NP = PPT / 2;
+        float pxf[L::WX];
+        float2 pyf[NP], T[NP], dlr[NP], dlg[NP], dlb[NP], bd[NP];
         uint32_t mylast[PPT], gmax[PPT];
 #pragma unroll
         for (int b = 0; b < L::WX; b++) pxf[b] = (float)ti.x[b * L::WY] + 0.5f;  // the warp's x bands
         unsigned int wmax = start;
 #pragma unroll
+        for (int i = 0; i < NP; i++) {
+            pyf[i] = make_float2((float)ti.y[2 * i] + 0.5f, (float)ti.y[2 * i + 1] + 0.5f);
+            T[i] = dlr[i] = dlg[i] = dlb[i] = f2(0.f);
+            bd[i] = f2(0.f);  // dL . (colour of the splats behind), "behind"
+        }
+#pragma unroll
         for (int p = 0; p < PPT; p++) {
-            pyf[p] = (float)ti.y[p] + 0.5f;
-            T[p] = 0.f;
-            dlr[p] = dlg[p] = dlb[p] = 0.f;
-            bd[p] = 0.f;  // dL . (colour of the splats behind), "behind"
+            const int i = p / 2;
             mylast[p] = start;
             if (ti.inside[p]) {
                 const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x[p];
-                T[p] = a.t_final[pix];
                 mylast[p] = a.last[pix];
-                dlr[p] = a.dl[pix * 3 + 0];
-                dlg[p] = a.dl[pix * 3 + 1];
-                dlb[p] = a.dl[pix * 3 + 2];
+                const float t = a.t_final[pix], r = a.dl[pix * 3 + 0], g = a.dl[pix * 3 + 1],
+                            bl = a.dl[pix * 3 + 2];
+                if (p & 1) {
+                    T[i].y = t, dlr[i].y = r, dlg[i].y = g, dlb[i].y = bl;
+                } else {
+                    T[i].x = t, dlr[i].x = r, dlg[i].x = g, dlb[i].x = bl;
+                }
             }
             // Each group walks from the largest last of its pixels.
             unsigned int gm = mylast[p];
@@ -550,45 +595,73 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                         const float4 q = qs[j];
                         const float4 c = cs[j];
                         const float qlo = c.w, qhi = 2.0f * qthr - c.w;  // the splat's band
+                        const float2 qc = f2(q.z), ngy = f2(-g0.y);
+                        const float2 cx = f2(c.x), cy = f2(c.y), cz = f2(c.z);
                         XTerm xt[L::WX];
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
-                        // Per pixel: colour terms and the moments of dP = dL/dpower over the
-                        // offsets (sum dP, dP dx, dP dy, dP dx^2, dP dx dy, dP dy^2); the
-                        // splat's conic and opacity turn the warp sums into the gradients of
-                        // (opacity logit, u, v, A, B, C) after the reduction.
-                        float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                        float v8 = 0.f;
+                        // Per pixel: colour terms and dP = dL/dpower, summed per x band as
+                        // sum dP, sum dP dy, sum dP dy^2 (dx is the band's); after the group
+                        // loop the bands give the moments (sum dP, dP dx, dP dy, dP dx^2,
+                        // dP dx dy, dP dy^2) from which the splat's conic and opacity make
+                        // the gradients of (opacity logit, u, v, A, B, C) after the reduction.
+                        float2 gr = f2(0.f), gg = f2(0.f), gbl = f2(0.f);
+                        float2 s0[L::WX], sy[L::WX], syy[L::WX];
 #pragma unroll
-                        for (int p = 0; p < PPT; p++) {
-                            if (!(m & (1u << p))) continue;
+                        for (int b = 0; b < L::WX; b++) s0[b] = sy[b] = syy[b] = f2(0.f);
+#pragma unroll
+                        for (int i = 0; i < NP; i++) {
+                            if (!((m >> (2 * i)) & 3u)) continue;
                             // Branch-free per lane: alpha = 0 adds zeros and leaves T
                             // (T / 1) and dL.behind as they are.
-                            const XTerm& x = xt[p / L::WY];
-                            const float dx = x.dx, dy = pyf[p] - g0.y;
-                            float alpha = alpha_at(g0, g1, q, x, dy, a.alpha_max, a.alpha_min, qlo, qhi);
-                            alpha = k < mylast[p] ? alpha : 0.f;
-                            const float ioma = rcp_approx(1.0f - alpha);
-                            const float Tk = T[p] * ioma;
-                            const float at = alpha * Tk;
-                            v[0] += dlr[p] * at;
-                            v[1] += dlg[p] * at;
-                            v[2] += dlb[p] * at;
+                            const int b = (2 * i) / L::WY;
+                            const XTerm& x = xt[b];
+                            const float2 dy = add2(pyf[i], ngy);
+                            const float2 e = exponent2(x, qc, dy);
+                            bool h0, h1;
+                            const float a0 = alpha_pix(e.x, x.dx, dy.x, x.inb && k < mylast[2 * i], g0, g1,
+                                                       a.alpha_max, a.alpha_min, qlo, qhi, h0);
+                            const float a1 = alpha_pix(e.y, x.dx, dy.y, x.inb && k < mylast[2 * i + 1], g0, g1,
+                                                       a.alpha_max, a.alpha_min, qlo, qhi, h1);
+                            const float2 alpha = make_float2(a0, a1);
+                            // alpha clamped at alpha_max has no gradient through the power.
+                            const float2 ag = make_float2(a0 < a.alpha_max ? a0 : 0.f, a1 < a.alpha_max ? a1 : 0.f);
+                            const float2 oma = fma2(alpha, f2(-1.0f), f2(1.0f));  // 1 - alpha
+                            const float2 ioma = make_float2(rcp_approx(oma.x), rcp_approx(oma.y));
+                            const float2 Tk = mul2(T[i], ioma);
+                            const float2 at = mul2(alpha, Tk);
+                            gr = fma2(dlr[i], at, gr);
+                            gg = fma2(dlg[i], at, gg);
+                            gbl = fma2(dlb[i], at, gbl);
                             // dL/dalpha = dL.(c T_k - behind / (1 - alpha)); only dL.behind is
                             // kept per pixel.
-                            const float dlc = dlr[p] * c.x + dlg[p] * c.y + dlb[p] * c.z;
-                            const float dA = Tk * dlc - ioma * bd[p];
-                            bd[p] += dlc * at;
-                            T[p] = Tk;
-                            // alpha clamped at alpha_max has no gradient through the power.
-                            const float dP = alpha < a.alpha_max ? dA * alpha : 0.f;
-                            const float dPx = dP * dx, dPy = dP * dy;
-                            v[3] += dP;
-                            v[4] += dPx;
-                            v[5] += dPy;
-                            v[6] += dPx * dx;
-                            v[7] += dPx * dy;
-                            v8 += dPy * dy;
+                            const float2 dlc = fma2(dlb[i], cz, fma2(dlg[i], cy, mul2(dlr[i], cx)));
+                            const float2 ib = mul2(ioma, bd[i]);
+                            const float2 dA = fma2(Tk, dlc, make_float2(-ib.x, -ib.y));
+                            bd[i] = fma2(dlc, at, bd[i]);
+                            T[i] = Tk;
+                            const float2 dP = mul2(dA, ag);
+                            const float2 dPy = mul2(dP, dy);
+                            s0[b] = add2(s0[b], dP);
+                            sy[b] = add2(sy[b], dPy);
+                            syy[b] = fma2(dPy, dy, syy[b]);
+                        }
+                        float v[8];
+                        v[0] = gr.x + gr.y;
+                        v[1] = gg.x + gg.y;
+                        v[2] = gbl.x + gbl.y;
+                        float v8 = 0.f;
+#pragma unroll
+                        for (int b = 0; b < L::WX; b++) {
+                            const float dx = xt[b].dx;
+                            const float t0 = s0[b].x + s0[b].y, t1 = sy[b].x + sy[b].y;
+                            const float tx = t0 * dx;
+                            v[3] = b ? v[3] + t0 : t0;
+                            v[4] = b ? v[4] + tx : tx;
+                            v[5] = b ? v[5] + t1 : t1;
+                            v[6] = b ? fmaf(tx, dx, v[6]) : tx * dx;
+                            v[7] = b ? fmaf(t1, dx, v[7]) : t1 * dx;
+                            v8 += syy[b].x + syy[b].y;
                         }
                         float s = warp_sum8_transposed(v);
                         float s8 = v8;
@@ -636,13 +709,12 @@ static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
         }                                                    \
     } while (0)
 
-// The (tile, pixels per thread) pairs that exist: 8 x 8 tiles with 1 or 2 pixels per
-// thread, 16 x 16 with 1, 2, 4 or 8, 32 x 32 with 2, 4 or 8 (raster_variant_ok).
+// The (tile, pixels per thread) pairs that exist: 8 x 8 tiles with 2 pixels per thread,
+// 16 x 16 and 32 x 32 with 2, 4 or 8 (raster_variant_ok).
 #define RASTER_SWITCH(FN, tile, batch, ppt, ...)                                           \
     do {                                                                                   \
         if ((tile) == 8) {                                                                 \
-            if ((ppt) == 2) RASTER_BATCHES(FN, 8, batch, 2, __VA_ARGS__);                  \
-            else RASTER_BATCHES(FN, 8, batch, 1, __VA_ARGS__);                             \
+            RASTER_BATCHES(FN, 8, batch, 2, __VA_ARGS__);                                  \
         } else if ((tile) == 32) {                                                         \
             if ((ppt) == 8) RASTER_BATCHES(FN, 32, batch, 8, __VA_ARGS__);                 \
             else if ((ppt) == 4) RASTER_BATCHES(FN, 32, batch, 4, __VA_ARGS__);            \
@@ -650,14 +722,13 @@ static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
         } else {                                                                           \
             if ((ppt) == 8) RASTER_BATCHES(FN, 16, batch, 8, __VA_ARGS__);                 \
             else if ((ppt) == 4) RASTER_BATCHES(FN, 16, batch, 4, __VA_ARGS__);            \
-            else if ((ppt) == 2) RASTER_BATCHES(FN, 16, batch, 2, __VA_ARGS__);            \
-            else RASTER_BATCHES(FN, 16, batch, 1, __VA_ARGS__);                            \
+            else RASTER_BATCHES(FN, 16, batch, 2, __VA_ARGS__);                            \
         }                                                                                  \
     } while (0)
 
 bool raster_variant_ok(int tile, int ppt) {
-    if (tile == 8) return ppt == 1 || ppt == 2;
-    if (tile == 16) return ppt == 1 || ppt == 2 || ppt == 4 || ppt == 8;
+    if (tile == 8) return ppt == 2;
+    if (tile == 16) return ppt == 2 || ppt == 4 || ppt == 8;
     if (tile == 32) return ppt == 2 || ppt == 4 || ppt == 8;
     return false;
 }

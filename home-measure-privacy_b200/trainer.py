@@ -78,7 +78,7 @@ class Renderer:
         cfg.lpt_order = 1 if lpt_order else 0
         cfg.instance_capacity = int(instance_capacity)
         # pixels per raster thread: 1 (16- and 8-pixel tiles) or 4 (32-pixel tiles) unless given
-        cfg.raster_ppt = int(raster_ppt) if raster_ppt is not None else (4 if int(tile_size) == 32 else 1)
+        cfg.raster_ppt = int(raster_ppt) if raster_ppt is not None else 0
         cfg.tile_cull = 1 if tile_cull else 0
         cfg.tile_size = int(tile_size)
         # gpuTiles=False is the reference's CPU tileLists path (trainer/gpu.js:703, :799-806):

@@ -74,9 +74,9 @@ typedef struct GsConfig {
     int32_t instance_capacity; /* initial key-instance capacity; 0 = measured by a first
                               forward.  A step that overflows skips its update, the
                               buffer grows and a synchronous step is redone.           */
-    int32_t raster_ppt;    /* pixels per raster thread: 1 (256 threads per 16 x 16
-                              tile), 2 (128 threads), 4 (64 threads) or 8 (one warp
-                              per tile); 0 = 1                                          */
+    int32_t raster_ppt;    /* pixels per raster thread: 2 (128 threads per 16 x 16
+                              tile), 4 (64 threads) or 8 (one warp per tile); 8-pixel
+                              tiles take 2 only; 0 = 4 (2 for 8-pixel tiles)            */
     int32_t tile_cull;     /* 1 (default) = a tile list holds only splats whose
                               alpha >= alpha_min ellipse reaches the tile: same images
                               and gradients, fewer entries; 0 = the reference's

@@ -163,7 +163,7 @@ def test_batched_equals_plain(hmp):
     assert np.array_equal(out[True], out[False])
 
 
-@pytest.mark.parametrize("ppt", [1, 2, 4, 8])
+@pytest.mark.parametrize("ppt", [2, 4, 8])
 def test_raster_variants_agree(hmp, ppt):
     """Every (shared-memory batch, pixels per thread) variant the autotuner may pick,
     persistent over four uneven views: the same images bit for bit (each pixel blends the
@@ -187,7 +187,7 @@ def test_raster_variants_agree(hmp, ppt):
             r.loss(ssim=0.2, window=1)
             return img, r.backward()
 
-    ref_img, ref_g = run(256, 1)
+    ref_img, ref_g = run(256, 2)
     for batch in (64, 128, 256):
         img, g = run(batch, ppt)
         assert np.array_equal(img, ref_img), batch
@@ -477,8 +477,8 @@ def test_tile_sizes_agree(hmp):
             r.loss(ssim=0.2, window=1)
             return img, r.backward()
 
-    ref_img, ref_g = run(16, 1, 256)
-    for tile, ppts in ((8, (1, 2)), (16, (8,)), (32, (2, 4, 8))):
+    ref_img, ref_g = run(16, 2, 256)
+    for tile, ppts in ((8, (2,)), (16, (4, 8)), (32, (2, 4, 8))):
         for ppt in ppts:
             for batch in (64, 256):
                 img, g = run(tile, ppt, batch)
