@@ -358,15 +358,14 @@ def run_b200(args, rank, local, world, dist):
 def profile_case(args):
     """Small case for ncu captures (one kernel, few launches, ~2 GB on the device): the
     benchmark scene (1M Gaussians, SH3) seen by its three largest views, raster variants
-    fixed at batch 128 and --profile-ppt pixels per thread (default 4, the tuned
-    backward variant; 2 is the tuned forward variant), three graph-replayed training
-    steps."""
+    fixed at batch 128, --profile-ppt pixels per thread (default 4) and --profile-tile
+    pixel tiles (default 16), three graph-replayed training steps."""
     hmp = importlib.import_module("home-measure-privacy_b200")
     c = hmp.config(3)
     cams = c["cameras"][-3:]
     targets = make_targets(hmp, c, cams, 0)
     with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=128, raster_ppt=args.profile_ppt,
-                            device=0) as r:
+                            tile_size=args.profile_tile, device=0) as r:
         r.set_gaussians(c["records"])
         r.set_views(cams)
         off = 0
@@ -651,6 +650,8 @@ def main():
                     help="use the data-parallel step (gradients, NCCL all-reduce, update) even on one GPU")
     ap.add_argument("--autotune-cache", default=None,
                     help="file caching the raster variant choice (a profiled run then uses the unprofiled choice)")
+    ap.add_argument("--profile-tile", type=int, default=16, choices=(8, 16, 32),
+                    help="--profile-case: tile edge in pixels")
     ap.add_argument("--profile-ppt", type=int, default=4, choices=(2, 4, 8),
                     help="pixels per raster thread in --profile-case")
     ap.add_argument("--profile-case", action="store_true",
@@ -705,8 +706,10 @@ def main():
             vs_baseline=None, dtype="f32", data="synthetic",
             config=config_dict(hmp, res["c"], res["cams"], args.config, world),
             raster_variant=dict(tile=res["tuned"]["tile"],
-                                fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1]),
-                                bwd=dict(batch=res["tuned"]["bwd"][0], pixels_per_thread=res["tuned"]["bwd"][1])),
+                                fwd=dict(batch=res["tuned"]["fwd"][0], pixels_per_thread=res["tuned"]["fwd"][1],
+                                         work_tile=res["tuned"]["fwd"][2]),
+                                bwd=dict(batch=res["tuned"]["bwd"][0], pixels_per_thread=res["tuned"]["bwd"][1],
+                                         work_tile=res["tuned"]["bwd"][2])),
             skipped_steps=res["counts"]["skipped_steps"],
             overflow=res["counts"]["overflow"],
             plain_steps_per_s=round(res["plain"], 4) if res["plain"] else None,

@@ -32,7 +32,8 @@ class GsConfig(ctypes.Structure):
                 ("alpha_min", c_float), ("t_min", c_float), ("sh_degree", c_int32), ("rect_mode", c_int32),
                 ("batched", c_int32), ("use_graph", c_int32), ("device", c_int32), ("autotune", c_int32),
                 ("raster_batch", c_int32), ("lpt_order", c_int32), ("instance_capacity", c_int32),
-                ("raster_ppt", c_int32), ("tile_cull", c_int32), ("tile_size", c_int32)]
+                ("raster_ppt", c_int32), ("tile_cull", c_int32), ("tile_size", c_int32),
+                ("raster_work_tile", c_int32)]
 
 
 class GsAdamConfig(ctypes.Structure):

@@ -169,7 +169,8 @@ struct GsContext {
     bool have_loss = false;
     // raster tuning: shared-memory batch and pixels per thread of each kernel
     int tile = GS_TILE;                 // tile edge of binning and raster (8, 16 or 32)
-    int batch_fwd = 256, batch_bwd = 256, ppt_fwd = 1, ppt_bwd = 1;
+    int batch_fwd = 256, batch_bwd = 256, ppt_fwd = 4, ppt_bwd = 4;
+    int wt_fwd = GS_TILE, wt_bwd = GS_TILE;  // raster work-tile edges (<= the tile edge)
     int ctas_fwd = 0, ctas_bwd = 0;
     // graphs
     int64_t generation = 0;
@@ -434,8 +435,8 @@ static int size_instances(GsContext* c, int64_t cap) {
 static SegInfo* seg_ptr(GsContext* c, int idx) { return c->segs.as<SegInfo>() + idx; }
 
 static int persistent_ctas(GsContext* c, bool backward) {
-    const int per_sm = backward ? raster_max_ctas_per_sm(c->tile, c->batch_bwd, c->ppt_bwd, true)
-                                : raster_max_ctas_per_sm(c->tile, c->batch_fwd, c->ppt_fwd, false);
+    const int per_sm = backward ? raster_max_ctas_per_sm(c->tile, c->wt_bwd, c->batch_bwd, c->ppt_bwd, true)
+                                : raster_max_ctas_per_sm(c->tile, c->wt_fwd, c->batch_fwd, c->ppt_fwd, false);
     return c->num_sms * per_sm;
 }
 
@@ -586,7 +587,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
         r.work_counter = &st->work_counter;
     }
     CKI(mark(c, ST_RASTER_FWD));
-    launch_raster_fwd(r, c->tile, c->batch_fwd, c->ppt_fwd, batched ? c->ctas_fwd : 0, c->stream);
+    launch_raster_fwd(r, c->tile, c->wt_fwd, c->batch_fwd, c->ppt_fwd, batched ? c->ctas_fwd : 0, c->stream);
     count_launches(c, ST_RASTER_FWD, 1);
     CK(cudaGetLastError());
     return GS_OK;
@@ -633,7 +634,7 @@ static int enqueue_backward_view(GsContext* c, int first, int step_first, int co
         r.work_counter = &st->work_counter_bwd;
         if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
     }
-    launch_raster_bwd(r, c->tile, c->batch_bwd, c->ppt_bwd, batched ? c->ctas_bwd : 0, c->stream);
+    launch_raster_bwd(r, c->tile, c->wt_bwd, c->batch_bwd, c->ppt_bwd, batched ? c->ctas_bwd : 0, c->stream);
     count_launches(c, ST_RASTER_BWD, 1);
     CKI(mark(c, ST_PROJECT_BWD));
     ProjectBwdArgs pb;
@@ -961,9 +962,12 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     if (cfg.raster_ppt == 0) cfg.raster_ppt = cfg.tile_size == 8 ? 2 : 4;
     if (cfg.tile_size != 8 && cfg.tile_size != 16 && cfg.tile_size != 32)
         return fail(GS_ERR_INVALID_ARG, "tile_size must be 8, 16 or 32");
-    if (!raster_variant_ok(cfg.tile_size, cfg.raster_ppt))
-        return fail(GS_ERR_INVALID_ARG, "raster_ppt %d does not exist for %d-pixel tiles (8: 2; 16 and 32: 2, 4, 8)",
-                    cfg.raster_ppt, cfg.tile_size);
+    if (cfg.raster_work_tile == 0) cfg.raster_work_tile = cfg.tile_size;
+    if (!raster_variant_ok(cfg.tile_size, cfg.raster_work_tile, cfg.raster_ppt))
+        return fail(GS_ERR_INVALID_ARG,
+                    "no raster variant with %d pixels per thread and %d-pixel work tiles for %d-pixel tiles "
+                    "(8: 2 px, work tile 8; 16: 2, 4 or 8 px, work tile 16; 32: 2, 4 or 8 px, work tile 32 or 16)",
+                    cfg.raster_ppt, cfg.raster_work_tile, cfg.tile_size);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0) {
@@ -985,6 +989,7 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     c->tile = cfg.tile_size;
     c->batch_fwd = c->batch_bwd = cfg.raster_batch;
     c->ppt_fwd = c->ppt_bwd = cfg.raster_ppt;
+    c->wt_fwd = c->wt_bwd = cfg.raster_work_tile;
     int rc = GS_OK;
     auto bail = [&](int r) {
         gs_destroy(c);
@@ -1886,9 +1891,11 @@ int gs_get_stats(GsContext* c, GsStats* out) {
     }
     out->kernel_launches_per_step = c->last_step_launches;
     out->raster_batch = c->batch_bwd;
-    out->raster_threads = c->tile * c->tile / c->ppt_bwd;
-    out->raster_variant = (int32_t)((uint32_t)c->batch_fwd | ((uint32_t)c->ppt_fwd << 12) |
-                                    ((uint32_t)c->batch_bwd << 16) | ((uint32_t)c->ppt_bwd << 28));
+    out->raster_threads = c->wt_bwd * c->wt_bwd / c->ppt_bwd;
+    auto wt_code = [](int wt) { return (uint32_t)(wt == 8 ? 3 : (wt == 16 ? 4 : 5)) << 9; };  // log2
+    out->raster_variant = (int32_t)(((uint32_t)c->batch_fwd | wt_code(c->wt_fwd) | ((uint32_t)c->ppt_fwd << 12)) |
+                                    (((uint32_t)c->batch_bwd | wt_code(c->wt_bwd)) << 16) |
+                                    ((uint32_t)c->ppt_bwd << 28));
     out->tile_size = c->tile;
     out->overflow = (int32_t)c->skipped_steps;
     return GS_OK;
@@ -2283,6 +2290,11 @@ int gs_scene_extent(const GsCamera* cams, int32_t count, float* extent_out) {
 static int set_tile(GsContext* c, int tile) {
     if (c->tile == tile) return GS_OK;
     c->tile = tile;
+    // Keep raster variants that exist for the new tile size.
+    for (int* v : {&c->ppt_fwd, &c->ppt_bwd})
+        if (tile == 8) *v = 2;
+    if (!raster_variant_ok(tile, c->wt_fwd, c->ppt_fwd)) c->wt_fwd = tile;
+    if (!raster_variant_ok(tile, c->wt_bwd, c->ppt_bwd)) c->wt_bwd = tile;
     CKI(layout(c));
     // The instance buffers are sized again for this tile size: the sort and emission
     // grids follow their capacity, which another tile size may have grown.
@@ -2298,12 +2310,12 @@ static int set_tile(GsContext* c, int tile) {
 }
 
 // Tuning: for each tile size (16, 8, 32) the persistent forward and backward raster
-// kernels are timed for every (shared-memory batch, pixels per thread) variant that
-// exists for it, on all training views after one forward and loss, keeping the fastest
-// of each; then the tile size's whole forward + loss + backward (projection, binning,
-// blending, loss, their backward; no update) is timed with those variants, and the tile
-// size with the fastest is kept.  The choice is cached per device and workload in
-// `cache_path` (lines "key|tile fwd_batch fwd_ppt bwd_batch bwd_ppt").
+// kernels are timed for every (work tile, shared-memory batch, pixels per thread)
+// variant that exists for it, on all training views after one forward and loss, keeping
+// the fastest of each; then the tile size's whole forward + loss + backward (projection,
+// binning, blending, loss, their backward; no update) is timed with those variants, and
+// the tile size with the fastest is kept.  The choice is cached per device and workload
+// in `cache_path` (lines "key|tile fwd_batch fwd_ppt fwd_wt bwd_batch bwd_ppt bwd_wt").
 int gs_autotune(GsContext* c, const char* cache_path) {
     GS_TRACE("gs_autotune");
     CTX_CHECK(c);
@@ -2313,12 +2325,14 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     char key[256];
     snprintf(key, sizeof key, "%s n=%d views=%d px=%lld deg=%d", c->device_name.c_str(), c->n, c->V,
              (long long)c->total_pixels, c->degree);
-    auto apply = [&](int tile, int bf, int pf, int bb, int pb) -> int {
+    auto apply = [&](int tile, int bf, int pf, int wf, int bb, int pb, int wb) -> int {
         CKI(set_tile(c, tile));
         c->batch_fwd = bf;
         c->ppt_fwd = pf;
+        c->wt_fwd = wf;
         c->batch_bwd = bb;
         c->ppt_bwd = pb;
+        c->wt_bwd = wb;
         c->ctas_fwd = persistent_ctas(c, false);
         c->ctas_bwd = persistent_ctas(c, true);
         drop_graphs(c);
@@ -2330,14 +2344,15 @@ int gs_autotune(GsContext* c, const char* cache_path) {
         if (f) {
             char line[512];
             while (fgets(line, sizeof line, f)) {
-                int t, bf, pf, bb, pb;
+                int t, bf, pf, wf, bb, pb, wb;
                 char* bar = strrchr(line, '|');
                 if (!bar) continue;
                 *bar = 0;
-                if (strcmp(line, key) == 0 && sscanf(bar + 1, "%d %d %d %d %d", &t, &bf, &pf, &bb, &pb) == 5 &&
-                    ok_batch(bf) && ok_batch(bb) && raster_variant_ok(t, pf) && raster_variant_ok(t, pb)) {
+                if (strcmp(line, key) == 0 &&
+                    sscanf(bar + 1, "%d %d %d %d %d %d %d", &t, &bf, &pf, &wf, &bb, &pb, &wb) == 7 && ok_batch(bf) &&
+                    ok_batch(bb) && raster_variant_ok(t, wf, pf) && raster_variant_ok(t, wb, pb)) {
                     fclose(f);
-                    return apply(t, bf, pf, bb, pb);
+                    return apply(t, bf, pf, wf, bb, pb, wb);
                 }
             }
             fclose(f);
@@ -2350,7 +2365,7 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     const GsLossConfig lc{0.2f, 1};
     cudaEvent_t e0 = c->user_events[62], e1 = c->user_events[63];
     float best_total = 1e30f;
-    int best[5] = {c->tile, c->batch_fwd, c->ppt_fwd, c->batch_bwd, c->ppt_bwd};
+    int best[7] = {c->tile, c->batch_fwd, c->ppt_fwd, c->wt_fwd, c->batch_bwd, c->ppt_bwd, c->wt_bwd};
     for (int ti = 0; ti < 3; ti++) {
         const int tile = tiles[ti];
         CKI(set_tile(c, tile));
@@ -2360,14 +2375,16 @@ int gs_autotune(GsContext* c, const char* cache_path) {
         CKI(rc);
         CKI(gs_loss(c, &lc, nullptr));
         float best_f = 1e30f, best_b = 1e30f;
-        int bf = 0, pf = 0, bb = 0, pb = 0;
+        int bf = 0, pf = 0, wf = 0, bb = 0, pb = 0, wb = 0;
         RasterArgs r = raster_args(c, 0, c->V);
         if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
         for (int bi = 0; bi < 3; bi++)
-            for (int ppt = 1; ppt <= 8; ppt *= 2) {
-                if (!raster_variant_ok(tile, ppt)) continue;
+            for (int vi = 0; vi < 6; vi++) {
+                const int ppt = 2 << (vi % 3), wt = vi < 3 ? tile : tile / 2;
+                if (!raster_variant_ok(tile, wt, ppt)) continue;
                 for (int backward = 0; backward < 2; backward++) {
-                    const int ctas = c->num_sms * raster_max_ctas_per_sm(tile, batches[bi], ppt, backward != 0);
+                    const int ctas =
+                        c->num_sms * raster_max_ctas_per_sm(tile, wt, batches[bi], ppt, backward != 0);
                     float total = 0.f;
                     for (int rep = 0; rep < 3; rep++) {
                         CK(cudaMemsetAsync(&st->work_counter, 0, 8, c->stream));
@@ -2378,10 +2395,10 @@ int gs_autotune(GsContext* c, const char* cache_path) {
                         CK(cudaEventRecord(e0, c->stream));
                         if (backward) {
                             r.work_counter = &st->work_counter_bwd;
-                            launch_raster_bwd(r, tile, batches[bi], ppt, ctas, c->stream);
+                            launch_raster_bwd(r, tile, wt, batches[bi], ppt, ctas, c->stream);
                         } else {
                             r.work_counter = &st->work_counter;
-                            launch_raster_fwd(r, tile, batches[bi], ppt, ctas, c->stream);
+                            launch_raster_fwd(r, tile, wt, batches[bi], ppt, ctas, c->stream);
                         }
                         CK(cudaEventRecord(e1, c->stream));
                         CK(cudaGetLastError());
@@ -2394,15 +2411,17 @@ int gs_autotune(GsContext* c, const char* cache_path) {
                         best_b = total;
                         bb = batches[bi];
                         pb = ppt;
+                        wb = wt;
                     }
                     if (!backward && total < best_f) {
                         best_f = total;
                         bf = batches[bi];
                         pf = ppt;
+                        wf = wt;
                     }
                 }
             }
-        CKI(apply(tile, bf, pf, bb, pb));
+        CKI(apply(tile, bf, pf, wf, bb, pb, wb));
         // The tile size's whole forward, loss and backward with its best variants.
         float total = 0.f;
         for (int rep = 0; rep < 3; rep++) {
@@ -2424,17 +2443,20 @@ int gs_autotune(GsContext* c, const char* cache_path) {
             best[0] = tile;
             best[1] = bf;
             best[2] = pf;
-            best[3] = bb;
-            best[4] = pb;
+            best[3] = wf;
+            best[4] = bb;
+            best[5] = pb;
+            best[6] = wb;
         }
     }
-    CKI(apply(best[0], best[1], best[2], best[3], best[4]));
+    CKI(apply(best[0], best[1], best[2], best[3], best[4], best[5], best[6]));
     c->have_loss = false;
     c->last_first = -1;
     if (cache_path) {
         FILE* f = fopen(cache_path, "a");
         if (f) {
-            fprintf(f, "%s|%d %d %d %d %d\n", key, best[0], best[1], best[2], best[3], best[4]);
+            fprintf(f, "%s|%d %d %d %d %d %d %d\n", key, best[0], best[1], best[2], best[3], best[4], best[5],
+                    best[6]);
             fclose(f);
         }
     }

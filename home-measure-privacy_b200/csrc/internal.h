@@ -154,11 +154,14 @@ struct RasterArgs {
     const uint32_t* tile_order;     // optional permutation of the tiles (heavy first)
 };
 // Raster variants: tile edge (8, 16 or 32 pixels), shared-memory batch (64, 128 or 256
-// splats), pixels per thread (raster_variant_ok lists the pairs that exist).
-bool raster_variant_ok(int tile, int ppt);
-void launch_raster_fwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s);
-void launch_raster_bwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s);
-int raster_max_ctas_per_sm(int tile, int batch, int ppt, bool backward);
+// splats), pixels per thread, and the work tile a CTA covers (the tile itself, or for
+// 32-pixel tiles a 16 x 16 quarter of it; raster_variant_ok lists what exists).
+bool raster_variant_ok(int tile, int wt, int ppt);
+void launch_raster_fwd(const RasterArgs& a, int tile, int wt, int batch, int ppt, int persistent_ctas,
+                       cudaStream_t s);
+void launch_raster_bwd(const RasterArgs& a, int tile, int wt, int batch, int ppt, int persistent_ctas,
+                       cudaStream_t s);
+int raster_max_ctas_per_sm(int tile, int wt, int batch, int ppt, bool backward);
 
 // Blends (pixel, splat evaluations) of the last forward, added to *out.
 void launch_blend_count(const ViewDesc* views, int view_first, int num_views, int max_pixels, const uint2* ranges,

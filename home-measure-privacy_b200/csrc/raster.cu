@@ -28,6 +28,9 @@
 // 32-byte vector of float reductions and lane 0 a ninth: one global atomic transaction
 // per (warp, splat) instead of nine CAS loops per pixel (the reference's addF, :148-157).
 //
+// A CTA covers the whole tile or, for 32 x 32 tiles, one 16 x 16 quarter of it (a work
+// tile); every quarter walks the tile's whole list.
+//
 // In the persistent mode a fixed grid pulls (view, tile) work items from a global
 // counter, in an order that puts the longest tile lists first.
 #include "internal.h"
@@ -108,11 +111,21 @@ struct TileInfo {
     float cx0, cy0;              // centre of the tile's first pixel
 };
 
-template <int TILE, int PPT>
+// Work item -> the CTA's pixels: a tile (in the queue's order) and, when the CTA covers a
+// WT x WT work tile smaller than the TILE x TILE list tile, which of the tile's
+// (TILE / WT)^2 work tiles; all of them walk the tile's whole list.
+template <int TILE, int WT>
+constexpr int work_tiles() {
+    return (TILE / WT) * (TILE / WT);
+}
+
+template <int TILE, int WT, int PPT>
 __device__ __forceinline__ TileInfo<PPT> tile_info(const RasterArgs& a, int item) {
-    using L = Lay<TILE, PPT>;
+    using L = Lay<WT, PPT>;
+    constexpr int Q = work_tiles<TILE, WT>();
     TileInfo<PPT> ti;
-    const int local = a.tile_order ? (int)a.tile_order[item] : item;
+    const int tile_item = item / Q, q = item % Q;
+    const int local = a.tile_order ? (int)a.tile_order[tile_item] : tile_item;
     ti.g = a.tile_first + local;
     int vi = a.view_first;
     const int vend = a.view_first + a.num_views;
@@ -121,7 +134,7 @@ __device__ __forceinline__ TileInfo<PPT> tile_info(const RasterArgs& a, int item
     const int lt = ti.g - vw.tile_offset;
     const int tx = lt % vw.tiles_x, ty = lt / vw.tiles_x;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x0 = tx * TILE, y0 = ty * TILE;
+    const int x0 = tx * TILE + (q % (TILE / WT)) * WT, y0 = ty * TILE + (q / (TILE / WT)) * WT;
 #pragma unroll
     for (int p = 0; p < PPT; p++) {
         ti.x[p] = x0 + 8 * L::xg(w, p) + (lane & 7);
@@ -131,7 +144,7 @@ __device__ __forceinline__ TileInfo<PPT> tile_info(const RasterArgs& a, int item
     ti.width = vw.width;
     ti.height = vw.height;
     ti.pixel_offset = vw.pixel_offset;
-    ti.cx0 = (float)x0 + 0.5f;
+    ti.cx0 = (float)x0 + 0.5f;  // first pixel centre of the work tile
     ti.cy0 = (float)y0 + 0.5f;
     return ti;
 }
@@ -326,9 +339,10 @@ constexpr int scale_ctas(int c16, int tile) {
 constexpr int fwd_min_ctas(int tile, int ppt) { return scale_ctas(fwd_min_ctas16(ppt), tile); }
 constexpr int bwd_min_ctas(int tile, int ppt) { return scale_ctas(bwd_min_ctas16(ppt), tile); }
 
-template <int TILE, int BATCH, int PPT>
-__global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) raster_fwd_kernel(RasterArgs a) {
-    using L = Lay<TILE, PPT>;
+template <int TILE, int WT, int BATCH, int PPT>
+__global__ void __launch_bounds__(Lay<WT, PPT>::NT, fwd_min_ctas(WT, PPT)) raster_fwd_kernel(RasterArgs a) {
+    using L = Lay<WT, PPT>;
+    const int items = a.num_tiles * work_tiles<TILE, WT>();
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -338,8 +352,8 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) r
     const float log_amin = __logf(a.alpha_min);
     const float qthr = __log2f(a.alpha_min);
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
-    while (item < a.num_tiles) {
-        const TileInfo<PPT> ti = tile_info<TILE, PPT>(a, item);
+    while (item < items) {
+        const TileInfo<PPT> ti = tile_info<TILE, WT, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x, end = rg.y;
         // Pixel pairs (2i, 2i + 1) share an x band.  A pixel blends while T > t_min (the
@@ -380,7 +394,7 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, fwd_min_ctas(TILE, PPT)) r
             const float4* qs = s_q[buf];
             for (int gb = 0; gb < cnt && gdone != all_groups<PPT>(); gb += 32) {
                 const int jl = gb + lane;
-                const uint32_t gm = jl < cnt ? group_mask<TILE, PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) : 0u;
+                const uint32_t gm = jl < cnt ? group_mask<WT, PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) : 0u;
                 uint32_t live = __ballot_sync(FULL_MASK, (gm & ~gdone) != 0u);
                 while (live) {
                     const int jj = __ffs(live) - 1;
@@ -479,9 +493,10 @@ __device__ __forceinline__ float warp_sum8_transposed(float v[8]) {
     return v[0];
 }
 
-template <int TILE, int BATCH, int PPT>
-__global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) raster_bwd_kernel(RasterArgs a) {
-    using L = Lay<TILE, PPT>;
+template <int TILE, int WT, int BATCH, int PPT>
+__global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raster_bwd_kernel(RasterArgs a) {
+    using L = Lay<WT, PPT>;
+    const int items = a.num_tiles * work_tiles<TILE, WT>();
     __shared__ __align__(16) float4 s_g0[2][BATCH];
     __shared__ __align__(16) float4 s_g1[2][BATCH];
     __shared__ __align__(16) float4 s_c[2][BATCH];
@@ -504,8 +519,8 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
         sel_b = (g == 4 || g == 5) ? 1.f : 0.f;
     }
     int item = next_item(a.work_counter, &s_item, blockIdx.x);
-    while (item < a.num_tiles) {
-        const TileInfo<PPT> ti = tile_info<TILE, PPT>(a, item);
+    while (item < items) {
+        const TileInfo<PPT> ti = tile_info<TILE, WT, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
         // Pixel pairs (2i, 2i + 1) share an x band (see f2).
@@ -581,7 +596,7 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
                         uint32_t act = 0u;  // groups with a pixel whose last is past this entry
 #pragma unroll
                         for (int p = 0; p < PPT; p++) act |= kl < gmax[p] ? (1u << p) : 0u;
-                        if (act) gm = group_mask<TILE, PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) & act;
+                        if (act) gm = group_mask<WT, PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) & act;
                     }
                     uint32_t live = __ballot_sync(FULL_MASK, gm != 0u);
                     while (live) {
@@ -690,72 +705,80 @@ __global__ void __launch_bounds__(Lay<TILE, PPT>::NT, bwd_min_ctas(TILE, PPT)) r
     }
 }
 
-// Variant = (tile edge, shared-memory batch, pixels per thread); the autotuner picks one.
-template <int TILE, int BATCH, int PPT>
+// Variant = (list tile edge, work tile edge, shared-memory batch, pixels per thread);
+// the autotuner picks one.
+template <int TILE, int WT, int BATCH, int PPT>
 static void fwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
-    raster_fwd_kernel<TILE, BATCH, PPT><<<ctas, Lay<TILE, PPT>::NT, 0, s>>>(a);
+    if (!a.work_counter) ctas = a.num_tiles * work_tiles<TILE, WT>();
+    raster_fwd_kernel<TILE, WT, BATCH, PPT><<<ctas, Lay<WT, PPT>::NT, 0, s>>>(a);
 }
-template <int TILE, int BATCH, int PPT>
+template <int TILE, int WT, int BATCH, int PPT>
 static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
-    raster_bwd_kernel<TILE, BATCH, PPT><<<ctas, Lay<TILE, PPT>::NT, 0, s>>>(a);
+    if (!a.work_counter) ctas = a.num_tiles * work_tiles<TILE, WT>();
+    raster_bwd_kernel<TILE, WT, BATCH, PPT><<<ctas, Lay<WT, PPT>::NT, 0, s>>>(a);
 }
 
-#define RASTER_BATCHES(FN, T, batch, P, ...)                 \
-    do {                                                     \
-        switch (batch) {                                     \
-            case 64: FN<T, 64, P>(__VA_ARGS__); break;       \
-            case 128: FN<T, 128, P>(__VA_ARGS__); break;     \
-            default: FN<T, 256, P>(__VA_ARGS__); break;      \
-        }                                                    \
+#define RASTER_BATCHES(FN, T, W, batch, P, ...)                 \
+    do {                                                        \
+        switch (batch) {                                        \
+            case 64: FN<T, W, 64, P>(__VA_ARGS__); break;       \
+            case 128: FN<T, W, 128, P>(__VA_ARGS__); break;     \
+            default: FN<T, W, 256, P>(__VA_ARGS__); break;      \
+        }                                                       \
     } while (0)
 
-// The (tile, pixels per thread) pairs that exist: 8 x 8 tiles with 2 pixels per thread,
-// 16 x 16 and 32 x 32 with 2, 4 or 8 (raster_variant_ok).
-#define RASTER_SWITCH(FN, tile, batch, ppt, ...)                                           \
+#define RASTER_PPTS(FN, T, W, batch, ppt, ...)                                   \
+    do {                                                                         \
+        if ((ppt) == 8) RASTER_BATCHES(FN, T, W, batch, 8, __VA_ARGS__);         \
+        else if ((ppt) == 4) RASTER_BATCHES(FN, T, W, batch, 4, __VA_ARGS__);    \
+        else RASTER_BATCHES(FN, T, W, batch, 2, __VA_ARGS__);                    \
+    } while (0)
+
+// The (list tile, work tile, pixels per thread) variants that exist: 8 x 8 tiles with
+// 2 pixels per thread; 16 x 16 tiles with 2, 4 or 8; 32 x 32 tiles with work tiles of
+// 32 x 32 or 16 x 16 and 2, 4 or 8 (raster_variant_ok).
+#define RASTER_SWITCH(FN, tile, wt, batch, ppt, ...)                                       \
     do {                                                                                   \
         if ((tile) == 8) {                                                                 \
-            RASTER_BATCHES(FN, 8, batch, 2, __VA_ARGS__);                                  \
+            RASTER_BATCHES(FN, 8, 8, batch, 2, __VA_ARGS__);                               \
         } else if ((tile) == 32) {                                                         \
-            if ((ppt) == 8) RASTER_BATCHES(FN, 32, batch, 8, __VA_ARGS__);                 \
-            else if ((ppt) == 4) RASTER_BATCHES(FN, 32, batch, 4, __VA_ARGS__);            \
-            else RASTER_BATCHES(FN, 32, batch, 2, __VA_ARGS__);                            \
+            if ((wt) == 16) RASTER_PPTS(FN, 32, 16, batch, ppt, __VA_ARGS__);              \
+            else RASTER_PPTS(FN, 32, 32, batch, ppt, __VA_ARGS__);                         \
         } else {                                                                           \
-            if ((ppt) == 8) RASTER_BATCHES(FN, 16, batch, 8, __VA_ARGS__);                 \
-            else if ((ppt) == 4) RASTER_BATCHES(FN, 16, batch, 4, __VA_ARGS__);            \
-            else RASTER_BATCHES(FN, 16, batch, 2, __VA_ARGS__);                            \
+            RASTER_PPTS(FN, 16, 16, batch, ppt, __VA_ARGS__);                              \
         }                                                                                  \
     } while (0)
 
-bool raster_variant_ok(int tile, int ppt) {
-    if (tile == 8) return ppt == 2;
-    if (tile == 16) return ppt == 2 || ppt == 4 || ppt == 8;
-    if (tile == 32) return ppt == 2 || ppt == 4 || ppt == 8;
+bool raster_variant_ok(int tile, int wt, int ppt) {
+    if (tile == 8) return wt == 8 && ppt == 2;
+    if (tile == 16) return wt == 16 && (ppt == 2 || ppt == 4 || ppt == 8);
+    if (tile == 32) return (wt == 32 || wt == 16) && (ppt == 2 || ppt == 4 || ppt == 8);
     return false;
 }
 
-void launch_raster_fwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
-    const int ctas = a.work_counter ? persistent_ctas : a.num_tiles;
-    if (ctas <= 0 || a.num_tiles <= 0) return;
-    RASTER_SWITCH(fwd_launch, tile, batch, ppt, a, ctas, s);
+void launch_raster_fwd(const RasterArgs& a, int tile, int wt, int batch, int ppt, int persistent_ctas,
+                       cudaStream_t s) {
+    if (a.num_tiles <= 0 || (a.work_counter && persistent_ctas <= 0)) return;
+    RASTER_SWITCH(fwd_launch, tile, wt, batch, ppt, a, persistent_ctas, s);
 }
 
-void launch_raster_bwd(const RasterArgs& a, int tile, int batch, int ppt, int persistent_ctas, cudaStream_t s) {
-    const int ctas = a.work_counter ? persistent_ctas : a.num_tiles;
-    if (ctas <= 0 || a.num_tiles <= 0) return;
-    RASTER_SWITCH(bwd_launch, tile, batch, ppt, a, ctas, s);
+void launch_raster_bwd(const RasterArgs& a, int tile, int wt, int batch, int ppt, int persistent_ctas,
+                       cudaStream_t s) {
+    if (a.num_tiles <= 0 || (a.work_counter && persistent_ctas <= 0)) return;
+    RASTER_SWITCH(bwd_launch, tile, wt, batch, ppt, a, persistent_ctas, s);
 }
 
-template <int TILE, int BATCH, int PPT>
+template <int TILE, int WT, int BATCH, int PPT>
 static void occ(int* n, bool backward) {
     if (backward)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_bwd_kernel<TILE, BATCH, PPT>, Lay<TILE, PPT>::NT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_bwd_kernel<TILE, WT, BATCH, PPT>, Lay<WT, PPT>::NT, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_fwd_kernel<TILE, BATCH, PPT>, Lay<TILE, PPT>::NT, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, raster_fwd_kernel<TILE, WT, BATCH, PPT>, Lay<WT, PPT>::NT, 0);
 }
 
-int raster_max_ctas_per_sm(int tile, int batch, int ppt, bool backward) {
+int raster_max_ctas_per_sm(int tile, int wt, int batch, int ppt, bool backward) {
     int n = 0;
-    RASTER_SWITCH(occ, tile, batch, ppt, &n, backward);
+    RASTER_SWITCH(occ, tile, wt, batch, ppt, &n, backward);
     cudaGetLastError();
     return n < 1 ? 1 : n;
 }

@@ -274,6 +274,8 @@ napi_value Create(napi_env env, napi_callback_info info) {
         cfg.tile_cull = (int32_t)num(env, o, "tileCull", cfg.tile_cull);
         cfg.raster_batch = (int32_t)num(env, o, "rasterBatch", cfg.raster_batch);
         cfg.raster_ppt = (int32_t)num(env, o, "rasterPixelsPerThread", cfg.raster_ppt);
+        cfg.tile_size = (int32_t)num(env, o, "tileSize", cfg.tile_size);
+        cfg.raster_work_tile = (int32_t)num(env, o, "rasterWorkTile", cfg.raster_work_tile);
     }
     GsContext* ctx = nullptr;
     const int rc = gs_create(&cfg, &ctx);

@@ -65,7 +65,7 @@ class Renderer:
 
     def __init__(self, gpuTiles=True, sh_degree=0, near=0.2, batched=True, use_graph=True, device=0,
                  raster_batch=256, lpt_order=True, rect_mode=None, instance_capacity=0, raster_ppt=None,
-                 tile_cull=True, tile_size=16):
+                 tile_cull=True, tile_size=16, raster_work_tile=0):
         self.lib = N.load()
         cfg = N.GsConfig()
         self.lib.gs_config_default(ctypes.byref(cfg))
@@ -81,6 +81,7 @@ class Renderer:
         cfg.raster_ppt = int(raster_ppt) if raster_ppt is not None else 0
         cfg.tile_cull = 1 if tile_cull else 0
         cfg.tile_size = int(tile_size)
+        cfg.raster_work_tile = int(raster_work_tile)
         # gpuTiles=False is the reference's CPU tileLists path (trainer/gpu.js:703, :799-806):
         # here the binning always runs on the GPU, with tileLists' tile rectangle.
         cfg.rect_mode = int(rect_mode) if rect_mode is not None else (0 if gpuTiles else 1)
@@ -472,13 +473,19 @@ class Renderer:
         N.check(self.lib.gs_debug_lookback_wait(self.ctx, int(polls)))
 
     def autotune(self, cache_path=None):
-        """Picks the tile size and raster variants; returns {tile, fwd: (batch, ppt),
-        bwd: (batch, ppt)}."""
+        """Picks the tile size and raster variants; returns {tile, fwd: (batch, ppt,
+        work tile), bwd: (batch, ppt, work tile)}."""
         N.check(self.lib.gs_autotune(self.ctx, cache_path.encode() if cache_path else None))
+        return self.raster_variant()
+
+    def raster_variant(self):
+        """The raster variants in use: {tile, fwd: (batch, ppt, work tile), bwd: ...}."""
         st = self.stats()
-        v = st["raster_variant"]
-        return dict(tile=int(st["tile_size"]), fwd=(v & 0xfff, (v >> 12) & 0xf),
-                    bwd=((v >> 16) & 0xfff, (v >> 28) & 0xf))
+        v = st["raster_variant"] & 0xffffffff
+
+        def one(h):
+            return (h & 0x1ff, (h >> 12) & 0xf, 1 << ((h >> 9) & 0x7))
+        return dict(tile=int(st["tile_size"]), fwd=one(v & 0xffff), bwd=one(v >> 16))
 
     def stage_times(self):
         ms = np.zeros(N.GS_NUM_STAGES, np.float64)

@@ -84,6 +84,9 @@ typedef struct GsConfig {
     int32_t tile_size;     /* tile edge in pixels: 16 (default, the reference's,
                               trainer/gpu.js:118), 8 or 32; 0 = 16.  Images are the same
                               for every size; gs_autotune may change it                 */
+    int32_t raster_work_tile; /* pixels a raster CTA covers: the whole tile (0 or the
+                              tile edge) or, for 32-pixel tiles, 16 (each 16 x 16
+                              quarter a CTA of its own, walking the tile's list)        */
 } GsConfig;
 
 /* Adam settings.  The per-group learning rates are the reference's (trainer/gpu.js:846,
@@ -414,7 +417,9 @@ typedef struct GsStats {
     int32_t raster_batch;
     int32_t raster_threads;
     int32_t overflow;
-    int32_t raster_variant;  /* fwd batch | fwd ppt << 12 | bwd batch << 16 | bwd ppt << 28 */
+    int32_t raster_variant;  /* per kernel (forward in bits 0-15, backward in 16-31): batch
+                                (bits 0-8) | log2(work tile edge) << 9 | pixels per
+                                thread << 12                                           */
     int32_t tile_size;       /* tile edge in pixels in use (gs_autotune may have changed it) */
 } GsStats;
 GS_API int gs_get_stats(GsContext* ctx, GsStats* out);

@@ -58,7 +58,7 @@ def test_struct_layouts_match_header(hmp):
     from importlib import import_module
     N = import_module("home-measure-privacy_b200._native")
     assert ctypes.sizeof(N.GsCamera) == 72
-    assert ctypes.sizeof(N.GsConfig) == 4 * 17
+    assert ctypes.sizeof(N.GsConfig) == 4 * 18
     assert ctypes.sizeof(N.GsAdamConfig) == 36
     assert ctypes.sizeof(N.GsLossConfig) == 8
 

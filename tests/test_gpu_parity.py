@@ -454,15 +454,15 @@ def test_pipelined_host_step_matches_synchronous(hmp):
 
 # ------------------------------------------------------------------------------ tile sizes
 def test_tile_sizes_agree(hmp):
-    """8-, 16- and 32-pixel tiles with every (batch, pixels per thread) variant that exists
-    for them: the same images bit for bit (each pixel blends the same splats in the same
-    order, whatever the tiles) and the same gradients up to atomic order."""
+    """8-, 16- and 32-pixel tiles with every (batch, pixels per thread, work tile) variant
+    that exists for them: the same images bit for bit (each pixel blends the same splats
+    in the same order, whatever the tiles) and the same gradients up to atomic order."""
     rec = hmp.synthetic_scene(40_000, 3, 17, "normal", (-4.5, 0.7), (0.0, 1.5))
     tg = hmp.scene.jitter_means(rec, 18)
     cams = hmp.ring_cameras([(333, 250), (512, 384), (200, 411)], 4.0)
 
-    def run(tile, ppt, batch):
-        with make(hmp, 3, tile_size=tile, raster_ppt=ppt, raster_batch=batch) as r:
+    def run(tile, ppt, batch, wt=0):
+        with make(hmp, 3, tile_size=tile, raster_ppt=ppt, raster_batch=batch, raster_work_tile=wt) as r:
             r.set_gaussians(tg)
             r.set_views(cams)
             timgs = r.forward(0, 3)
@@ -474,16 +474,18 @@ def test_tile_sizes_agree(hmp):
             r.set_gaussians(rec)
             img = r.forward(0, 3)
             assert r.stats()["tile_size"] == tile
+            v = r.raster_variant()
+            assert v["fwd"][2] == (wt or tile) and v["bwd"][2] == (wt or tile)
             r.loss(ssim=0.2, window=1)
             return img, r.backward()
 
     ref_img, ref_g = run(16, 2, 256)
-    for tile, ppts in ((8, (2,)), (16, (4, 8)), (32, (2, 4, 8))):
+    for tile, wt, ppts in ((8, 0, (2,)), (16, 0, (4, 8)), (32, 0, (2, 4, 8)), (32, 16, (2, 4, 8))):
         for ppt in ppts:
             for batch in (64, 256):
-                img, g = run(tile, ppt, batch)
-                assert np.array_equal(img, ref_img), (tile, ppt, batch)
-                assert rel_err(g, ref_g) < 1e-5, (tile, ppt, batch)
+                img, g = run(tile, ppt, batch, wt)
+                assert np.array_equal(img, ref_img), (tile, wt, ppt, batch)
+                assert rel_err(g, ref_g) < 1e-5, (tile, wt, ppt, batch)
 
 
 def test_autotune_picks_a_tile_size_and_trains_the_same(hmp):
