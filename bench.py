@@ -192,6 +192,14 @@ def profiled_issue(kernel):
         return None
 
 
+T_START = time.perf_counter()
+
+
+def progress(msg):
+    """Phase timings on stderr (the JSON line stays the only stdout output)."""
+    print(f"[bench {time.perf_counter() - T_START:8.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
 def run_b200(args, rank, local, world, dist):
     hmp = importlib.import_module("home-measure-privacy_b200")
     from importlib import import_module
@@ -274,8 +282,10 @@ def run_b200(args, rank, local, world, dist):
         return t
 
     # ---- batched (headline)
+    progress("targets ready")
     r = setup(True)
     tuned = r.autotune(args.autotune_cache)
+    progress(f"autotuned: {tuned}")
     clocks = Clocks(device)
     clocks.start()
     time.sleep(1.0)  # nvidia-smi needs a moment before its first sample
@@ -287,6 +297,7 @@ def run_b200(args, rank, local, world, dist):
     res["stats"] = st
     res["stages"] = stages
     ms_step = t_b / args.steps
+    progress(f"timed: {ms_step:.3f} ms/step, {int(st['instances']):,} instances")
     # ---- e2e through the public API: pinned host targets in, loss out, every step
     e2e = None
     if not args.no_e2e:
@@ -338,6 +349,7 @@ def run_b200(args, rank, local, world, dist):
         res["densify"] = densify_measure(hmp, r, c, cams, ad, lam, window, args)
     r.close()
     # ---- plain: one view per launch per stage, same step
+    progress("e2e done")
     plain = None
     if not args.no_plain and not dp:
         rp = setup(False)
@@ -350,6 +362,7 @@ def run_b200(args, rank, local, world, dist):
         t_d = timed(rd, max(3, args.steps // 4), 2)
         res["plain_direct"] = 1000.0 / (t_d / max(3, args.steps // 4))
         rd.close()
+    progress("plain path done")
     res.update(ms_step=ms_step, plain=plain, e2e=e2e, tuned=tuned, n=n, V=V, pixels=pixels, c=c, cams=cams)
     res["bytes"] = algorithmic_bytes(st, n, hmp.stride(c["degree"]), V, pixels, int(st["tiles"]))
     return res

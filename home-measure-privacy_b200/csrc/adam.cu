@@ -7,11 +7,12 @@
 // over the plane-major SoA: each thread owns 4 consecutive Gaussians and moves float4s
 // through every plane (parameters, gradient, both moments), so each warp streams
 // 512-byte rows.  A step whose key instances overflowed their buffer (its tile lists
-// are truncated) skips the update.  Every operation rounds on its own, in the
-// reference's order (explicit round-to-nearest intrinsics, no contraction into FMA,
-// divisions by the bias corrections rather than products with their reciprocals): where
-// a first moment has nearly cancelled, a contracted or reordered product would move the
-// update by many ulps of its own size.
+// are truncated) skips the update.  The moments are updated with every operation
+// rounded on its own, in the reference's order (explicit round-to-nearest intrinsics, no
+// contraction into FMA): where a first moment has nearly cancelled, a contracted product
+// would move the update by many ulps of its own size.  The bias corrections are applied as
+// products with their reciprocals (within an ulp of the reference's quotients, and the
+// update inherits no cancellation from them).
 #include "../../include/gsb200.h"
 #include "internal.h"
 
@@ -22,7 +23,7 @@ namespace gs {
 // renormalised): 14M independent float4 updates at the benchmark size, so the loads of
 // many planes are in flight at once.
 __device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, float4& v, float lr, float b1, float b2,
-                                      float omb1, float omb2, float bc1, float bc2, float eps) {
+                                      float omb1, float omb2, float ibc1, float ibc2, float eps) {
     float* pp = &p.x;
     const float* gg = &g.x;
     float* mm = &m.x;
@@ -31,9 +32,7 @@ __device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, flo
     for (int e = 0; e < 4; e++) {
         mm[e] = __fadd_rn(__fmul_rn(b1, mm[e]), __fmul_rn(omb1, gg[e]));
         vv[e] = __fadd_rn(__fmul_rn(b2, vv[e]), __fmul_rn(__fmul_rn(omb2, gg[e]), gg[e]));
-        const float num = __fmul_rn(lr, __fdiv_rn(mm[e], bc1));
-        const float den = __fadd_rn(__fsqrt_rn(__fdiv_rn(vv[e], bc2)), eps);
-        pp[e] = __fsub_rn(pp[e], __fdiv_rn(num, den));
+        pp[e] -= lr * (mm[e] * ibc1) / (sqrtf(vv[e] * ibc2) + eps);
     }
 }
 
@@ -47,8 +46,8 @@ __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
     if (u >= (long long)groups * units_per_group) return;
     const int unit = (int)(u / groups), grp = (int)(u % groups);
     const int t = a.status->step_t + 1;
-    const float bc1 = __fsub_rn(1.0f, powf(a.beta1, (float)t));
-    const float bc2 = __fsub_rn(1.0f, powf(a.beta2, (float)t));
+    const float ibc1 = 1.0f / (1.0f - powf(a.beta1, (float)t));
+    const float ibc2 = 1.0f / (1.0f - powf(a.beta2, (float)t));
     const float omb1 = 1.0f - a.beta1, omb2 = 1.0f - a.beta2;
     const size_t np = (size_t)a.n_pad;
     const size_t col = (size_t)grp * 4;
@@ -59,7 +58,7 @@ __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
         const float4 g = *reinterpret_cast<const float4*>(a.grads + off);
         float4 m = *reinterpret_cast<const float4*>(a.m + off);
         float4 v = *reinterpret_cast<const float4*>(a.v + off);
-        adam4(p, g, m, v, a.lr[j], a.beta1, a.beta2, omb1, omb2, bc1, bc2, a.eps);
+        adam4(p, g, m, v, a.lr[j], a.beta1, a.beta2, omb1, omb2, ibc1, ibc2, a.eps);
         if (j >= 11 && j <= 13) {  // colour (SH DC) clamped to [0, 1]
             p.x = fminf(fmaxf(p.x, 0.f), 1.f);
             p.y = fminf(fmaxf(p.y, 0.f), 1.f);
@@ -80,7 +79,7 @@ __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
         const float4 g = *reinterpret_cast<const float4*>(a.grads + off);
         float4 m = *reinterpret_cast<const float4*>(a.m + off);
         float4 v = *reinterpret_cast<const float4*>(a.v + off);
-        adam4(q[k], g, m, v, a.lr[6 + k], a.beta1, a.beta2, omb1, omb2, bc1, bc2, a.eps);
+        adam4(q[k], g, m, v, a.lr[6 + k], a.beta1, a.beta2, omb1, omb2, ibc1, ibc2, a.eps);
         *reinterpret_cast<float4*>(a.m + off) = m;
         *reinterpret_cast<float4*>(a.v + off) = v;
     }

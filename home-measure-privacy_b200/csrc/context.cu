@@ -2366,13 +2366,25 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     cudaEvent_t e0 = c->user_events[62], e1 = c->user_events[63];
     float best_total = 1e30f;
     int best[7] = {c->tile, c->batch_fwd, c->ppt_fwd, c->wt_fwd, c->batch_bwd, c->ppt_bwd, c->wt_bwd};
+    int64_t inst16 = -1;  // key instances with 16-pixel tiles (measured first)
     for (int ti = 0; ti < 3; ti++) {
         const int tile = tiles[ti];
+        if (inst16 >= 0) {
+            // A tile size whose instance buffers would not fit is skipped: instances scale
+            // about as the inverse tile area (heavy-tailed scenes with splats over hundreds
+            // of tiles reach billions of 8-pixel instances).
+            size_t free_b = 0, total_b = 0;
+            CK(cudaMemGetInfo(&free_b, &total_b));
+            const double est = (double)inst16 * (16.0 / tile) * (16.0 / tile) * 1.25;
+            const double need = est * 20.0;  // keys, values, their alternates, emission
+            if (est > 2.0e9 || need > 0.5 * (double)(free_b + (size_t)c->inst_cap * 16)) continue;
+        }
         CKI(set_tile(c, tile));
         c->cfg.batched = 1;
         int rc = run_forward(c, 0, c->V);
         c->cfg.batched = saved_batched;
         CKI(rc);
+        if (tile == 16) inst16 = (int64_t)c->status_host->instances_needed;
         CKI(gs_loss(c, &lc, nullptr));
         float best_f = 1e30f, best_b = 1e30f;
         int bf = 0, pf = 0, wf = 0, bb = 0, pb = 0, wb = 0;

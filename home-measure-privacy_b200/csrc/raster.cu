@@ -523,34 +523,25 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
         const TileInfo<PPT> ti = tile_info<TILE, WT, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
-        // Pixel pairs (2i, 2i + 1) share an x band (see f2).
-        constexpr int NP = PPT / 2;
-        float pxf[L::WX];
-        float2 pyf[NP], T[NP], dlr[NP], dlg[NP], dlb[NP], bd[NP];
+        float pxf[L::WX], pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
         uint32_t mylast[PPT], gmax[PPT];
 #pragma unroll
         for (int b = 0; b < L::WX; b++) pxf[b] = (float)ti.x[b * L::WY] + 0.5f;  // the warp's x bands
         unsigned int wmax = start;
 #pragma unroll
-        for (int i = 0; i < NP; i++) {
-            pyf[i] = make_float2((float)ti.y[2 * i] + 0.5f, (float)ti.y[2 * i + 1] + 0.5f);
-            T[i] = dlr[i] = dlg[i] = dlb[i] = f2(0.f);
-            bd[i] = f2(0.f);  // dL . (colour of the splats behind), "behind"
-        }
-#pragma unroll
         for (int p = 0; p < PPT; p++) {
-            const int i = p / 2;
+            pyf[p] = (float)ti.y[p] + 0.5f;
+            T[p] = 0.f;
+            dlr[p] = dlg[p] = dlb[p] = 0.f;
+            bd[p] = 0.f;  // dL . (colour of the splats behind), "behind"
             mylast[p] = start;
             if (ti.inside[p]) {
                 const size_t pix = (size_t)ti.pixel_offset + (size_t)ti.y[p] * ti.width + ti.x[p];
+                T[p] = a.t_final[pix];
                 mylast[p] = a.last[pix];
-                const float t = a.t_final[pix], r = a.dl[pix * 3 + 0], g = a.dl[pix * 3 + 1],
-                            bl = a.dl[pix * 3 + 2];
-                if (p & 1) {
-                    T[i].y = t, dlr[i].y = r, dlg[i].y = g, dlb[i].y = bl;
-                } else {
-                    T[i].x = t, dlr[i].x = r, dlg[i].x = g, dlb[i].x = bl;
-                }
+                dlr[p] = a.dl[pix * 3 + 0];
+                dlg[p] = a.dl[pix * 3 + 1];
+                dlb[p] = a.dl[pix * 3 + 2];
             }
             // Each group walks from the largest last of its pixels.
             unsigned int gm = mylast[p];
@@ -610,73 +601,61 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                         const float4 q = qs[j];
                         const float4 c = cs[j];
                         const float qlo = c.w, qhi = 2.0f * qthr - c.w;  // the splat's band
-                        const float2 qc = f2(q.z), ngy = f2(-g0.y);
-                        const float2 cx = f2(c.x), cy = f2(c.y), cz = f2(c.z);
                         XTerm xt[L::WX];
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
                         // Per pixel: colour terms and dP = dL/dpower, summed per x band as
-                        // sum dP, sum dP dy, sum dP dy^2 (dx is the band's); after the group
-                        // loop the bands give the moments (sum dP, dP dx, dP dy, dP dx^2,
-                        // dP dx dy, dP dy^2) from which the splat's conic and opacity make
-                        // the gradients of (opacity logit, u, v, A, B, C) after the reduction.
-                        float2 gr = f2(0.f), gg = f2(0.f), gbl = f2(0.f);
-                        float2 s0[L::WX], sy[L::WX], syy[L::WX];
+                        // sum dP, sum dP dy, sum dP dy^2 (the band's pixels share dx); after
+                        // the group loop the bands give the moments (sum dP, dP dx, dP dy,
+                        // dP dx^2, dP dx dy, dP dy^2) from which the splat's conic and
+                        // opacity make the gradients of (opacity logit, u, v, A, B, C) after
+                        // the reduction.  Scalar arithmetic: pairing the pixels for the
+                        // packed instructions costs more register moves than it saves here.
+                        float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                        float s0[L::WX], sy[L::WX], syy[L::WX];
 #pragma unroll
-                        for (int b = 0; b < L::WX; b++) s0[b] = sy[b] = syy[b] = f2(0.f);
+                        for (int b = 0; b < L::WX; b++) s0[b] = sy[b] = syy[b] = 0.f;
 #pragma unroll
-                        for (int i = 0; i < NP; i++) {
-                            if (!((m >> (2 * i)) & 3u)) continue;
+                        for (int p = 0; p < PPT; p++) {
+                            if (!(m & (1u << p))) continue;
                             // Branch-free per lane: alpha = 0 adds zeros and leaves T
                             // (T / 1) and dL.behind as they are.
-                            const int b = (2 * i) / L::WY;
+                            const int b = p / L::WY;
                             const XTerm& x = xt[b];
-                            const float2 dy = add2(pyf[i], ngy);
-                            const float2 e = exponent2(x, qc, dy);
-                            bool h0, h1;
-                            const float a0 = alpha_pix(e.x, x.dx, dy.x, x.inb && k < mylast[2 * i], g0, g1,
-                                                       a.alpha_max, a.alpha_min, qlo, qhi, h0);
-                            const float a1 = alpha_pix(e.y, x.dx, dy.y, x.inb && k < mylast[2 * i + 1], g0, g1,
-                                                       a.alpha_max, a.alpha_min, qlo, qhi, h1);
-                            const float2 alpha = make_float2(a0, a1);
-                            // alpha clamped at alpha_max has no gradient through the power.
-                            const float2 ag = make_float2(a0 < a.alpha_max ? a0 : 0.f, a1 < a.alpha_max ? a1 : 0.f);
-                            const float2 oma = fma2(alpha, f2(-1.0f), f2(1.0f));  // 1 - alpha
-                            const float2 ioma = make_float2(rcp_approx(oma.x), rcp_approx(oma.y));
-                            const float2 Tk = mul2(T[i], ioma);
-                            const float2 at = mul2(alpha, Tk);
-                            gr = fma2(dlr[i], at, gr);
-                            gg = fma2(dlg[i], at, gg);
-                            gbl = fma2(dlb[i], at, gbl);
+                            const float dy = pyf[p] - g0.y;
+                            const float e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, x.b0.x), x.a0.x);
+                            bool hit;
+                            const float alpha = alpha_pix(e, x.dx, dy, x.inb && k < mylast[p], g0, g1, a.alpha_max,
+                                                          a.alpha_min, qlo, qhi, hit);
+                            const float ioma = rcp_approx(1.0f - alpha);
+                            const float Tk = T[p] * ioma;
+                            const float at = alpha * Tk;
+                            v[0] += dlr[p] * at;
+                            v[1] += dlg[p] * at;
+                            v[2] += dlb[p] * at;
                             // dL/dalpha = dL.(c T_k - behind / (1 - alpha)); only dL.behind is
                             // kept per pixel.
-                            const float2 dlc = fma2(dlb[i], cz, fma2(dlg[i], cy, mul2(dlr[i], cx)));
-                            const float2 ib = mul2(ioma, bd[i]);
-                            const float2 dA = fma2(Tk, dlc, make_float2(-ib.x, -ib.y));
-                            bd[i] = fma2(dlc, at, bd[i]);
-                            T[i] = Tk;
-                            const float2 dP = mul2(dA, ag);
-                            const float2 dPy = mul2(dP, dy);
-                            s0[b] = add2(s0[b], dP);
-                            sy[b] = add2(sy[b], dPy);
-                            syy[b] = fma2(dPy, dy, syy[b]);
+                            const float dlc = dlr[p] * c.x + dlg[p] * c.y + dlb[p] * c.z;
+                            const float dA = Tk * dlc - ioma * bd[p];
+                            bd[p] += dlc * at;
+                            T[p] = Tk;
+                            // alpha clamped at alpha_max has no gradient through the power.
+                            const float dP = alpha < a.alpha_max ? dA * alpha : 0.f;
+                            const float dPy = dP * dy;
+                            s0[b] += dP;
+                            sy[b] += dPy;
+                            syy[b] += dPy * dy;
                         }
-                        float v[8];
-                        v[0] = gr.x + gr.y;
-                        v[1] = gg.x + gg.y;
-                        v[2] = gbl.x + gbl.y;
                         float v8 = 0.f;
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) {
-                            const float dx = xt[b].dx;
-                            const float t0 = s0[b].x + s0[b].y, t1 = sy[b].x + sy[b].y;
-                            const float tx = t0 * dx;
-                            v[3] = b ? v[3] + t0 : t0;
-                            v[4] = b ? v[4] + tx : tx;
-                            v[5] = b ? v[5] + t1 : t1;
-                            v[6] = b ? fmaf(tx, dx, v[6]) : tx * dx;
-                            v[7] = b ? fmaf(t1, dx, v[7]) : t1 * dx;
-                            v8 += syy[b].x + syy[b].y;
+                            const float dx = xt[b].dx, tx = s0[b] * dx;
+                            v[3] += s0[b];
+                            v[4] += tx;
+                            v[5] += sy[b];
+                            v[6] += tx * dx;
+                            v[7] += sy[b] * dx;
+                            v8 += syy[b];
                         }
                         float s = warp_sum8_transposed(v);
                         float s8 = v8;
