@@ -240,8 +240,14 @@ def run_b200(args, rank, local, world, dist):
                     px = cm["width"] * cm["height"] * 3
                     r.set_target(v, host[off:off + px])
                     off += px
-            tr = trainer.setdefault(id(r), DP.DataParallelTrainer(r, first=0, count=V))
-            return tr.step(ad, lam, window, wait=want_loss)
+            # The library's own NCCL communicator sums the buffer (no torch on the data
+            # path); NCCL's id goes from rank 0 to the others over a TCP socket.
+            if id(r) not in trainer:
+                port = int(os.environ.get("MASTER_PORT", "29500")) + 101 + len(trainer)
+                trainer[id(r)] = DP.NcclDataParallelTrainer(r, rank=rank, world=world,
+                                                            addr=os.environ.get("MASTER_ADDR", "127.0.0.1"),
+                                                            port=port, first=0, count=V)
+            return trainer[id(r)].step(ad, lam, window, wait=want_loss)
         return r.train_step(ad, lam, window, loss=want_loss, host_targets=host)
 
     def sync_all(r):
@@ -660,7 +666,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-densify", action="store_true")
     ap.add_argument("--dp", action="store_true",
-                    help="use the data-parallel step (gradients, NCCL all-reduce, update) even on one GPU")
+                    help="use the data-parallel step (gradients, the library's NCCL all-reduce, update) even on one GPU")
     ap.add_argument("--autotune-cache", default=None,
                     help="file caching the raster variant choice (a profiled run then uses the unprofiled choice)")
     ap.add_argument("--profile-tile", type=int, default=16, choices=(8, 16, 32),

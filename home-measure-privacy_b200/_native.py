@@ -112,6 +112,10 @@ SIGNATURES = {
     "gs_step_apply": (ctypes.c_int, [CTX, ctypes.POINTER(GsAdamConfig), ctypes.POINTER(c_float),
                                      ctypes.POINTER(c_int32)]),
     "gs_get_stream": (ctypes.c_int, [CTX, ctypes.POINTER(VP)]),
+    "gs_dp_unique_id": (ctypes.c_int, [VP, c_int32]),
+    "gs_dp_init": (ctypes.c_int, [CTX, VP, c_int32, c_int32, c_int32]),
+    "gs_dp_allreduce": (ctypes.c_int, [CTX]),
+    "gs_dp_finalize": (ctypes.c_int, [CTX]),
     "gs_get_blend_count": (ctypes.c_int, [CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "gs_neighbour_sizes": (ctypes.c_int, [CTX, VP, c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, VP]),
     "gs_init_from_points": (ctypes.c_int, [CTX, VP, VP, c_int32, c_float]),

@@ -124,6 +124,8 @@ struct GsContext {
     // then GS_GRAD_TAIL_FLOATS (loss sum, overflow, views)
     DevBuf params, grads, mom1, mom2;
     bool grads_pending = false;         // gs_step_gradients queued, gs_step_apply not yet
+    void* dp_comm = nullptr;            // NCCL communicator of gs_dp_init (data parallel)
+    int dp_rank = 0, dp_world = 1;
     DevBuf stats;                       // densification statistics [2][n_pad]: norm sums, view counts
     bool stats_on = false;              // training steps accumulate them
     bool stats_active = false;          // set while a training step's kernels are enqueued
@@ -933,6 +935,7 @@ const char* gs_status_string(int status) {
         case GS_ERR_NO_DEVICE: return "no CUDA device";
         case GS_ERR_STATE: return "call out of order";
         case GS_ERR_NONFINITE: return "non-finite value";
+        case GS_ERR_COMM: return "data-parallel exchange failed";
         default: return "unknown status";
     }
 }
@@ -1024,6 +1027,8 @@ int gs_destroy(GsContext* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
+    dp_comm_destroy(c->dp_comm);
+    c->dp_comm = nullptr;
     DevBuf* bufs[] = {&c->params, &c->grads, &c->mom1, &c->mom2, &c->views_d, &c->target_u8, &c->target_f32,
                       &c->image, &c->t_final, &c->last, &c->dl, &c->ranges, &c->tile_order, &c->geo0, &c->geo1,
                       &c->rgb, &c->erec, &c->pcount, &c->pkeys, &c->pvals, &c->pkeys_alt, &c->pvals_alt, &c->sg8, &c->sg1,
@@ -1701,6 +1706,56 @@ int gs_get_stream(GsContext* c, void** stream_out) {
     CTX_CHECK(c);
     if (!stream_out) return fail(GS_ERR_INVALID_ARG, "stream_out is null");
     *stream_out = (void*)c->stream;
+    return GS_OK;
+}
+
+int gs_dp_unique_id(void* id_out, int32_t bytes) {
+    GS_TRACE("gs_dp_unique_id");
+    if (!id_out || bytes < dp_unique_id_bytes())
+        return fail(GS_ERR_INVALID_ARG, "id buffer needs %d bytes", dp_unique_id_bytes());
+    char err[256];
+    if (!dp_unique_id(id_out, err, sizeof err)) return fail(GS_ERR_COMM, "%s", err);
+    return GS_OK;
+}
+
+int gs_dp_init(GsContext* c, const void* id, int32_t bytes, int32_t rank, int32_t world) {
+    GS_TRACE("gs_dp_init");
+    CTX_CHECK(c);
+    if (!id || bytes < dp_unique_id_bytes())
+        return fail(GS_ERR_INVALID_ARG, "id needs %d bytes", dp_unique_id_bytes());
+    if (world < 1 || rank < 0 || rank >= world) return fail(GS_ERR_INVALID_ARG, "rank %d of %d", rank, world);
+    if (c->dp_comm) return fail(GS_ERR_STATE, "data parallel already initialised");
+    char err[256];
+    void* comm = dp_comm_create(id, rank, world, err, sizeof err);
+    if (!comm) return fail(GS_ERR_COMM, "%s", err);
+    c->dp_comm = comm;
+    c->dp_rank = rank;
+    c->dp_world = world;
+    return GS_OK;
+}
+
+int gs_dp_allreduce(GsContext* c) {
+    GS_TRACE("gs_dp_allreduce");
+    CTX_CHECK(c);
+    if (!c->dp_comm) return fail(GS_ERR_STATE, "gs_dp_init first");
+    if (!c->grads_pending) return fail(GS_ERR_STATE, "gs_step_gradients first");
+    char err[256];
+    if (!dp_allreduce_sum(c->dp_comm, c->grads.as<float>(), grad_buffer_floats(c), c->stream, err, sizeof err))
+        return fail(GS_ERR_COMM, "%s", err);
+    CK(cudaGetLastError());
+    return GS_OK;
+}
+
+int gs_dp_finalize(GsContext* c) {
+    GS_TRACE("gs_dp_finalize");
+    CTX_CHECK(c);
+    if (c->dp_comm) {
+        CK(cudaStreamSynchronize(c->stream));
+        dp_comm_destroy(c->dp_comm);
+        c->dp_comm = nullptr;
+    }
+    c->dp_rank = 0;
+    c->dp_world = 1;
     return GS_OK;
 }
 

@@ -163,6 +163,13 @@ void launch_raster_bwd(const RasterArgs& a, int tile, int wt, int batch, int ppt
                        cudaStream_t s);
 int raster_max_ctas_per_sm(int tile, int wt, int batch, int ppt, bool backward);
 
+// ---- data-parallel exchange (NCCL, loaded at run time) --------------------------------
+int dp_unique_id_bytes();
+bool dp_unique_id(void* out, char* err, size_t n);
+void* dp_comm_create(const void* id, int rank, int world, char* err, size_t n);
+bool dp_allreduce_sum(void* comm, float* buf, size_t count, cudaStream_t s, char* err, size_t n);
+void dp_comm_destroy(void* comm);
+
 // Blends (pixel, splat evaluations) of the last forward, added to *out.
 void launch_blend_count(const ViewDesc* views, int view_first, int num_views, int max_pixels, const uint2* ranges,
                         const uint32_t* last, unsigned long long* out, cudaStream_t s);

@@ -39,6 +39,7 @@ extern "C" {
 #define GS_ERR_NO_DEVICE   -4   /* no CUDA device visible                          */
 #define GS_ERR_STATE       -5   /* call out of order (no scene / no views / ...)   */
 #define GS_ERR_NONFINITE   -6   /* a non-finite loss or parameter was detected     */
+#define GS_ERR_COMM        -7   /* the data-parallel exchange (NCCL) failed        */
 
 /* ---- plain data types ---------------------------------------------------------- */
 
@@ -274,6 +275,19 @@ GS_API int gs_step_apply(GsContext* ctx, const GsAdamConfig* adam, float* loss_o
 /* The context's CUDA stream (a cudaStream_t), for work the caller orders with the
  * library's: a collective over gs_step_gradients' buffer, a copy, an event. */
 GS_API int gs_get_stream(GsContext* ctx, void** stream_out);
+
+/* Data parallel without a framework: NCCL (opened at run time; a libnccl already loaded
+ * in the process is shared) sums the gradient buffer across replicas on the context's
+ * stream.  Rank 0 makes an id (gs_dp_unique_id, 128 bytes), every rank receives it by
+ * any means (a socket, a file) and calls gs_dp_init with its rank; then each step is
+ * gs_step_gradients (own views), gs_dp_allreduce, gs_step_apply.  gs_dp_init waits for
+ * all `world` ranks.  GS_ERR_COMM when NCCL is missing or fails.  Replaces the single
+ * device of the reference (trainer/gpu.js:915-933: one view per step on one WebGPU
+ * device); there is no reference interface for it. */
+GS_API int gs_dp_unique_id(void* id_out, int32_t bytes);
+GS_API int gs_dp_init(GsContext* ctx, const void* id, int32_t bytes, int32_t rank, int32_t world);
+GS_API int gs_dp_allreduce(GsContext* ctx);
+GS_API int gs_dp_finalize(GsContext* ctx);
 
 /* ---- Initialisation from a point cloud ----------------------------------------------
  * neighbourSizes (trainer/neighbours.js:13-53): per point, the root mean square distance
