@@ -959,8 +959,8 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
     else gs_config_default(&cfg);
     if (cfg.sh_degree < 0 || cfg.sh_degree > 3) return fail(GS_ERR_INVALID_ARG, "sh_degree must be 0..3");
     if (cfg.rect_mode < 0 || cfg.rect_mode > 1) return fail(GS_ERR_INVALID_ARG, "rect_mode must be 0 or 1");
-    if (cfg.raster_batch != 64 && cfg.raster_batch != 128 && cfg.raster_batch != 256)
-        return fail(GS_ERR_INVALID_ARG, "raster_batch must be 64, 128 or 256");
+    if (cfg.raster_batch != 32 && cfg.raster_batch != 64 && cfg.raster_batch != 128 && cfg.raster_batch != 256)
+        return fail(GS_ERR_INVALID_ARG, "raster_batch must be 32, 64, 128 or 256");
     if (cfg.tile_size == 0) cfg.tile_size = GS_TILE;
     if (cfg.raster_ppt == 0) cfg.raster_ppt = cfg.tile_size == 8 ? 2 : 4;
     if (cfg.tile_size != 8 && cfg.tile_size != 16 && cfg.tile_size != 32)
@@ -2393,7 +2393,7 @@ int gs_autotune(GsContext* c, const char* cache_path) {
         drop_graphs(c);
         return GS_OK;
     };
-    auto ok_batch = [](int b) { return b == 64 || b == 128 || b == 256; };
+    auto ok_batch = [](int b) { return b == 32 || b == 64 || b == 128 || b == 256; };
     if (cache_path) {
         FILE* f = fopen(cache_path, "r");
         if (f) {
@@ -2415,7 +2415,7 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     }
     const int saved_batched = c->cfg.batched;
     DevStatus* st = c->status.as<DevStatus>();
-    const int batches[3] = {64, 128, 256};
+    const int batches[4] = {32, 64, 128, 256};
     const int tiles[3] = {16, 8, 32};
     const GsLossConfig lc{0.2f, 1};
     cudaEvent_t e0 = c->user_events[62], e1 = c->user_events[63];
@@ -2445,7 +2445,7 @@ int gs_autotune(GsContext* c, const char* cache_path) {
         int bf = 0, pf = 0, wf = 0, bb = 0, pb = 0, wb = 0;
         RasterArgs r = raster_args(c, 0, c->V);
         if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
-        for (int bi = 0; bi < 3; bi++)
+        for (int bi = 0; bi < 4; bi++)
             for (int vi = 0; vi < 6; vi++) {
                 const int ppt = 2 << (vi % 3), wt = vi < 3 ? tile : tile / 2;
                 if (!raster_variant_ok(tile, wt, ppt)) continue;

@@ -132,26 +132,33 @@ __global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const T
     const int tid = threadIdx.x;
     __syncthreads();  // byte table
     if (use_ssim) {
-        // All of a thread's region loads are issued before the first shared-memory store.
-        constexpr int NL = (D::RH * D::RW + LB_THREADS - 1) / LB_THREADS;
-        float xl[NL], yl[NL];
+        // A thread owns one region column and every NRG-th row of it: one address step
+        // per row, no index division.  All of its loads are issued before the first
+        // shared-memory store.
+        constexpr int NRG = LB_THREADS / D::RW;            // row groups
+        constexpr int NL = (D::RH + NRG - 1) / NRG;        // rows per thread
+        const int rx = tid % D::RW, rg = tid / D::RW;
+        if (rg < NRG) {
+            const int gx = bx0 - 2 * R + rx;
+            const bool col_ok = gx >= 0 && gx < W;
+            const int gy0 = by0 - 2 * R + rg;
+            const long long q0 = ((long long)poff + (long long)gy0 * W + gx) * 3 + c;
+            const long long step = (long long)NRG * W * 3;
+            float xl[NL], yl[NL];
 #pragma unroll
-        for (int i = 0; i < NL; i++) {
-            const int idx = tid + i * LB_THREADS;
-            const int ry = idx / D::RW, rx = idx % D::RW;
-            const int gx = bx0 - 2 * R + rx, gy = by0 - 2 * R + ry;
-            xl[i] = 0.f;
-            yl[i] = 0.f;
-            if (idx < D::RH * D::RW && gx >= 0 && gy >= 0 && gx < W && gy < H) {
-                const size_t q = (poff + (size_t)gy * W + gx) * 3 + c;
-                xl[i] = a.image[q];
-                yl[i] = load_target<TT>(target, q, s_lut);
+            for (int i = 0; i < NL; i++) {
+                const int gy = gy0 + i * NRG;
+                xl[i] = 0.f;
+                yl[i] = 0.f;
+                if (col_ok && rg + i * NRG < D::RH && gy >= 0 && gy < H) {
+                    const size_t q = (size_t)(q0 + i * step);
+                    xl[i] = a.image[q];
+                    yl[i] = load_target<TT>(target, q, s_lut);
+                }
             }
-        }
 #pragma unroll
-        for (int i = 0; i < NL; i++) {
-            const int idx = tid + i * LB_THREADS;
-            if (idx < D::RH * D::RW) XY[idx] = make_float2(xl[i], yl[i]);
+            for (int i = 0; i < NL; i++)
+                if (rg + i * NRG < D::RH) XY[(rg + i * NRG) * D::RW + rx] = make_float2(xl[i], yl[i]);
         }
         __syncthreads();
         // P1: horizontal moments (x, y, x^2 + y^2, xy) at the centre columns of a strip.

@@ -175,6 +175,9 @@ constexpr float LOG2E = 1.4426950408889634f;
 constexpr float ALPHA_Q_BAND = 1e-4f;  // |q - log2(alpha_min)| below this: reference formula
 constexpr float KAPPA_CULL_MAX = 256.f; // elongation above which culling uses the bounding square only
 constexpr float KAPPA_EXACT = 32.f;     // elongation above which every pixel uses the reference expression
+#ifndef BWD_GROUPS
+#define BWD_GROUPS 2  // backward: 8 x 4 pixel groups evaluated together (1, 2 or 4)
+#endif
 
 // Elongation of a splat's conic, kappa = A C / (A C - B^2) >= 1: the quadratic form's
 // terms reach kappa times its value, so rounding errors in the exponent (and in the
@@ -504,6 +507,7 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
     __shared__ uint32_t s_pair[2][BATCH];
     __shared__ int s_item;
     __shared__ unsigned int s_end;
+    __shared__ uint32_t s_gmax[L::NT / 32][PPT];  // per warp and group: the largest last
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const float log_amin = __logf(a.alpha_min);
     const float qthr = __log2f(a.alpha_min);
@@ -523,14 +527,16 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
         const TileInfo<PPT> ti = tile_info<TILE, WT, PPT>(a, item);
         const uint2 rg = a.ranges[ti.g];
         const uint32_t start = rg.x;
-        float pxf[L::WX], pyf[PPT], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
-        uint32_t mylast[PPT], gmax[PPT];
+        // Pixel rows: p's centre is pyf0 + 4 (p % WY), exact in float (recomputed where
+        // used rather than held in registers).
+        const float pyf0 = (float)ti.y[0] + 0.5f;
+        float pxf[L::WX], T[PPT], dlr[PPT], dlg[PPT], dlb[PPT], bd[PPT];
+        uint32_t mylast[PPT];
 #pragma unroll
         for (int b = 0; b < L::WX; b++) pxf[b] = (float)ti.x[b * L::WY] + 0.5f;  // the warp's x bands
         unsigned int wmax = start;
 #pragma unroll
         for (int p = 0; p < PPT; p++) {
-            pyf[p] = (float)ti.y[p] + 0.5f;
             T[p] = 0.f;
             dlr[p] = dlg[p] = dlb[p] = 0.f;
             bd[p] = 0.f;  // dL . (colour of the splats behind), "behind"
@@ -547,7 +553,7 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
             unsigned int gm = mylast[p];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) gm = max(gm, __shfl_xor_sync(FULL_MASK, gm, o));
-            gmax[p] = gm;
+            if (lane == 0) s_gmax[w][p] = gm;
             wmax = max(wmax, gm);
         }
         if (threadIdx.x == 0) s_end = start;
@@ -586,7 +592,7 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                         const uint32_t kl = bend - 1 - (uint32_t)jl;
                         uint32_t act = 0u;  // groups with a pixel whose last is past this entry
 #pragma unroll
-                        for (int p = 0; p < PPT; p++) act |= kl < gmax[p] ? (1u << p) : 0u;
+                        for (int p = 0; p < PPT; p++) act |= kl < s_gmax[w][p] ? (1u << p) : 0u;
                         if (act) gm = group_mask<WT, PPT>(g0s[jl], g1s[jl], ti.cx0, ti.cy0, w) & act;
                     }
                     uint32_t live = __ballot_sync(FULL_MASK, gm != 0u);
@@ -615,14 +621,22 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                         float s0[L::WX], sy[L::WX], syy[L::WX];
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) s0[b] = sy[b] = syy[b] = 0.f;
+                        // Groups go in blocks of BWD_GROUPS (a block is evaluated when any
+                        // of its groups is live; the others' own tests give alpha = 0), so
+                        // the compiler can interleave the dependency chains of a block's
+                        // pixels.
+                        constexpr int GB = BWD_GROUPS < PPT ? BWD_GROUPS : PPT;
 #pragma unroll
-                        for (int p = 0; p < PPT; p++) {
-                            if (!(m & (1u << p))) continue;
+                        for (int gi = 0; gi < PPT / GB; gi++) {
+                            if (!((m >> (GB * gi)) & ((1u << GB) - 1u))) continue;
+#pragma unroll
+                            for (int h = 0; h < GB; h++) {
+                            const int p = GB * gi + h;
                             // Branch-free per lane: alpha = 0 adds zeros and leaves T
                             // (T / 1) and dL.behind as they are.
                             const int b = p / L::WY;
                             const XTerm& x = xt[b];
-                            const float dy = pyf[p] - g0.y;
+                            const float dy = (pyf0 + (float)(4 * (p % L::WY))) - g0.y;
                             const float e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, x.b0.x), x.a0.x);
                             bool hit;
                             const float alpha = alpha_pix(e, x.dx, dy, x.inb && k < mylast[p], g0, g1, a.alpha_max,
@@ -645,6 +659,7 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                             s0[b] += dP;
                             sy[b] += dPy;
                             syy[b] += dPy * dy;
+                            }
                         }
                         float v8 = 0.f;
 #pragma unroll
@@ -700,6 +715,7 @@ static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
 #define RASTER_BATCHES(FN, T, W, batch, P, ...)                 \
     do {                                                        \
         switch (batch) {                                        \
+            case 32: FN<T, W, 32, P>(__VA_ARGS__); break;       \
             case 64: FN<T, W, 64, P>(__VA_ARGS__); break;       \
             case 128: FN<T, W, 128, P>(__VA_ARGS__); break;     \
             default: FN<T, W, 256, P>(__VA_ARGS__); break;      \

@@ -70,7 +70,7 @@ typedef struct GsConfig {
     int32_t device;        /* CUDA device ordinal                                     */
     int32_t autotune;      /* 1 = run gs_autotune before the first training step over
                               all views                                                 */
-    int32_t raster_batch;  /* Gaussians per shared-memory batch: 64, 128 or 256        */
+    int32_t raster_batch;  /* Gaussians per shared-memory batch: 32, 64, 128 or 256    */
     int32_t lpt_order;     /* 1 = persistent raster takes heavy tiles first           */
     int32_t instance_capacity; /* initial key-instance capacity; 0 = measured by a first
                               forward.  A step that overflows skips its update, the

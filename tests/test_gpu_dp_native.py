@@ -1,8 +1,8 @@
 """The library's own NCCL communicator on one GPU (world of one rank, no torch in the
 data path): gs_step_gradients, gs_dp_allreduce, gs_step_apply over all views equals
 gs_train_step over all views (a sum over one rank is the buffer itself: the same
-kernels in the same order, so the same results up to the last bits), and the call order
-is checked (allreduce before init or before gradients is refused)."""
+kernels, so the same results up to the order of the backward's float atomics), and the
+call order is checked (allreduce before init or before gradients is refused)."""
 import importlib
 
 import numpy as np
@@ -49,5 +49,5 @@ def test_native_nccl_one_rank_equals_whole_step(hmp):
         out = r.get_gaussians()
         assert r.step_count() == 3
         tr.close()
-    np.testing.assert_allclose(losses, ref_losses, rtol=1e-6)
-    assert np.abs(out - ref).max() <= 1e-6
+    np.testing.assert_allclose(losses, ref_losses, rtol=1e-5)
+    assert np.abs(out - ref).max() <= 1e-4

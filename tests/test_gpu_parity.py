@@ -188,7 +188,7 @@ def test_raster_variants_agree(hmp, ppt):
             return img, r.backward()
 
     ref_img, ref_g = run(256, 2)
-    for batch in (64, 128, 256):
+    for batch in (32, 64, 128, 256):
         img, g = run(batch, ppt)
         assert np.array_equal(img, ref_img), batch
         assert rel_err(g, ref_g) < 1e-5, batch
@@ -482,7 +482,7 @@ def test_tile_sizes_agree(hmp):
     ref_img, ref_g = run(16, 2, 256)
     for tile, wt, ppts in ((8, 0, (2,)), (16, 0, (4, 8)), (32, 0, (2, 4, 8)), (32, 16, (2, 4, 8))):
         for ppt in ppts:
-            for batch in (64, 256):
+            for batch in (32, 256):
                 img, g = run(tile, ppt, batch, wt)
                 assert np.array_equal(img, ref_img), (tile, wt, ppt, batch)
                 assert rel_err(g, ref_g) < 1e-5, (tile, wt, ppt, batch)
