@@ -178,6 +178,9 @@ constexpr float KAPPA_EXACT = 32.f;     // elongation above which every pixel us
 #ifndef BWD_GROUPS
 #define BWD_GROUPS 2  // backward: 8 x 4 pixel groups evaluated together (1, 2 or 4)
 #endif
+#ifndef FWD_GROUPS
+#define FWD_GROUPS 2  // forward: the same, in pixel pairs (2 or 4)
+#endif
 
 // Elongation of a splat's conic, kappa = A C / (A C - B^2) >= 1: the quadratic form's
 // terms reach kappa times its value, so rounding errors in the exponent (and in the
@@ -415,9 +418,15 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, fwd_min_ctas(WT, PPT)) raste
                     XTerm xt[L::WX];
 #pragma unroll
                     for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
+                    // Groups go in blocks of FWD_GROUPS (pixel pairs of a block share a
+                    // basic block, so their dependency chains interleave).
+                    constexpr int GB = FWD_GROUPS < PPT ? FWD_GROUPS : PPT;
 #pragma unroll
-                    for (int i = 0; i < NP; i++) {
-                        if (!((m >> (2 * i)) & 3u)) continue;
+                    for (int gi = 0; gi < PPT / GB; gi++) {
+                        if (!((m >> (GB * gi)) & ((1u << GB) - 1u))) continue;
+#pragma unroll
+                        for (int hh = 0; hh < GB / 2; hh++) {
+                        const int i = gi * (GB / 2) + hh;
                         // Branch-free per lane: alpha = 0 leaves colour, T and last as they are
                         // (also for a pair member whose group the mask left out).
                         const XTerm& x = xt[(2 * i) / L::WY];
@@ -436,6 +445,7 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, fwd_min_ctas(WT, PPT)) raste
                         T[i] = mul2(T[i], fma2(alpha, f2(-1.0f), f2(1.0f)));  // T (1 - alpha)
                         last[2 * i] = h0 ? pos : last[2 * i];
                         last[2 * i + 1] = h1 ? pos : last[2 * i + 1];
+                        }
                     }
                 }
 #pragma unroll
