@@ -36,40 +36,64 @@ __device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, flo
     }
 }
 
+#ifndef ADAM_GROUPS
+#define ADAM_GROUPS 1  // groups of 4 Gaussians per thread (1 or 2)
+#endif
+
 __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
     // Skip the update when this step's instances overflowed -- on every replica at once
     // when the gradients were reduced across replicas (the tail's overflow count).
     if (a.skip ? (*a.skip > 0.f) : (a.status->overflow != 0u || a.status->sort_timeout != 0u)) return;
     const int groups = a.n_pad / 4;
     const int units_per_group = a.planes - 3;  // planes other than 6..9, plus one rotation unit
+    // A thread takes ADAM_GROUPS groups of 4 Gaussians of one unit, gper apart (so a
+    // warp's loads stay contiguous), loading all of them before it stores any.
+    const int gper = (groups + ADAM_GROUPS - 1) / ADAM_GROUPS;
     const long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= (long long)groups * units_per_group) return;
-    const int unit = (int)(u / groups), grp = (int)(u % groups);
+    if (u >= (long long)gper * units_per_group) return;
+    const int unit = (int)(u / gper), grp0 = (int)(u % gper);
     const int t = a.status->step_t + 1;
     const float ibc1 = 1.0f / (1.0f - powf(a.beta1, (float)t));
     const float ibc2 = 1.0f / (1.0f - powf(a.beta2, (float)t));
     const float omb1 = 1.0f - a.beta1, omb2 = 1.0f - a.beta2;
     const size_t np = (size_t)a.n_pad;
-    const size_t col = (size_t)grp * 4;
     if (unit != 6) {
         const int j = unit < 6 ? unit : unit + 3;  // skip planes 7..9 (unit 6 = rotation)
-        const size_t off = (size_t)j * np + col;
-        float4 p = *reinterpret_cast<const float4*>(a.params + off);
-        const float4 g = *reinterpret_cast<const float4*>(a.grads + off);
-        float4 m = *reinterpret_cast<const float4*>(a.m + off);
-        float4 v = *reinterpret_cast<const float4*>(a.v + off);
-        adam4(p, g, m, v, a.lr[j], a.beta1, a.beta2, omb1, omb2, ibc1, ibc2, a.eps);
-        if (j >= 11 && j <= 13) {  // colour (SH DC) clamped to [0, 1]
-            p.x = fminf(fmaxf(p.x, 0.f), 1.f);
-            p.y = fminf(fmaxf(p.y, 0.f), 1.f);
-            p.z = fminf(fmaxf(p.z, 0.f), 1.f);
-            p.w = fminf(fmaxf(p.w, 0.f), 1.f);
+        float4 p[ADAM_GROUPS], g[ADAM_GROUPS], m[ADAM_GROUPS], v[ADAM_GROUPS];
+        size_t off[ADAM_GROUPS];
+        bool ok[ADAM_GROUPS];
+#pragma unroll
+        for (int r = 0; r < ADAM_GROUPS; r++) {
+            const int grp = grp0 + r * gper;
+            ok[r] = grp < groups;
+            off[r] = (size_t)j * np + (size_t)grp * 4;
+            if (ok[r]) {
+                p[r] = *reinterpret_cast<const float4*>(a.params + off[r]);
+                g[r] = *reinterpret_cast<const float4*>(a.grads + off[r]);
+                m[r] = *reinterpret_cast<const float4*>(a.m + off[r]);
+                v[r] = *reinterpret_cast<const float4*>(a.v + off[r]);
+            }
         }
-        *reinterpret_cast<float4*>(a.params + off) = p;
-        *reinterpret_cast<float4*>(a.m + off) = m;
-        *reinterpret_cast<float4*>(a.v + off) = v;
+#pragma unroll
+        for (int r = 0; r < ADAM_GROUPS; r++) {
+            if (!ok[r]) continue;
+            adam4(p[r], g[r], m[r], v[r], a.lr[j], a.beta1, a.beta2, omb1, omb2, ibc1, ibc2, a.eps);
+            if (j >= 11 && j <= 13) {  // colour (SH DC) clamped to [0, 1]
+                p[r].x = fminf(fmaxf(p[r].x, 0.f), 1.f);
+                p[r].y = fminf(fmaxf(p[r].y, 0.f), 1.f);
+                p[r].z = fminf(fmaxf(p[r].z, 0.f), 1.f);
+                p[r].w = fminf(fmaxf(p[r].w, 0.f), 1.f);
+            }
+            *reinterpret_cast<float4*>(a.params + off[r]) = p[r];
+            *reinterpret_cast<float4*>(a.m + off[r]) = m[r];
+            *reinterpret_cast<float4*>(a.v + off[r]) = v[r];
+        }
         return;
     }
+    for (int r = 0; r < ADAM_GROUPS; r++) {
+    const int grp = grp0 + r * gper;
+    if (grp >= groups) break;
+    const size_t col = (size_t)grp * 4;
     // Rotation planes 6..9: update, then renormalise the quaternions.
     float4 q[4];
 #pragma unroll
@@ -100,10 +124,11 @@ __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) *reinterpret_cast<float4*>(a.params + (size_t)(6 + k) * np + col) = q[k];
+    }
 }
 
 void launch_adam(const AdamArgs& a, cudaStream_t s) {
-    const long long units = (long long)(a.n_pad / 4) * (a.planes - 3);
+    const long long units = (long long)((a.n_pad / 4 + ADAM_GROUPS - 1) / ADAM_GROUPS) * (a.planes - 3);
     const int threads = 256;
     const long long blocks = (units + threads - 1) / threads;
     if (blocks > 0) adam_kernel<<<(unsigned)blocks, threads, 0, s>>>(a);
