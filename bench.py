@@ -669,7 +669,7 @@ def main():
                     help="use the data-parallel step (gradients, the library's NCCL all-reduce, update) even on one GPU")
     ap.add_argument("--autotune-cache", default=None,
                     help="file caching the raster variant choice (a profiled run then uses the unprofiled choice)")
-    ap.add_argument("--profile-tile", type=int, default=16, choices=(8, 16, 32),
+    ap.add_argument("--profile-tile", type=int, default=16, choices=(8, 16, 32, 64),
                     help="--profile-case: tile edge in pixels")
     ap.add_argument("--profile-wt", type=int, default=0, choices=(0, 8, 16, 32),
                     help="--profile-case: raster work tile edge (0 = the tile edge)")

@@ -963,13 +963,14 @@ int gs_create(const GsConfig* cfg_in, GsContext** out) {
         return fail(GS_ERR_INVALID_ARG, "raster_batch must be 32, 64, 128 or 256");
     if (cfg.tile_size == 0) cfg.tile_size = GS_TILE;
     if (cfg.raster_ppt == 0) cfg.raster_ppt = cfg.tile_size == 8 ? 2 : 4;
-    if (cfg.tile_size != 8 && cfg.tile_size != 16 && cfg.tile_size != 32)
-        return fail(GS_ERR_INVALID_ARG, "tile_size must be 8, 16 or 32");
-    if (cfg.raster_work_tile == 0) cfg.raster_work_tile = cfg.tile_size;
+    if (cfg.tile_size != 8 && cfg.tile_size != 16 && cfg.tile_size != 32 && cfg.tile_size != 64)
+        return fail(GS_ERR_INVALID_ARG, "tile_size must be 8, 16, 32 or 64");
+    if (cfg.raster_work_tile == 0) cfg.raster_work_tile = cfg.tile_size == 64 ? 16 : cfg.tile_size;
     if (!raster_variant_ok(cfg.tile_size, cfg.raster_work_tile, cfg.raster_ppt))
         return fail(GS_ERR_INVALID_ARG,
                     "no raster variant with %d pixels per thread and %d-pixel work tiles for %d-pixel tiles "
-                    "(8: 2 px, work tile 8; 16: 2, 4 or 8 px, work tile 16; 32: 2, 4 or 8 px, work tile 32 or 16)",
+                    "(8: 2 px, work tile 8; 16: 2, 4 or 8 px, work tile 16; 32: 2, 4 or 8 px, work tile 32 or 16; "
+                    "64: 2, 4 or 8 px, work tile 16)",
                     cfg.raster_ppt, cfg.raster_work_tile, cfg.tile_size);
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
@@ -2348,8 +2349,8 @@ static int set_tile(GsContext* c, int tile) {
     // Keep raster variants that exist for the new tile size.
     for (int* v : {&c->ppt_fwd, &c->ppt_bwd})
         if (tile == 8) *v = 2;
-    if (!raster_variant_ok(tile, c->wt_fwd, c->ppt_fwd)) c->wt_fwd = tile;
-    if (!raster_variant_ok(tile, c->wt_bwd, c->ppt_bwd)) c->wt_bwd = tile;
+    if (!raster_variant_ok(tile, c->wt_fwd, c->ppt_fwd)) c->wt_fwd = tile == 64 ? 16 : tile;
+    if (!raster_variant_ok(tile, c->wt_bwd, c->ppt_bwd)) c->wt_bwd = tile == 64 ? 16 : tile;
     CKI(layout(c));
     // The instance buffers are sized again for this tile size: the sort and emission
     // grids follow their capacity, which another tile size may have grown.
@@ -2364,7 +2365,7 @@ static int set_tile(GsContext* c, int tile) {
     return GS_OK;
 }
 
-// Tuning: for each tile size (16, 8, 32) the persistent forward and backward raster
+// Tuning: for each tile size (16, 8, 32, 64) the persistent forward and backward raster
 // kernels are timed for every (work tile, shared-memory batch, pixels per thread)
 // variant that exists for it, on all training views after one forward and loss, keeping
 // the fastest of each; then the tile size's whole forward + loss + backward (projection,
@@ -2416,13 +2417,13 @@ int gs_autotune(GsContext* c, const char* cache_path) {
     const int saved_batched = c->cfg.batched;
     DevStatus* st = c->status.as<DevStatus>();
     const int batches[4] = {32, 64, 128, 256};
-    const int tiles[3] = {16, 8, 32};
+    const int tiles[4] = {16, 8, 32, 64};
     const GsLossConfig lc{0.2f, 1};
     cudaEvent_t e0 = c->user_events[62], e1 = c->user_events[63];
     float best_total = 1e30f;
     int best[7] = {c->tile, c->batch_fwd, c->ppt_fwd, c->wt_fwd, c->batch_bwd, c->ppt_bwd, c->wt_bwd};
     int64_t inst16 = -1;  // key instances with 16-pixel tiles (measured first)
-    for (int ti = 0; ti < 3; ti++) {
+    for (int ti = 0; ti < 4; ti++) {
         const int tile = tiles[ti];
         if (inst16 >= 0) {
             // A tile size whose instance buffers would not fit is skipped: instances scale
@@ -2447,7 +2448,7 @@ int gs_autotune(GsContext* c, const char* cache_path) {
         if (c->cfg.lpt_order) r.tile_order = c->tile_order.as<uint32_t>();
         for (int bi = 0; bi < 4; bi++)
             for (int vi = 0; vi < 6; vi++) {
-                const int ppt = 2 << (vi % 3), wt = vi < 3 ? tile : tile / 2;
+                const int ppt = 2 << (vi % 3), wt = tile == 64 ? (vi < 3 ? 16 : 0) : (vi < 3 ? tile : tile / 2);
                 if (!raster_variant_ok(tile, wt, ppt)) continue;
                 for (int backward = 0; backward < 2; backward++) {
                     const int ctas =

@@ -741,7 +741,8 @@ static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
 
 // The (list tile, work tile, pixels per thread) variants that exist: 8 x 8 tiles with
 // 2 pixels per thread; 16 x 16 tiles with 2, 4 or 8; 32 x 32 tiles with work tiles of
-// 32 x 32 or 16 x 16 and 2, 4 or 8 (raster_variant_ok).
+// 32 x 32 or 16 x 16 and 2, 4 or 8; 64 x 64 tiles with 16 x 16 work tiles and 2, 4 or 8
+// (raster_variant_ok).
 #define RASTER_SWITCH(FN, tile, wt, batch, ppt, ...)                                       \
     do {                                                                                   \
         if ((tile) == 8) {                                                                 \
@@ -749,6 +750,8 @@ static void bwd_launch(const RasterArgs& a, int ctas, cudaStream_t s) {
         } else if ((tile) == 32) {                                                         \
             if ((wt) == 16) RASTER_PPTS(FN, 32, 16, batch, ppt, __VA_ARGS__);              \
             else RASTER_PPTS(FN, 32, 32, batch, ppt, __VA_ARGS__);                         \
+        } else if ((tile) == 64) {                                                         \
+            RASTER_PPTS(FN, 64, 16, batch, ppt, __VA_ARGS__);                              \
         } else {                                                                           \
             RASTER_PPTS(FN, 16, 16, batch, ppt, __VA_ARGS__);                              \
         }                                                                                  \
@@ -758,6 +761,7 @@ bool raster_variant_ok(int tile, int wt, int ppt) {
     if (tile == 8) return wt == 8 && ppt == 2;
     if (tile == 16) return wt == 16 && (ppt == 2 || ppt == 4 || ppt == 8);
     if (tile == 32) return (wt == 32 || wt == 16) && (ppt == 2 || ppt == 4 || ppt == 8);
+    if (tile == 64) return wt == 16 && (ppt == 2 || ppt == 4 || ppt == 8);
     return false;
 }
 

@@ -83,11 +83,12 @@ typedef struct GsConfig {
                               and gradients, fewer entries; 0 = the reference's
                               rectangle lists (rect_mode), whose keys match BIN + SORT  */
     int32_t tile_size;     /* tile edge in pixels: 16 (default, the reference's,
-                              trainer/gpu.js:118), 8 or 32; 0 = 16.  Images are the same
-                              for every size; gs_autotune may change it                 */
+                              trainer/gpu.js:118), 8, 32 or 64; 0 = 16.  Images are the
+                              same for every size; gs_autotune may change it            */
     int32_t raster_work_tile; /* pixels a raster CTA covers: the whole tile (0 or the
-                              tile edge) or, for 32-pixel tiles, 16 (each 16 x 16
-                              quarter a CTA of its own, walking the tile's list)        */
+                              tile edge) or, for 32- and 64-pixel tiles, 16 (each 16 x
+                              16 part a CTA of its own, walking the tile's list); 64-
+                              pixel tiles take 16 only (0 = 16)                        */
 } GsConfig;
 
 /* Adam settings.  The per-group learning rates are the reference's (trainer/gpu.js:846,
@@ -459,11 +460,13 @@ GS_API int gs_get_tile_lists(GsContext* ctx, int32_t view, uint32_t* list_out,
 GS_API int gs_get_splats(GsContext* ctx, int32_t view, float* splats12_out);
 
 /* Tuning (no counterpart in the reference, whose tile size, workgroup size and batch are
- * fixed): for each tile size (16, 8 and 32 pixels) times the raster kernels' candidate
- * variants (splats per shared-memory batch, pixels per thread) on the current views and
- * keeps the fastest forward and backward, then times that tile size's whole forward,
- * loss and backward (no update) and keeps the tile size with the fastest.  Images do not
- * depend on the choice.  The views need targets.  cache_path (optional): a text file
+ * fixed): for each tile size (16, 8, 32 and 64 pixels) times the raster kernels'
+ * candidate variants (splats per shared-memory batch, pixels per thread, work tile) on
+ * the current views and keeps the fastest forward and backward, then times that tile
+ * size's whole forward, loss and backward (no update) and keeps the tile size with the
+ * fastest.  A tile size whose key instances would not fit in half the free device
+ * memory (estimated from the 16-pixel count) is skipped.  Images do not depend on the
+ * choice.  The views need targets.  cache_path (optional): a text file
  * that records the choice per device and workload. */
 GS_API int gs_autotune(GsContext* ctx, const char* cache_path);
 

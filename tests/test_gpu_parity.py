@@ -475,12 +475,12 @@ def test_tile_sizes_agree(hmp):
             img = r.forward(0, 3)
             assert r.stats()["tile_size"] == tile
             v = r.raster_variant()
-            assert v["fwd"][2] == (wt or tile) and v["bwd"][2] == (wt or tile)
+            assert v["fwd"][2] == (wt or tile) and v["bwd"][2] == (wt or tile), v
             r.loss(ssim=0.2, window=1)
             return img, r.backward()
 
     ref_img, ref_g = run(16, 2, 256)
-    for tile, wt, ppts in ((8, 0, (2,)), (16, 0, (4, 8)), (32, 0, (2, 4, 8)), (32, 16, (2, 4, 8))):
+    for tile, wt, ppts in ((8, 0, (2,)), (16, 0, (4, 8)), (32, 0, (2, 4, 8)), (32, 16, (2, 4, 8)), (64, 16, (4, 8))):
         for ppt in ppts:
             for batch in (32, 256):
                 img, g = run(tile, ppt, batch, wt)
