@@ -37,7 +37,7 @@ __device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, flo
 }
 
 #ifndef ADAM_GROUPS
-#define ADAM_GROUPS 1  // groups of 4 Gaussians per thread (1 or 2)
+#define ADAM_GROUPS 2  // groups of 4 Gaussians per thread: 2 keeps twice the loads in flight
 #endif
 
 __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {

@@ -206,9 +206,6 @@ void launch_project_fwd(const ProjectArgs& a, cudaStream_t s) {
 // ---------------------------------------------------------------------------------
 // Backward.
 // ---------------------------------------------------------------------------------
-#ifndef PBWD_PREFETCH
-#define PBWD_PREFETCH 0  // 1: load the next view's screen gradients one view early
-#endif
 template <int DEG>
 __global__ void __launch_bounds__(128, 4) project_bwd_kernel(ProjectBwdArgs a) {
     constexpr int NK = (DEG + 1) * (DEG + 1) - 1;
@@ -260,32 +257,11 @@ __global__ void __launch_bounds__(128, 4) project_bwd_kernel(ProjectBwdArgs a) {
 #pragma unroll
             for (int k = 0; k < 3 * NK; k++) s_sh[k][tid] = __ldg(a.params + (14 + k) * np + i);
         }
-#if PBWD_PREFETCH
-        // The views' screen gradients, the next view's loaded while this one is worked on.
-        size_t pair = (size_t)a.pair_slot_first * np + i;
-        float4 s0n = make_float4(0.f, 0.f, 0.f, 0.f), s1n = s0n;
-        float gCn = 0.f;
-        if (a.num_views > 0) {
-            s0n = a.sg8[pair * 2 + 0];
-            s1n = a.sg8[pair * 2 + 1];
-            gCn = a.sg1[pair];
-        }
-        for (int sidx = 0; sidx < a.num_views; sidx++) {
-            const float4 s0 = s0n, s1 = s1n;
-            const float gC = gCn;
-            if (sidx + 1 < a.num_views) {
-                pair += (size_t)np;
-                s0n = a.sg8[pair * 2 + 0];
-                s1n = a.sg8[pair * 2 + 1];
-                gCn = a.sg1[pair];
-            }
-#else
         for (int sidx = 0; sidx < a.num_views; sidx++) {
             const size_t pair = (size_t)(a.pair_slot_first + sidx) * np + i;
             const float4 s0 = a.sg8[pair * 2 + 0];
             const float4 s1 = a.sg8[pair * 2 + 1];
             const float gC = a.sg1[pair];
-#endif
             if (s0.x == 0.f && s0.y == 0.f && s0.z == 0.f && s0.w == 0.f && s1.x == 0.f && s1.y == 0.f &&
                 s1.z == 0.f && s1.w == 0.f && gC == 0.f)
                 continue;
