@@ -280,7 +280,7 @@ __host__ __device__ __forceinline__ bool splat_reaches_box(float u, float v, flo
     return conic_qmin_box(A, B, C, xl - u, xh - u, yl - v, yh - v) <= thr;
 }
 
-#define GS_SPAN_ROWS 8            // pairs up to this many tile rows get per-row tile spans
+#define GS_SPAN_ROWS 12           // pairs up to this many tile rows get per-row tile spans
 #define GS_PCOUNT_RECT 0x80000000u  // pcount flag: instances are the whole rectangle
 
 // ---------------------------------------------------------------------------------

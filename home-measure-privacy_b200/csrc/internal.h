@@ -8,12 +8,11 @@ namespace gs {
 
 // What the instance emission gathers for one (view, Gaussian) pair, in one 32-byte
 // sector: the global tile of the rectangle's corner (x0, y0), tiles_x | (x1 - x0) << 16
-// | whole-rectangle flag << 31, the instance count, and the per-row tile spans.
+// | whole-rectangle flag << 31, and the per-row tile spans of up to 12 rows.
 struct __align__(32) EmitRec {
     uint32_t first_tile;
     uint32_t geom;
-    uint32_t count;
-    uint32_t pad;
+    uint32_t spans_hi[2];    // rows 8..11, packed as below
     uint4 spans;             // row r < 8: tiles [xs, xe) as bytes (xs | xe << 8) << 16 * (r & 1), x0-relative
 };
 

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
         else
             p.ok = false;
         uint32_t count = (p.ok && x1 > x0 && y1 > y0) ? (uint32_t)((x1 - x0) * (y1 - y0)) : 0u;
-        uint32_t sp[4] = {0u, 0u, 0u, 0u};
+        uint32_t sp[GS_SPAN_ROWS / 2] = {};
         // Conic elongation kappa = A C / (A C - B^2): above 256 the ellipse arithmetic below
         // is not trusted (its rounding grows with kappa) and the whole rectangle is kept.
         const float kap_ac = p.a * p.c;
@@ -142,8 +142,8 @@ __global__ void __launch_bounds__(128) project_fwd_kernel(ProjectArgs a) {
         if (covers) {
             uint4* er = reinterpret_cast<uint4*>(a.erec + pair);
             er[0] = make_uint4((uint32_t)(vw.tile_offset + y0 * vw.tiles_x + x0),
-                               (uint32_t)vw.tiles_x | ((uint32_t)(x1 - x0) << 16) | (count & GS_PCOUNT_RECT),
-                               count & ~GS_PCOUNT_RECT, 0u);
+                               (uint32_t)vw.tiles_x | ((uint32_t)(x1 - x0) << 16) | (count & GS_PCOUNT_RECT), sp[4],
+                               sp[5]);
             er[1] = make_uint4(sp[0], sp[1], sp[2], sp[3]);
         }
         my_visible += covers ? 1u : 0u;

@@ -529,13 +529,13 @@ __device__ __forceinline__ uint32_t block_incl_max(uint32_t v, uint32_t* s_tmp) 
 // s_head is padded by one word per 32 (HP): each thread walks PER consecutive entries,
 // and without the padding threads t and t + 32 / PER would hit the same bank.
 __device__ __forceinline__ uint32_t HP(uint32_t i) { return i + (i >> 5); }
-constexpr size_t EM_EXPAND_SMEM = (size_t)(EM_OUT + 1) * (4 + 4 + 8 + 16) + (size_t)(EM_OUT + EM_OUT / 32) * 4;
+constexpr size_t EM_EXPAND_SMEM = (size_t)(EM_OUT + 1) * (4 + 4 + 16 + 16) + (size_t)(EM_OUT + EM_OUT / 32) * 4;
 
 __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
     constexpr int PER = EM_OUT / EM_THREADS;  // instances per thread
     extern __shared__ __align__(16) unsigned char em_smem[];
     uint4* s_span = reinterpret_cast<uint4*>(em_smem);                               // rows' tile spans
-    uint2* s_geom = reinterpret_cast<uint2*>(s_span + (EM_OUT + 1));                 // first tile, tiles_x | width << 16 | rect flag
+    uint4* s_geom = s_span + (EM_OUT + 1);  // first tile, tiles_x | width << 16 | rect flag, spans of rows 8..11
     uint32_t* s_off = reinterpret_cast<uint32_t*>(s_geom + (EM_OUT + 1));
     uint32_t* s_pair = s_off + (EM_OUT + 1);
     uint32_t* s_head = s_pair + (EM_OUT + 1);
@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
             const uint4 h = __ldg(er);
             s_off[j] = a.pair_offsets[p_lo + j];
             s_pair[j] = pair;
-            s_geom[j] = make_uint2(h.x, h.y);
+            s_geom[j] = h;
             s_span[j] = __ldg(er + 1);
         }
         __syncthreads();
@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
             const uint32_t ol = threadIdx.x * PER + k;
             const uint32_t j = max(before, loc[k]);
             jj[k] = j;
-            const uint2 gm = s_geom[j];
+            const uint4 gm = s_geom[j];
             const uint32_t tx = gm.y & 0xffffu, w = (gm.y >> 16) & 0x7fffu;
             uint32_t t = o0 + ol - s_off[j];
             uint32_t tile;
@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(EM_THREADS) emit_expand(EmitArgs a) {
             } else {
                 // Walk the rows' spans (at most GS_SPAN_ROWS).
                 const uint4 sp = s_span[j];
-                const uint32_t words[4] = {sp.x, sp.y, sp.z, sp.w};
+                const uint32_t words[6] = {sp.x, sp.y, sp.z, sp.w, gm.z, gm.w};
                 tile = gm.x;
 #pragma unroll
                 for (int r = 0; r < GS_SPAN_ROWS; r++) {
