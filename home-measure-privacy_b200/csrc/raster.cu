@@ -178,9 +178,6 @@ constexpr float KAPPA_EXACT = 32.f;     // elongation above which every pixel us
 #ifndef BWD_GROUPS
 #define BWD_GROUPS 2  // backward: 8 x 4 pixel groups evaluated together (1, 2 or 4)
 #endif
-#ifndef BWD_SKIP_EMPTY
-#define BWD_SKIP_EMPTY 1  // backward: skip the warp reduction of splats no pixel took
-#endif
 #ifndef FWD_GROUPS
 #define FWD_GROUPS 2  // forward: the same, in pixel pairs (2 or 4)
 #endif
@@ -634,7 +631,6 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                         float s0[L::WX], sy[L::WX], syy[L::WX];
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) s0[b] = sy[b] = syy[b] = 0.f;
-                        bool any_hit = false;  // a pixel of this lane took alpha != 0
                         // Groups go in blocks of BWD_GROUPS (a block is evaluated when any
                         // of its groups is live; the others' own tests give alpha = 0), so
                         // the compiler can interleave the dependency chains of a block's
@@ -655,7 +651,6 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                             bool hit;
                             const float alpha = alpha_pix(e, x.dx, dy, x.inb && k < mylast[p], g0, g1, a.alpha_max,
                                                           a.alpha_min, qlo, qhi, hit);
-                            any_hit = any_hit || hit;
                             const float ioma = rcp_approx(1.0f - alpha);
                             const float Tk = T[p] * ioma;
                             const float at = alpha * Tk;
@@ -676,9 +671,6 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                             syy[b] += dPy * dy;
                             }
                         }
-                        // The culling is conservative: when no pixel of the warp took the
-                        // splat, its sums are all zero and the reduction is skipped.
-                        if (BWD_SKIP_EMPTY && !__any_sync(FULL_MASK, any_hit)) continue;
                         float v8 = 0.f;
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) {
