@@ -399,9 +399,10 @@ constexpr int EM_THREADS = 256;
 constexpr int EM_ITEMS = 8;
 constexpr int EM_CHUNK = EM_THREADS * EM_ITEMS;
 #ifndef GS_EM_OUT
-#define GS_EM_OUT 1024
+#define GS_EM_OUT 512  // measured: 512 beats 1024 (-27 % emission) and 2048
 #endif
 constexpr int EM_OUT = GS_EM_OUT;  // instances per expansion block
+static_assert(EM_OUT % EM_THREADS == 0, "whole instances per expansion thread");
 
 int emit_chunk_items() { return EM_CHUNK; }
 int emit_out_items() { return EM_OUT; }

@@ -62,3 +62,43 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(hmp):
     assert lib.gs_loss_gradient_noalloc(p, p, 9, 1, 1, 0.2, 1, p, None, None) == N.GS_ERR_CAPACITY
     assert lib.gs_loss_gradient_noalloc(p, p, 0, 1, 1, 0.2, 1, p, None, None) == N.GS_ERR_CAPACITY
     assert lib.gs_loss_gradient_noalloc(None, p, 1, 1, 1, 0.2, 1, p, None, None) == N.GS_ERR_INVALID_ARG
+
+
+def test_noalloc_allocates_nothing_and_replays_from_a_graph(hmp):
+    """After a first call on the device, a call changes no device memory reservation
+    (cudaMemGetInfo unchanged), and the call captured into a CUDA graph on a side stream
+    and replayed gives the allocating path's gradient."""
+    import torch
+    from importlib import import_module
+    N = import_module("home-measure-privacy_b200._native")
+    lib = N.load()
+    w, h, lam, window, n = 96, 64, 0.2, 1, 2
+    img, tgt = _images(7, n, w, h)
+    with hmp.createRenderer() as r:
+        ref = [r.lossGradientOf(img[i], tgt[i], w, h, lam, window) for i in range(n)]
+    d_img = torch.from_numpy(img).cuda()
+    d_tgt = torch.from_numpy(tgt).cuda()
+    d_grad = torch.zeros((n, w * h * 3), device="cuda")
+    d_loss = torch.zeros((n,), device="cuda")
+
+    def call(stream):
+        return lib.gs_loss_gradient_noalloc(d_img.data_ptr(), d_tgt.data_ptr(), n, w, h, lam, window,
+                                            d_grad.data_ptr(), d_loss.data_ptr(), ctypes.c_void_p(stream))
+
+    assert call(torch.cuda.current_stream().cuda_stream) == N.GS_OK  # first call on the device
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    assert call(torch.cuda.current_stream().cuda_stream) == N.GS_OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    g = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.graph(g, stream=side):
+        rc = call(side.cuda_stream)
+    assert rc == N.GS_OK
+    d_grad.fill_(float("nan"))
+    g.replay()
+    torch.cuda.synchronize()
+    got = d_grad.cpu().numpy()
+    for i in range(n):
+        assert np.abs(got[i] - ref[i]).max() <= 1e-6 * np.abs(ref[i]).max(), i
