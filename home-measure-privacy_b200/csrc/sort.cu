@@ -172,8 +172,12 @@ constexpr int OS_THREADS = 256;
 constexpr int OS_ITEMS = RS_TILE / OS_THREADS;
 constexpr int OS_WARPS = OS_THREADS / 32;
 
+#ifndef OS_MIN_BLOCKS
+#define OS_MIN_BLOCKS 4  // resident partitions per SM the registers are sized for
+#endif
+
 template <typename W>
-__global__ void __launch_bounds__(OS_THREADS, 4) radix_onesweep(
+__global__ void __launch_bounds__(OS_THREADS, OS_MIN_BLOCKS) radix_onesweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ gex,
     W* look, uint32_t* counter, unsigned int* timeout, const unsigned int* debug_wait,
