@@ -425,7 +425,14 @@ __global__ void __launch_bounds__(EM_THREADS) emit_reduce(EmitArgs a) {
 #pragma unroll
         for (int j = 0; j < EM_ITEMS; j++) {
             const uint32_t sidx = c * EM_CHUNK + j * EM_THREADS + threadIdx.x;
-            if (sidx < M) sum += pair_count(a, __ldg(a.sorted_pairs + base + sidx));
+            if (sidx < M) {
+                // The gathered count is kept in depth order (in pair_offsets, which
+                // emit_offsets overwrites with the offsets), so the offsets pass reads it
+                // sequentially instead of gathering it again.
+                const uint32_t cnt = pair_count(a, __ldg(a.sorted_pairs + base + sidx));
+                a.pair_offsets[sidx] = cnt;
+                sum += cnt;
+            }
         }
         uint32_t tot;
         block_excl_scan<EM_THREADS>(sum, s_tmp, tot);
@@ -465,16 +472,13 @@ __global__ void __launch_bounds__(EM_THREADS) emit_offsets(EmitArgs a) {
     __shared__ uint32_t s_cnt[EM_CHUNK];
     __shared__ uint32_t s_tmp[32];
     const uint32_t M = *a.visible;
-    const uint32_t base = a.pair_seg->base;
     const uint32_t chunks = (M + EM_CHUNK - 1) / EM_CHUNK;
     const uint32_t total = a.inst_seg->count;
     for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
         const uint32_t first = c * EM_CHUNK;
         for (uint32_t j = threadIdx.x; j < EM_CHUNK; j += EM_THREADS) {
             const uint32_t s = first + j;
-            uint32_t cnt = 0;
-            if (s < M) cnt = pair_count(a, __ldg(a.sorted_pairs + base + s));
-            s_cnt[j] = cnt;
+            s_cnt[j] = s < M ? a.pair_offsets[s] : 0u;  // the counts emit_reduce kept
         }
         __syncthreads();
         uint32_t cnt[EM_ITEMS];
