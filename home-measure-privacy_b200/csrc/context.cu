@@ -170,7 +170,7 @@ struct GsContext {
     int last_first = -1, last_count = 0, last_batched = 1;
     bool have_loss = false;
     // raster tuning: shared-memory batch and pixels per thread of each kernel
-    int tile = GS_TILE;                 // tile edge of binning and raster (8, 16 or 32)
+    int tile = GS_TILE;                 // tile edge of binning and raster (8, 16, 32 or 64)
     int batch_fwd = 256, batch_bwd = 256, ppt_fwd = 4, ppt_bwd = 4;
     int wt_fwd = GS_TILE, wt_bwd = GS_TILE;  // raster work-tile edges (<= the tile edge)
     int ctas_fwd = 0, ctas_bwd = 0;

@@ -34,7 +34,7 @@ struct ViewDesc {
     int tile_offset;     // first global tile id of this view
     int pixel_offset;    // first pixel of this view in the per-pixel buffers
     int loss_blocks_x, loss_blocks_y, loss_block_offset;
-    int tile;            // tile edge in pixels (8, 16 or 32; the same for every view)
+    int tile;            // tile edge in pixels (8, 16, 32 or 64; the same for every view)
 };
 
 // Step status kept on the device; mirrored to pinned host memory.  The first 24 bytes

@@ -152,9 +152,9 @@ struct RasterArgs {
     unsigned int* work_counter;     // persistent queue head (nullptr = one CTA per tile)
     const uint32_t* tile_order;     // optional permutation of the tiles (heavy first)
 };
-// Raster variants: tile edge (8, 16 or 32 pixels), shared-memory batch (32, 64, 128 or 256
+// Raster variants: tile edge (8, 16, 32 or 64 pixels), shared-memory batch (32, 64, 128 or 256
 // splats), pixels per thread, and the work tile a CTA covers (the tile itself, or for
-// 32-pixel tiles a 16 x 16 quarter of it; raster_variant_ok lists what exists).
+// 32- and 64-pixel tiles a 16 x 16 part of it; raster_variant_ok lists what exists).
 bool raster_variant_ok(int tile, int wt, int ppt);
 void launch_raster_fwd(const RasterArgs& a, int tile, int wt, int batch, int ppt, int persistent_ctas,
                        cudaStream_t s);

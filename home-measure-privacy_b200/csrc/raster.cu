@@ -1,8 +1,9 @@
 // Tiled alpha blending, forward and backward.
 //
-// A tile of TILE x TILE pixels (8, 16 or 32; 16 is the reference's) is cut into groups of
-// 8 x 4 pixels; lane l of a warp holds pixel (l & 7, l >> 3) of each group the warp owns.
-// With PPT pixels per thread a CTA of TILE^2 / PPT threads owns one tile and each warp a
+// A tile of TILE x TILE pixels (8, 16, 32 or 64; 16 is the reference's) is cut into
+// groups of 8 x 4 pixels; lane l of a warp holds pixel (l & 7, l >> 3) of each group the
+// warp owns.  With PPT pixels per thread a CTA of WT^2 / PPT threads owns a WT x WT work
+// tile (the whole tile, or a 16 x 16 part of a 32- or 64-pixel tile) and each warp a
 // block of PPT groups (1 x PPT groups, or 2 x 4 with 8 pixels per thread; Lay below).
 // The tile's depth-ordered list is walked in batches: the CTA stages a batch of splat
 // records (32-byte geometry + 16-byte colour, gathered by pair index) in shared memory
@@ -28,8 +29,8 @@
 // 32-byte vector of float reductions and lane 0 a ninth: one global atomic transaction
 // per (warp, splat) instead of nine CAS loops per pixel (the reference's addF, :148-157).
 //
-// A CTA covers the whole tile or, for 32 x 32 tiles, one 16 x 16 quarter of it (a work
-// tile); every quarter walks the tile's whole list.
+// A CTA covers the whole tile or, for 32 x 32 and 64 x 64 tiles, one 16 x 16 part of it
+// (a work tile); every part walks the tile's whole list.
 //
 // In the persistent mode a fixed grid pulls (view, tile) work items from a global
 // counter, in an order that puts the longest tile lists first.
