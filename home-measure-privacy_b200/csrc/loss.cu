@@ -26,9 +26,27 @@
 
 namespace gs {
 
-constexpr int LB_W = 32;
-constexpr int LB_H = 32;
-constexpr int LB_THREADS = 256;
+// Output block of a CTA and its threads (build options; every pass gives each thread one
+// strip of outputs, which the static assert below checks).
+#ifndef LOSS_BW
+#define LOSS_BW 32
+#endif
+#ifndef LOSS_BH
+#define LOSS_BH 32
+#endif
+#ifndef LOSS_THREADS
+#define LOSS_THREADS 256
+#endif
+#ifndef LOSS_NS1
+#define LOSS_NS1 4  // strips per region row in the first pass
+#endif
+#ifndef LOSS_MIN_BLOCKS
+#define LOSS_MIN_BLOCKS 3
+#endif
+constexpr int LB_W = LOSS_BW;
+constexpr int LB_H = LOSS_BH;
+constexpr int LB_THREADS = LOSS_THREADS;
+static_assert(LB_THREADS >= 256 && LB_THREADS % 32 == 0, "the byte table takes one thread per value");
 
 struct LossWeights {
     float w[11];
@@ -48,8 +66,8 @@ struct LossDims {
     static constexpr int CFP = HW + 1;
     // Strips: P1 horizontal moments, P2 vertical moments -> coefficients, P3 horizontal
     // coefficients, P4 vertical coefficients -> gradient.  One task per thread each.
-    static constexpr int S1 = (HW + 3) / 4;                 // 4 strips per region row
-    static constexpr int NS1 = 4;
+    static constexpr int NS1 = LOSS_NS1;                    // strips per region row
+    static constexpr int S1 = (HW + NS1 - 1) / NS1;
     static constexpr int S2 = 7;
     static constexpr int NS2 = (CH + S2 - 1) / S2;
     static constexpr int S3 = 6;
@@ -94,14 +112,14 @@ __device__ __forceinline__ float load_target<float>(const float* t, size_t idx, 
 }
 
 template <int R, typename TT>
-__global__ void __launch_bounds__(LB_THREADS, 3) loss_kernel(LossArgs a, const TT* __restrict__ target,
+__global__ void __launch_bounds__(LB_THREADS, LOSS_MIN_BLOCKS) loss_kernel(LossArgs a, const TT* __restrict__ target,
                                                           LossWeights wts) {
     using D = LossDims<R>;
     constexpr int K = D::K;
     extern __shared__ __align__(16) float sm[];
     __shared__ float s_red[2][LB_THREADS / 32];
     __shared__ float s_lut[256];
-    if (sizeof(TT) == 1) s_lut[threadIdx.x] = (float)threadIdx.x / 255.0f;
+    if (sizeof(TT) == 1 && threadIdx.x < 256) s_lut[threadIdx.x] = (float)threadIdx.x / 255.0f;
     const int blk = a.block_first + (int)(blockIdx.x / 3u);
     const int c = (int)(blockIdx.x % 3u);
     int vi = a.view_first;
