@@ -377,13 +377,14 @@ def run_b200(args, rank, local, world, dist):
 def profile_case(args):
     """Small case for ncu captures (one kernel, few launches, ~2 GB on the device): the
     benchmark scene (1M Gaussians, SH3) seen by its three largest views, raster variants
-    fixed at batch 128, --profile-ppt pixels per thread (default 4), --profile-tile pixel
-    tiles (default 16) and --profile-wt work tiles, three graph-replayed training steps."""
+    fixed by --profile-batch (default 128), --profile-ppt pixels per thread (default 4),
+    --profile-tile pixel tiles (default 16) and --profile-wt work tiles, three
+    graph-replayed training steps."""
     hmp = importlib.import_module("home-measure-privacy_b200")
     c = hmp.config(3)
     cams = c["cameras"][-3:]
     targets = make_targets(hmp, c, cams, 0)
-    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=128, raster_ppt=args.profile_ppt,
+    with hmp.createRenderer(sh_degree=c["degree"], near=c["near"], raster_batch=args.profile_batch, raster_ppt=args.profile_ppt,
                             tile_size=args.profile_tile, raster_work_tile=args.profile_wt, device=0) as r:
         r.set_gaussians(c["records"])
         r.set_views(cams)
@@ -671,6 +672,8 @@ def main():
                     help="file caching the raster variant choice (a profiled run then uses the unprofiled choice)")
     ap.add_argument("--profile-tile", type=int, default=16, choices=(8, 16, 32, 64),
                     help="--profile-case: tile edge in pixels")
+    ap.add_argument("--profile-batch", type=int, default=128, choices=(32, 64, 128, 256),
+                    help="--profile-case: splats per raster batch")
     ap.add_argument("--profile-wt", type=int, default=0, choices=(0, 8, 16, 32),
                     help="--profile-case: raster work tile edge (0 = the tile edge)")
     ap.add_argument("--profile-ppt", type=int, default=4, choices=(2, 4, 8),
