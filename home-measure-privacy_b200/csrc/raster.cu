@@ -202,7 +202,7 @@ __device__ __forceinline__ float conic_kappa(float A, float B, float C) {
 // thousands of times q itself).  Above KAPPA_EXACT the rounding of the reference's own
 // exponent shows in alpha's value, so such splats (about 1 % of the benchmark's list
 // entries) get an unbounded band: every pixel takes alpha from the reference expression.
-// s_c.w holds the band's lower end qlo; its upper end is 2 log2(alpha_min) - qlo.
+// s_c.w holds the band's lower end qlo; the band is symmetric about log2(alpha_min).
 __device__ __forceinline__ void prepare_batch(int cnt, float4* s_g0, float4* s_g1, float4* s_q, float4* s_c,
                                               float log_amin, float qthr) {
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
@@ -319,16 +319,16 @@ __device__ __forceinline__ float2 exponent2(const XTerm& xt, float2 qc, float2 d
 
 // alpha at one pixel from its exponent e and row offset dy, or 0 when the pixel skips
 // the splat (live: the pixel still takes part and its column lies within the bounding
-// square): 2^e by the fast exp2; within [qlo, qhi) around the alpha_min threshold (the
-// splat's band) the reference expression decides.  hit = alpha != 0.  Branch-free but
-// for the band.
-__device__ __forceinline__ float alpha_pix(float e, float dx, float dy, bool live, const float4& g0,
-                                           const float4& g1, float amax, float amin, float qlo, float qhi,
-                                           bool& hit) {
+// square): 2^e by the fast exp2; where |e - log2(alpha_min)| < hw (the splat's band,
+// ec = e - log2(alpha_min)) the reference expression decides.  One compare tests the
+// band: it is symmetric about the threshold.  hit = alpha != 0.  Branch-free but for the
+// band.
+__device__ __forceinline__ float alpha_pix(float e, float ec, float dx, float dy, bool live, const float4& g0,
+                                           const float4& g1, float amax, float amin, float hw, bool& hit) {
     const bool inb = live && fabsf(dy) <= g1.z;
-    hit = inb && e >= qhi;
+    hit = inb && ec >= hw;
     float alpha = hit ? fminf(amax, ex2_approx(e)) : 0.f;
-    if (inb && e >= qlo && e < qhi) {
+    if (inb && fabsf(ec) < hw) {
         alpha = alpha_band(g0, g1, dx, dy, amax, amin);
         hit = alpha != 0.f;
     }
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, fwd_min_ctas(WT, PPT)) raste
                     const float4 g1 = g1s[j];
                     const float4 q = qs[j];
                     const float4 c = cs[j];
-                    const float qlo = c.w, qhi = 2.0f * qthr - c.w;  // the splat's band
+                    const float hw = qthr - c.w;  // half-width of the splat's band
                     const uint32_t pos = b0 + (uint32_t)j + 1u;
                     const float2 qc = f2(q.z), ngy = f2(-g0.y);
                     const float2 cx = f2(c.x), cy = f2(c.y), cz = f2(c.z);
@@ -433,11 +433,12 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, fwd_min_ctas(WT, PPT)) raste
                         const XTerm& x = xt[(2 * i) / L::WY];
                         const float2 dy = add2(pyf[i], ngy);
                         const float2 e = exponent2(x, qc, dy);
+                        const float2 ec = add2(e, f2(-qthr));
                         bool h0, h1;
-                        const float a0 = alpha_pix(e.x, x.dx, dy.x, x.inb && T[i].x > a.t_min, g0, g1, a.alpha_max,
-                                                   a.alpha_min, qlo, qhi, h0);
-                        const float a1 = alpha_pix(e.y, x.dx, dy.y, x.inb && T[i].y > a.t_min, g0, g1, a.alpha_max,
-                                                   a.alpha_min, qlo, qhi, h1);
+                        const float a0 = alpha_pix(e.x, ec.x, x.dx, dy.x, x.inb && T[i].x > a.t_min, g0, g1,
+                                                   a.alpha_max, a.alpha_min, hw, h0);
+                        const float a1 = alpha_pix(e.y, ec.y, x.dx, dy.y, x.inb && T[i].y > a.t_min, g0, g1,
+                                                   a.alpha_max, a.alpha_min, hw, h1);
                         const float2 alpha = make_float2(a0, a1);
                         const float2 wgt = mul2(alpha, T[i]);
                         cr[i] = fma2(cx, wgt, cr[i]);
@@ -617,7 +618,7 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                         const float4 g1 = g1s[j];
                         const float4 q = qs[j];
                         const float4 c = cs[j];
-                        const float qlo = c.w, qhi = 2.0f * qthr - c.w;  // the splat's band
+                        const float hw = qthr - c.w;  // half-width of the splat's band
                         XTerm xt[L::WX];
 #pragma unroll
                         for (int b = 0; b < L::WX; b++) xt[b] = xterm(q, pxf[b] - g0.x, g1.z);
@@ -650,8 +651,8 @@ __global__ void __launch_bounds__(Lay<WT, PPT>::NT, bwd_min_ctas(WT, PPT)) raste
                             const float dy = (pyf0 + (float)(4 * (p % L::WY))) - g0.y;
                             const float e = __fmaf_rn(dy, __fmaf_rn(q.z, dy, x.b0.x), x.a0.x);
                             bool hit;
-                            const float alpha = alpha_pix(e, x.dx, dy, x.inb && k < mylast[p], g0, g1, a.alpha_max,
-                                                          a.alpha_min, qlo, qhi, hit);
+                            const float alpha = alpha_pix(e, e - qthr, x.dx, dy, x.inb && k < mylast[p], g0, g1,
+                                                          a.alpha_max, a.alpha_min, hw, hit);
                             const float ioma = rcp_approx(1.0f - alpha);
                             const float Tk = T[p] * ioma;
                             const float at = alpha * Tk;
