@@ -562,7 +562,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ea.max_chunks = (int)((int64_t)vcount * c->n_pad / emit_chunk_items() + 1);
     launch_emit(ea, c->stream, c->num_sms);
     count_launches(c, ST_EMIT, 4);
-    // Stable sort by tile id, then the tile ranges.
+    // Stable sort by tile id; its last pass bounds the tile ranges.
     CKI(mark(c, ST_SORT_INST));
     RadixSortArgs rb = ra;
     rb.keys = c->ikeys.as<uint32_t>();
@@ -574,11 +574,12 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     rb.begin_bit = 0;
     rb.end_bit = c->tile_bits;
     rb.max_parts = (int)((c->inst_cap + radix_tile_items() - 1) / radix_tile_items());
+    rb.ranges = c->ranges.as<uint2>();
     launch_radix_sort(rb, c->stream, c->num_sms);
-    launch_ranges(c->ikeys.as<uint32_t>(), inst_seg, c->ranges.as<uint2>(), c->stream, c->num_sms);
+    RasterArgs r = raster_args(c, vfirst, vcount);
+    launch_ranges_finish(c->ranges.as<uint2>() + r.tile_first, r.num_tiles, c->stream);
     count_launches(c, ST_SORT_INST, 1 + radix_sort_passes(0, c->tile_bits) + 1);
     // Blend.
-    RasterArgs r = raster_args(c, vfirst, vcount);
     if (batched) {
         if (c->cfg.lpt_order) {
             launch_tile_order(c->ranges.as<uint2>(), r.tile_first, r.num_tiles, c->tile_order.as<uint32_t>(), nullptr,

@@ -94,6 +94,10 @@ struct RadixSortArgs {
     const unsigned int* debug_wait;  // test hook (device word): partition 1 of every pass first
                                      // polls *never_set this many times, then gives up
     const unsigned int* never_set;
+    // Non-null: the keys are tile ids and the last pass writes no keys; it bounds each
+    // tile's run instead, ranges[t] = (~first, last + 1) by atomic maxima into zeroed
+    // words (launch_ranges_finish turns ~first into first).
+    uint2* ranges = nullptr;
 };
 int radix_sort_passes(int begin_bit, int end_bit);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms);
@@ -125,9 +129,9 @@ void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms);
 int emit_chunk_items();
 int emit_out_items();
 
-// Tile ranges from tile-sorted instances.
-void launch_ranges(const uint32_t* sorted_tiles, const SegInfo* seg, uint2* ranges,
-                   cudaStream_t s, int num_sms);
+// Completes the ranges a tile sort's last pass bounded (RadixSortArgs::ranges) for tiles
+// [0, count) of `ranges`: tiles without instances stay (0, 0).
+void launch_ranges_finish(uint2* ranges, int count, cudaStream_t s);
 
 // ---- rasterisation ---------------------------------------------------------------------
 struct RasterArgs {

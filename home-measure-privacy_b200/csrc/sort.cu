@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(OS_THREADS, OS_MIN_BLOCKS) radix_onesweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, const SegInfo* seg, int shift, const uint32_t* __restrict__ gex,
     W* look, uint32_t* counter, unsigned int* timeout, const unsigned int* debug_wait,
-    const unsigned int* never_set) {
+    const unsigned int* never_set, uint2* ranges) {
     using LW = LookWord<W>;
     __shared__ uint32_t s_keys[RS_TILE];
     __shared__ uint32_t s_vals[RS_TILE];
@@ -344,6 +344,21 @@ __global__ void __launch_bounds__(OS_THREADS, OS_MIN_BLOCKS) radix_onesweep(
     }
     __syncthreads();
     const uint32_t total = min((uint32_t)RS_TILE, n - part_start);
+    if (ranges) {
+        // Last pass of the tile sort: the sorted tile ids themselves are not needed, only
+        // where each tile's run starts and ends.  Each run of one id in this partition
+        // bounds its tile's range from both sides; the maxima over all partitions are the
+        // range (the output is sorted, so a tile's instances are contiguous).
+        for (uint32_t i = threadIdx.x; i < total; i += OS_THREADS) {
+            const uint32_t key = s_keys[i];
+            const uint32_t dk = (key >> shift) & 0xffu;
+            const uint32_t out = base + s_global[dk] + (i - s_digit_start[dk]);
+            if (i == 0 || s_keys[i - 1] != key) atomicMax(&ranges[key].x, ~out);
+            if (i + 1 == total || s_keys[i + 1] != key) atomicMax(&ranges[key].y, out + 1);
+            vals_out[out] = s_vals[i];
+        }
+        return;
+    }
     for (uint32_t i = threadIdx.x; i < total; i += OS_THREADS) {
         const uint32_t key = s_keys[i];
         const uint32_t dk = (key >> shift) & 0xffu;
@@ -372,17 +387,19 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
     for (int p = 0; p < passes; p++) {
         const int in = p & 1, out = in ^ 1;
         const uint32_t* vin = (p == 0 && a.iota) ? nullptr : vb[in];
+        uint2* rg = p == passes - 1 ? a.ranges : nullptr;
         if (wide) {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(unsigned long long), s);
             radix_onesweep<unsigned long long><<<grid, OS_THREADS, 0, s>>>(
                 kb[in], vin, kb[out], vb[out], a.seg, a.begin_bit + p * step, gex + p * 256,
-                reinterpret_cast<unsigned long long*>(a.hist), counters + p, a.timeout, a.debug_wait, a.never_set);
+                reinterpret_cast<unsigned long long*>(a.hist), counters + p, a.timeout, a.debug_wait, a.never_set,
+                rg);
         } else {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
             radix_onesweep<uint32_t><<<grid, OS_THREADS, 0, s>>>(kb[in], vin, kb[out], vb[out], a.seg,
                                                                   a.begin_bit + p * step, gex + p * 256,
                                                                   reinterpret_cast<uint32_t*>(a.hist), counters + p,
-                                                                  a.timeout, a.debug_wait, a.never_set);
+                                                                  a.timeout, a.debug_wait, a.never_set, rg);
         }
     }
 }
@@ -655,38 +672,21 @@ void launch_emit(const EmitArgs& a, cudaStream_t s, int num_sms) {
 
 // ---------------------------------------------------------------------------------
 // Tile ranges: each tile's [first, last + 1) in the tile-sorted instances (absolute
-// indices).  Tiles without instances keep the zeroed (0, 0).
+// indices), bounded by the tile sort's last pass.  Tiles without instances keep the
+// zeroed (0, 0).
 // ---------------------------------------------------------------------------------
-constexpr int RG_ITEMS = 16;
-
-// Each thread takes RG_ITEMS consecutive sorted keys and compares neighbours in
-// registers (one extra load for the key before its chunk).
-__global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict__ tiles, const SegInfo* seg,
-                                                    uint2* ranges) {
-    const uint32_t base = seg->base, n = seg->count;
-    const uint32_t chunks = (n + RG_ITEMS - 1) / RG_ITEMS;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < chunks; c += gridDim.x * blockDim.x) {
-        const uint32_t i0 = c * RG_ITEMS;
-        uint32_t t[RG_ITEMS];
-#pragma unroll
-        for (int k = 0; k < RG_ITEMS; k++) t[k] = (i0 + k < n) ? __ldg(tiles + base + i0 + k) : 0xffffffffu;
-        uint32_t prev = i0 > 0 ? __ldg(tiles + base + i0 - 1) : 0xffffffffu;
-        const uint32_t next = (i0 + RG_ITEMS < n) ? __ldg(tiles + base + i0 + RG_ITEMS) : 0xffffffffu;
-#pragma unroll
-        for (int k = 0; k < RG_ITEMS; k++) {
-            const uint32_t i = i0 + k;
-            if (i >= n) break;
-            const uint32_t nx = (k + 1 < RG_ITEMS) ? t[k + 1] : next;
-            if (t[k] != prev) ranges[t[k]].x = base + i;
-            if (i + 1 == n || nx != t[k]) ranges[t[k]].y = base + i + 1;
-            prev = t[k];
-        }
+// (~first, last + 1) -> (first, last + 1); an untouched (0, 0) stays.  No tile starts at
+// index 0xffffffff (the instance capacity is below 2^32 - 1), so ~first is never 0.
+__global__ void __launch_bounds__(256) ranges_finish_kernel(uint2* ranges, int count) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const uint32_t x = ranges[t].x;
+        if (x) ranges[t].x = ~x;
     }
 }
 
-void launch_ranges(const uint32_t* sorted_tiles, const SegInfo* seg, uint2* ranges, cudaStream_t s,
-                   int num_sms) {
-    ranges_kernel<<<num_sms * 16, 256, 0, s>>>(sorted_tiles, seg, ranges);
+void launch_ranges_finish(uint2* ranges, int count, cudaStream_t s) {
+    if (count <= 0) return;
+    ranges_finish_kernel<<<(count + 255) / 256, 256, 0, s>>>(ranges, count);
 }
 
 cudaError_t radix_prepare() {
