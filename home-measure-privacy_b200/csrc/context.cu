@@ -530,6 +530,7 @@ static int forward_group(GsContext* c, int step_first, int vfirst, int vcount, b
     ra.seg = pair_seg;
     ra.begin_bit = 0;
     ra.end_bit = 31;
+    ra.discard_keys = true;  // the emission reads the sorted pairs only
     ra.hist = c->hist.as<unsigned long long>();
     ra.totals = c->totals.as<uint32_t>();
     ra.timeout = &c->status.as<DevStatus>()->sort_timeout;

@@ -98,6 +98,8 @@ struct RadixSortArgs {
     // tile's run instead, ranges[t] = (~first, last + 1) by atomic maxima into zeroed
     // words (launch_ranges_finish turns ~first into first).
     uint2* ranges = nullptr;
+    // True: only the sorted values are wanted; the last pass writes no keys.
+    bool discard_keys = false;
 };
 int radix_sort_passes(int begin_bit, int end_bit);
 void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms);

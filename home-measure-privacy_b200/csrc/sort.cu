@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(OS_THREADS, OS_MIN_BLOCKS) radix_onesweep(
         const uint32_t key = s_keys[i];
         const uint32_t dk = (key >> shift) & 0xffu;
         const uint32_t out = base + s_global[dk] + (i - s_digit_start[dk]);
-        keys_out[out] = key;
+        if (keys_out) keys_out[out] = key;
         vals_out[out] = s_vals[i];
     }
 }
@@ -388,15 +388,16 @@ void launch_radix_sort(const RadixSortArgs& a, cudaStream_t s, int num_sms) {
         const int in = p & 1, out = in ^ 1;
         const uint32_t* vin = (p == 0 && a.iota) ? nullptr : vb[in];
         uint2* rg = p == passes - 1 ? a.ranges : nullptr;
+        uint32_t* kout = (p == passes - 1 && a.discard_keys) ? nullptr : kb[out];
         if (wide) {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(unsigned long long), s);
             radix_onesweep<unsigned long long><<<grid, OS_THREADS, 0, s>>>(
-                kb[in], vin, kb[out], vb[out], a.seg, a.begin_bit + p * step, gex + p * 256,
+                kb[in], vin, kout, vb[out], a.seg, a.begin_bit + p * step, gex + p * 256,
                 reinterpret_cast<unsigned long long*>(a.hist), counters + p, a.timeout, a.debug_wait, a.never_set,
                 rg);
         } else {
             cudaMemsetAsync(a.hist, 0, (size_t)grid * 256 * sizeof(uint32_t), s);
-            radix_onesweep<uint32_t><<<grid, OS_THREADS, 0, s>>>(kb[in], vin, kb[out], vb[out], a.seg,
+            radix_onesweep<uint32_t><<<grid, OS_THREADS, 0, s>>>(kb[in], vin, kout, vb[out], a.seg,
                                                                   a.begin_bit + p * step, gex + p * 256,
                                                                   reinterpret_cast<uint32_t*>(a.hist), counters + p,
                                                                   a.timeout, a.debug_wait, a.never_set, rg);
