@@ -154,11 +154,12 @@ def algorithmic_bytes(st, n, planes, views, pixels, tiles):
     passes_pairs, passes_inst = 4, 2 * math.ceil(math.ceil(bits / 8) / 2)  # 8-bit digits, an even count
     return {
         "project": n * P + pairs * (48 + 8 + 4),
-        # one digit-count read of the keys, then per pass keys + values read and written
-        # (the first pair pass generates its values)
-        "sort_pairs": pairs * 4 + passes_pairs * pairs * 16 - pairs * 4,
+        # one digit-count read of the keys, then per pass keys + values read and written;
+        # the first pair pass generates its values and the last pass of either sort
+        # writes no keys (the tile sort's bounds the tile ranges instead)
+        "sort_pairs": pairs * 4 + passes_pairs * pairs * 16 - 2 * pairs * 4,
         "emit": pairs * (4 + 8) * 2 + inst * 8,
-        "sort_instances": inst * 4 + passes_inst * inst * 16 + inst * 4,
+        "sort_instances": inst * 4 + passes_inst * inst * 16 - inst * 4 + tiles * 8,
         # instance list, tile ranges, splat records of the visible pairs, per-pixel image / state
         "raster_fwd": inst * 4 + tiles * 8 + vis * 48 + pixels * (12 + 4 + 4),
         "loss": pixels * (12 + 3 + 12),
