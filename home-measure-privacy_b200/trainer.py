@@ -189,8 +189,11 @@ class Renderer:
         order, one view per step; gradient statistics every step and densification on the
         device every `densifyEvery` steps in [densifyFrom, densifyUntil] (split above 1 %
         of the scene extent, with `prune` drop above 10 %), the opacity reset halfway
-        when `opacityReset`; mean L1 sampled every 25 steps and reported every 50.
-        views: [{cam, image: uint8 RGB}]."""
+        when `opacityReset`; the step loss sampled every 25 steps and their mean reported
+        every 50.  The sampled loss is the training loss, (1 - ssim) L1 + ssim (1 - SSIM):
+        the reference samples plain L1 (trainer/gpu.js:934-940), the same at the default
+        ssim = 0.  The photo order and densify's split samples come from generators
+        seeded by `seed`.  views: [{cam, image: uint8 RGB}]."""
         self.set_gaussians(start)
         self.set_views([v["cam"] for v in views])
         for k, v in enumerate(views):
