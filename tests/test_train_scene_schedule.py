@@ -9,7 +9,6 @@ reset at round((from + until) / 2 / every) * every when `opacityReset`; the loss
 sampled every 25 steps, their mean reported every 50 steps with the splat count;
 `shouldStop` ends the loop before the next step.
 """
-import ctypes
 import importlib
 import math
 
